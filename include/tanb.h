@@ -1,0 +1,214 @@
+/*
+ * tanb.h -- C ABI of the B200-native TrueAudio Next convolution path.
+ *
+ * Every entry point here stands in for one member of amf::TANConvolution or one
+ * TAN factory function (tan/tanlibrary/include/TrueAudioNext.h); the comment
+ * above each names the reference declaration it replaces. Arguments keep the
+ * reference's meaning; C++ references and cl_mem become plain pointers (device
+ * pointers where the reference takes cl_mem). Return values are AMF_RESULT
+ * codes (amf/public/include/core/Result.h:43-125).
+ *
+ * Threading: one tanb_convolution is driven by one thread at a time for
+ * Process* and by one thread at a time for UpdateResponse*, like the
+ * reference's per-object locks (ConvolutionImpl.h:210-216). Each object owns a
+ * CUDA stream on its context's device.
+ */
+#ifndef TANB_H
+#define TANB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* AMF_RESULT subset (amf/public/include/core/Result.h:43-125). */
+enum {
+  TANB_OK = 0,
+  TANB_FAIL = 1,
+  TANB_UNEXPECTED = 2,
+  TANB_INVALID_ARG = 4,
+  TANB_OUT_OF_MEMORY = 6,
+  TANB_INVALID_POINTER = 7,
+  TANB_NOT_IMPLEMENTED = 9,
+  TANB_NOT_SUPPORTED = 10,
+  TANB_NOT_FOUND = 11,
+  TANB_ALREADY_INITIALIZED = 12,
+  TANB_NOT_INITIALIZED = 13,
+  TANB_WRONG_STATE = 15,
+  TANB_NO_DEVICE = 17,
+  TANB_TAN_UNSUPPORTED_VERSION = 43
+};
+
+/* TAN_CONVOLUTION_METHOD (TrueAudioNext.h:81-99). */
+enum {
+  TANB_METHOD_FFT_OVERLAP_ADD = 0,
+  TANB_METHOD_FFT_PARTITIONED_UNIFORM = 1,
+  TANB_METHOD_FFT_PARTITIONED_NONUNIFORM = 2,
+  TANB_METHOD_FFT_UNIFORM_PARTITIONED = 3,
+  TANB_METHOD_FHT_UNIFORM_PARTITIONED = 4,
+  TANB_METHOD_FFT_UNIFORM_HEAD_TAIL = 5,
+  TANB_METHOD_FHT_UNIFORM_HEAD_TAIL = 6,
+  TANB_METHOD_TIME_DOMAIN = 7,
+  TANB_METHOD_FHT_NONUNIFORM_PARTITIONED = 8,
+  TANB_METHOD_FFT_NONUNIFORM_PARTITIONED = 9,
+  TANB_METHOD_USE_PROCESS_FINALIZE = 0x8000,
+  TANB_METHOD_USE_PROCESS_TAILTHREAD = 0xC000
+};
+
+/* TAN_CONVOLUTION_CHANNEL_FLAG (TrueAudioNext.h:105-110). */
+enum {
+  TANB_CHANNEL_FLAG_PROCESS = 0,
+  TANB_CHANNEL_FLAG_STOP_INPUT = 0x01,
+  TANB_CHANNEL_FLAG_FLUSH_STREAM = 0x02
+};
+
+/* TAN_CONVOLUTION_OPERATION_FLAG (TrueAudioNext.h:116-120). */
+enum {
+  TANB_OPERATION_FLAG_NONE = 0x00,
+  TANB_OPERATION_FLAG_BLOCK_UNTIL_READY = 0x01
+};
+
+/* TAN_FULL_VERSION layout (TrueAudioNext.h:43-52): major in bits 48..63. */
+#define TANB_VERSION_MAJOR 1
+#define TANB_VERSION_MINOR 3
+#define TANB_FULL_VERSION                                          \
+  (((uint64_t)TANB_VERSION_MAJOR << 48) | ((uint64_t)TANB_VERSION_MINOR << 32) | \
+   ((uint64_t)1 << 16) | (uint64_t)1)
+
+typedef struct tanb_context tanb_context;
+typedef struct tanb_convolution tanb_convolution;
+
+/* TANCreateContext(amf_uint64 version, TANContext**) -- TrueAudioNext.h:647,
+ * TANContextImpl.cpp:87-127. Major version must be 1. `device` is the CUDA
+ * device ordinal the context's objects run on (the reference's OpenCL
+ * queues, TANContext::InitOpenCL, TrueAudioNext.h:587-592). */
+int32_t tanb_create_context(uint64_t version, int32_t device, tanb_context** ctx);
+
+/* TANContext::Release (AMFInterface refcount, amf/public/include/core/Interface.h:63-80). */
+int32_t tanb_context_release(tanb_context* ctx);
+
+/* TANCreateConvolution(TANContext*, TANConvolution**) -- TrueAudioNext.h:650-652,
+ * ConvolutionImpl.cpp:66-80. */
+int32_t tanb_create_convolution(tanb_context* ctx, tanb_convolution** conv);
+
+/* TANConvolution::Release (Interface.h:63-80); also terminates. */
+int32_t tanb_convolution_release(tanb_convolution* conv);
+
+/* TANConvolution::Init / InitCpu / InitGpu (TrueAudioNext.h:134-146,
+ * ConvolutionImpl.cpp:179-281, 1113-1259). `method` is a TANB_METHOD_* value,
+ * optionally or-ed with TANB_METHOD_USE_PROCESS_FINALIZE. Every partitioned
+ * and head/tail method runs the uniformly-partitioned engine; bufferSize must
+ * be a power of two in [32, 8192] (the reference's GPU rule, :1136-1146). */
+int32_t tanb_convolution_init(tanb_convolution* conv, uint32_t method,
+                              uint32_t responseLengthInSamples,
+                              uint32_t bufferSizeInSamples, uint32_t channels);
+
+/* TANConvolution::Terminate (TrueAudioNext.h:148, ConvolutionImpl.cpp:307-352). */
+int32_t tanb_convolution_terminate(tanb_convolution* conv);
+
+/* TANConvolution::UpdateResponseTD(float* ppBuffer[], ...) -- TrueAudioNext.h:158-162,
+ * ConvolutionImpl.cpp:357-382, 407-695. Host IRs, one array per channel of
+ * numOfSamples <= responseLength floats. Channels flagged STOP_INPUT keep
+ * their IR; FLUSH_STREAM channels are flushed. The new IR takes effect, with
+ * a one-block linear crossfade, on the next processed block. The caller may
+ * reuse the IR buffers as soon as this returns. */
+int32_t tanb_convolution_update_response_td(tanb_convolution* conv,
+                                            const float* const* ppBuffer,
+                                            size_t numOfSamples,
+                                            const uint32_t* flagMasks,
+                                            uint32_t operationFlags);
+
+/* TANConvolution::UpdateResponseTD(cl_mem ppBuffer[], ...) -- TrueAudioNext.h:163-167.
+ * Same as above with device-resident IR arrays. */
+int32_t tanb_convolution_update_response_td_device(tanb_convolution* conv,
+                                                   const float* const* ppDeviceBuffer,
+                                                   size_t numOfSamples,
+                                                   const uint32_t* flagMasks,
+                                                   uint32_t operationFlags);
+
+/* TANConvolution::UpdateResponseFD (both overloads) -- TrueAudioNext.h:177-186,
+ * ConvolutionImpl.cpp:697-717: not supported, as in the reference. */
+int32_t tanb_convolution_update_response_fd(tanb_convolution* conv,
+                                            const float* const* ppBuffer,
+                                            size_t numOfSamples,
+                                            const uint32_t* flagMasks,
+                                            uint32_t operationFlags);
+
+/* TANConvolution::Process(float* in[], float* out[], ...) -- TrueAudioNext.h:200-205,
+ * ConvolutionImpl.cpp:809-1043. Host buffers. Processes every whole block of
+ * bufferSize samples in numOfSamples; *pNumOfSamplesProcessed (nullable) gets
+ * that count. Outputs of stopped (free) channels are left untouched. */
+int32_t tanb_convolution_process(tanb_convolution* conv,
+                                 const float* const* ppBufferInput,
+                                 float* const* ppBufferOutput,
+                                 size_t numOfSamples,
+                                 const uint32_t* flagMasks,
+                                 size_t* pNumOfSamplesProcessed);
+
+/* TANConvolution::Process(float* in[], cl_mem out[], ...) -- TrueAudioNext.h:207-212,
+ * ConvolutionImpl.cpp:782-806. Host input, device output arrays. */
+int32_t tanb_convolution_process_host_to_device(tanb_convolution* conv,
+                                                const float* const* ppBufferInput,
+                                                float* const* ppDeviceOutput,
+                                                size_t numOfSamples,
+                                                const uint32_t* flagMasks,
+                                                size_t* pNumOfSamplesProcessed);
+
+/* TANConvolution::Process(cl_mem in[], cl_mem out[], ...) -- TrueAudioNext.h:215-220
+ * (AMF_NOT_IMPLEMENTED in the reference, ConvolutionImpl.cpp:835-845; implemented
+ * here). Device input and output arrays; returns once the work is enqueued on
+ * the object's stream (see tanb_convolution_synchronize). */
+int32_t tanb_convolution_process_device(tanb_convolution* conv,
+                                        const float* const* ppDeviceInput,
+                                        float* const* ppDeviceOutput,
+                                        size_t numOfSamples,
+                                        const uint32_t* flagMasks,
+                                        size_t* pNumOfSamplesProcessed);
+
+/* TANConvolution::ProcessDirect(float* ir[], float* in[], float* out[], ...) --
+ * TrueAudioNext.h:223-230, ConvolutionImpl.cpp:721-762. TIME_DOMAIN method only
+ * (AMF_NOT_SUPPORTED otherwise): direct FIR with a per-call IR over a circular
+ * history of nextpow2(responseLength) samples; nzFirstLast (nullable) holds
+ * [first, last) nonzero tap bounds per channel. */
+int32_t tanb_convolution_process_direct(tanb_convolution* conv,
+                                        const float* const* ppImpulseResponse,
+                                        const float* const* ppBufferInput,
+                                        float* const* ppBufferOutput,
+                                        size_t numOfSamples,
+                                        size_t* pNumOfSamplesProcessed,
+                                        const int32_t* nzFirstLast);
+
+/* TANConvolution::ProcessFinalize -- TrueAudioNext.h:232, ConvolutionImpl.cpp:1046-1079.
+ * With TANB_METHOD_USE_PROCESS_FINALIZE, Process returns after the head
+ * (partition 0) and this call enqueues the tail for the next block. */
+int32_t tanb_convolution_process_finalize(tanb_convolution* conv);
+
+/* TANConvolution::GetNextFreeChannel -- TrueAudioNext.h:247-249,
+ * ConvolutionImpl.cpp:1084-1110. */
+int32_t tanb_convolution_get_next_free_channel(tanb_convolution* conv,
+                                               uint32_t* pChannelIndex,
+                                               const uint32_t* flagMasks);
+
+/* No reference counterpart (the reference's CPU path is synchronous): waits
+ * until all work enqueued by this object has finished. */
+int32_t tanb_convolution_synchronize(tanb_convolution* conv);
+
+/* No reference counterpart: the object's CUDA stream (a cudaStream_t), for
+ * callers that order their own device work after Process_device. */
+void* tanb_convolution_stream(tanb_convolution* conv);
+
+/* No reference counterpart: layout facts for tools and tests --
+ * out[0] = partitions P, out[1] = block B, out[2] = channels C,
+ * out[3] = device bytes held by the object. */
+int32_t tanb_convolution_info(tanb_convolution* conv, int64_t out[4]);
+
+/* No reference counterpart: text of the last error raised on this thread. */
+const char* tanb_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TANB_H */

@@ -1,0 +1,126 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes binding of the oracle's C++ restatement
+of TAN's CPU uniformly-partitioned convolution (oracle/tan_cpu_ref.cpp).
+
+Used by tests/, the smoke check and bench.py's CPU legs as the checker and the
+timed CPU baseline; never by the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libtanref.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile libtanref.so with the oracle's Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp, i32, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+        fpp = ctypes.POINTER(ctypes.c_void_p)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.tanref_create.restype = vp
+        L.tanref_create.argtypes = [i32, i32, i32, i32]
+        L.tanref_destroy.argtypes = [vp]
+        L.tanref_partitions.argtypes = [vp]
+        L.tanref_partitions.restype = i32
+        L.tanref_update_td.argtypes = [vp, fpp, sz, u32p]
+        L.tanref_update_td.restype = i32
+        L.tanref_process.argtypes = [vp, fpp, fpp, sz, u32p, ctypes.POINTER(sz)]
+        L.tanref_process.restype = i32
+        L.tanref_next_free_channel.argtypes = [vp, u32p, u32p]
+        L.tanref_next_free_channel.restype = i32
+        fp = ctypes.c_void_p
+        L.tanref_rfft.argtypes = [i32, fp, fp, fp]
+        L.tanref_irfft.argtypes = [i32, fp, fp, fp]
+        _lib = L
+    return _lib
+
+
+def _ptrs(arrs):
+    return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+def _flags(flags, C):
+    if flags is None:
+        return None
+    f = np.ascontiguousarray(np.asarray(flags, dtype=np.uint32).reshape(C))
+    return f, f.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+class RefConvolution:
+    """Mirror of TANConvolution (Init / UpdateResponseTD / Process /
+    GetNextFreeChannel) over the restatement; arrays are (channels, samples)."""
+
+    def __init__(self, length: int, block: int, channels: int, threads: int = 1):
+        self.L, self.B, self.C = length, block, channels
+        self._h = lib().tanref_create(length, block, channels, threads)
+        if not self._h:
+            raise ValueError("invalid oracle configuration")
+
+    def close(self):
+        if self._h:
+            lib().tanref_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def partitions(self) -> int:
+        return lib().tanref_partitions(self._h)
+
+    def update_response_td(self, ir: np.ndarray, flags=None) -> int:
+        ir = np.ascontiguousarray(ir, dtype=np.float32)
+        rows = [np.ascontiguousarray(ir[c]) for c in range(self.C)]
+        fl = _flags(flags, self.C)
+        return lib().tanref_update_td(self._h, _ptrs(rows), ir.shape[1], fl[1] if fl else None)
+
+    def process(self, x: np.ndarray, flags=None, out: np.ndarray | None = None):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n = x.shape[1]
+        if out is None:
+            out = np.zeros_like(x)
+        rows_in = [x[c] for c in range(self.C)]
+        rows_out = [out[c] for c in range(self.C)]
+        fl = _flags(flags, self.C)
+        done = ctypes.c_size_t(0)
+        rc = lib().tanref_process(self._h, _ptrs(rows_in), _ptrs(rows_out), n,
+                                  fl[1] if fl else None, ctypes.byref(done))
+        return rc, out, done.value
+
+    def next_free_channel(self, flags=None):
+        idx = ctypes.c_uint32(0)
+        fl = _flags(flags, self.C)
+        rc = lib().tanref_next_free_channel(self._h, ctypes.byref(idx), fl[1] if fl else None)
+        return rc, idx.value
+
+
+def rfft(x: np.ndarray):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    N = x.size
+    re = np.zeros(N // 2 + 1, np.float32)
+    im = np.zeros(N // 2 + 1, np.float32)
+    lib().tanref_rfft(N, x.ctypes.data, re.ctypes.data, im.ctypes.data)
+    return re, im
+
+
+def irfft(re: np.ndarray, im: np.ndarray):
+    re = np.ascontiguousarray(re, dtype=np.float32)
+    im = np.ascontiguousarray(im, dtype=np.float32)
+    N = 2 * (re.size - 1)
+    y = np.zeros(N, np.float32)
+    lib().tanref_irfft(N, re.ctypes.data, im.ctypes.data, y.ctypes.data)
+    return y

@@ -1,0 +1,437 @@
+// TEST INFRASTRUCTURE ONLY -- the oracle. Nothing in the product (libtanb.so,
+// the tan_b200 package) links, loads or calls this file; only tests/, the
+// smoke check and bench.py's CPU-baseline / reference legs do, as the checker.
+//
+// A CPU restatement of AMD TrueAudio Next's uniformly-partitioned FFT
+// convolution (TAN_CONVOLUTION_METHOD_FFT_PARTITIONED_UNIFORM on the CPU):
+//
+//   layout      planar real-FFT partitions of stride S = 2B + 16 floats,
+//               re plane at [0, B+8), im plane at [B+8, 2B+16)
+//               (tan/tanlibrary/src/TrueAudioNext/convolution/ConvolutionImpl.h:50,
+//                ConvolutionImpl.cpp:1548-1663)
+//   IR prep     split the time-domain IR into P = nextpow2(L)/B partitions,
+//               zero-pad each to 2B and R2C-transform it
+//               (ConvolutionImpl.cpp:2080-2141)
+//   head        newest FDL slot <- R2C([x_k, 0^B]); acc += X_k * H_0;
+//               C2R (scaled 1/N); y = acc[0..B) + overlap; overlap <- acc[B..2B)
+//               (ConvolutionImpl.cpp:2380-2535)
+//   tail        acc_next = sum_{i=1}^{P-1} FDL[(cur+i-1) mod P] * H_i
+//               (ConvolutionImpl.cpp:2539-2643)
+//   MAC         cr += fmsub(ar, br, ai*bi); ci += fmadd(ar, bi, ai*br) on
+//               8-wide planar vectors, count B+8, OpenMP over channels
+//               (tan/tanlibrary/src/TrueAudioNext/math/MathImpl.cpp:495-530)
+//   C2R scale   1/N (tan/tanlibrary/src/TrueAudioNext/fft/FFTImpl.cpp:1046-1051)
+//   crossfade   out = new*(j/F) + old*((F-j)/F), F = B
+//               (ConvolutionImpl.cpp:877, 1392-1408)
+//   flags       STOP_INPUT ring-out of nextpow2(L) samples then flush,
+//               FLUSH_STREAM, free-channel query
+//               (ConvolutionImpl.cpp:2867-2907, 1084-1110)
+//
+// Differences from the reference, all deliberate:
+//  * The FFT is our own (radix-2, twiddles computed in double and rounded to
+//    float): the reference dlopens FFTW 3.3.5, which is absent here.
+//  * IR activation is deterministic: the new IR takes effect on the first
+//    block processed after UpdateResponseTD returns (the reference hands it to
+//    a background thread, so the swap block depends on thread timing).
+//  * The swap block computes the new IR's output over the full input history
+//    (its own tail and overlap) and blends it with the old IR's output; the
+//    reference runs ProcessInternal twice with time advancing twice
+//    (ConvolutionImpl.cpp:976-990), which corrupts the delay line.
+//  * Per-channel state is indexed by channel, not by running-channel rank, and
+//    a flush also clears the precomputed tail (the reference's CPU flush
+//    dereferences an unallocated state array, ConvolutionImpl.cpp:1284-1325).
+#include <immintrin.h>
+#include <omp.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+enum : int32_t {
+  kOk = 0,
+  kInvalidArg = 4,
+  kNotSupported = 10,
+  kNotFound = 11,
+  kNotInitialized = 13,
+  kWrongState = 15,
+};
+constexpr uint32_t kStopInput = 1;
+constexpr uint32_t kFlushStream = 2;
+constexpr int kPad = 16;  // PARTITION_PAD_FFTREAL_PLANAR
+
+// Real FFT of size N = 2M through a complex FFT of size M (even/odd packing).
+// Planar spectrum: re[0..M], im[0..M] (M+1 bins).
+struct RealFFT {
+  int N = 0, M = 0, logM = 0;
+  std::vector<float> wr, wi;   // W_N^j = exp(-2 pi i j / N), j in [0, N)
+  std::vector<int> rev;        // bit reversal over M points
+  std::vector<float> zr, zi;   // scratch, per thread
+
+  void init(int n) {
+    N = n;
+    M = n / 2;
+    logM = 0;
+    while ((1 << logM) < M) ++logM;
+    wr.resize(N);
+    wi.resize(N);
+    for (int j = 0; j < N; ++j) {
+      double a = -2.0 * M_PI * (double)j / (double)N;
+      wr[j] = (float)std::cos(a);
+      wi[j] = (float)std::sin(a);
+    }
+    rev.resize(M);
+    for (int i = 0; i < M; ++i) {
+      int r = 0;
+      for (int b = 0; b < logM; ++b) r |= ((i >> b) & 1) << (logM - 1 - b);
+      rev[i] = r;
+    }
+  }
+
+  // In-place radix-2 decimation-in-time FFT of size M on (re, im) that are
+  // already in bit-reversed order. sign = -1 forward, +1 inverse (unscaled).
+  void cfft(float* re, float* im, int sign) const {
+    for (int len = 2; len <= M; len <<= 1) {
+      int half = len >> 1;
+      int tstep = (N / len);  // W_len^k = W_N^(k * N/len)
+      for (int s = 0; s < M; s += len) {
+        for (int k = 0; k < half; ++k) {
+          float c = wr[k * tstep];
+          float d = sign < 0 ? wi[k * tstep] : -wi[k * tstep];
+          int a = s + k, b = a + half;
+          float tr = re[b] * c - im[b] * d;
+          float ti = re[b] * d + im[b] * c;
+          re[b] = re[a] - tr;
+          im[b] = im[a] - ti;
+          re[a] = re[a] + tr;
+          im[a] = im[a] + ti;
+        }
+      }
+    }
+  }
+
+  // x: N reals -> re[0..M], im[0..M]
+  void forward(const float* x, float* re, float* im, float* zr_, float* zi_) const {
+    for (int n = 0; n < M; ++n) {
+      int r = rev[n];
+      zr_[r] = x[2 * n];
+      zi_[r] = x[2 * n + 1];
+    }
+    cfft(zr_, zi_, -1);
+    // X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W_N^k (Z[k] - conj Z[M-k])
+    re[0] = zr_[0] + zi_[0];
+    im[0] = 0.f;
+    re[M] = zr_[0] - zi_[0];
+    im[M] = 0.f;
+    for (int k = 1; k < M; ++k) {
+      float ar = zr_[k], ai = zi_[k];
+      float br = zr_[M - k], bi = -zi_[M - k];  // conj Z[M-k]
+      float er = 0.5f * (ar + br), ei = 0.5f * (ai + bi);
+      float dr = 0.5f * (ar - br), di = 0.5f * (ai - bi);
+      // -i * W * d
+      float wrk = wr[k], wik = wi[k];
+      float tr = wrk * dr - wik * di;
+      float ti = wrk * di + wik * dr;
+      re[k] = er + ti;
+      im[k] = ei - tr;
+    }
+  }
+
+  // re[0..M], im[0..M] -> y: N reals, scaled by 1/N
+  void inverse(const float* re, const float* im, float* y, float* zr_, float* zi_) const {
+    const float scale = 1.0f / (float)N;
+    for (int k = 0; k < M; ++k) {
+      float ar = re[k], ai = (k == 0) ? 0.f : im[k];
+      float br = re[M - k], bi = (k == 0) ? 0.f : -im[M - k];  // conj A[M-k]
+      if (k == 0) { br = re[M]; bi = 0.f; }
+      float er = ar + br, ei = ai + bi;         // 2 X_e
+      float dr = ar - br, di = ai - bi;         // 2 X_o W^k
+      // X_o = d * W_N^{-k} = d * conj(W_N^k)
+      float wrk = wr[k], wik = -wi[k];
+      float orr = dr * wrk - di * wik;
+      float oi = dr * wik + di * wrk;
+      // Z = X_e + i X_o
+      int r = rev[k];
+      zr_[r] = (er - oi) * scale;
+      zi_[r] = (ei + orr) * scale;
+    }
+    cfft(zr_, zi_, +1);
+    for (int n = 0; n < M; ++n) {
+      y[2 * n] = zr_[n];
+      y[2 * n + 1] = zi_[n];
+    }
+  }
+};
+
+// Planar complex multiply-accumulate, 8 lanes at a time, same operation order
+// as TANMathImpl::PlanarComplexMultiplyAccumulate's AVX2 branch.
+inline void planar_cmac(const float* a, const float* b, float* acc, int count, int spacing) {
+  for (int k = 0; k < count; k += 8) {
+    __m256 ar = _mm256_loadu_ps(a + k);
+    __m256 ai = _mm256_loadu_ps(a + spacing + k);
+    __m256 br = _mm256_loadu_ps(b + k);
+    __m256 bi = _mm256_loadu_ps(b + spacing + k);
+    __m256 cr = _mm256_loadu_ps(acc + k);
+    __m256 ci = _mm256_loadu_ps(acc + spacing + k);
+    cr = _mm256_add_ps(_mm256_fmsub_ps(ar, br, _mm256_mul_ps(ai, bi)), cr);
+    ci = _mm256_add_ps(_mm256_fmadd_ps(ar, bi, _mm256_mul_ps(ai, br)), ci);
+    _mm256_storeu_ps(acc + k, cr);
+    _mm256_storeu_ps(acc + spacing + k, ci);
+  }
+}
+
+struct RefConv {
+  int L = 0, B = 0, C = 0, P = 0, S = 0, N = 0, length = 0, threads = 1;
+  RealFFT fft;
+  // IR spectra: [slot 0/1][channel] -> P*S floats
+  std::vector<float> H[2];
+  std::vector<int> active;       // per channel: active slot
+  std::vector<uint8_t> pending;  // per channel: new IR waiting in 1-active
+  std::vector<float> fdl;        // [channel] -> P*S floats (frequency-domain delay line)
+  std::vector<float> overlap;    // [channel] -> B
+  std::vector<float> tail;       // [channel] -> S (precomputed tail for the next block)
+  std::vector<float> work;       // per thread scratch: several S-sized buffers
+  int cur = 0;                   // newest FDL slot
+  // channel-flag state
+  std::vector<int> tailLeft;
+  std::vector<uint8_t> available, flushed;
+
+  float* h(int slot, int c) { return H[slot].data() + (size_t)c * P * S; }
+  float* fdlc(int c) { return fdl.data() + (size_t)c * P * S; }
+
+  void flush(int c) {
+    std::memset(fdlc(c), 0, sizeof(float) * (size_t)P * S);
+    std::memset(overlap.data() + (size_t)c * B, 0, sizeof(float) * B);
+    std::memset(tail.data() + (size_t)c * S, 0, sizeof(float) * S);
+  }
+
+  // sum_{i=i0}^{P-1} FDL[(base + i) mod P] * Hslot_i  into acc (S floats, zeroed first)
+  void fdl_mac(int c, const float* hs, int base, int i0, float* acc) {
+    std::memset(acc, 0, sizeof(float) * S);
+    for (int i = i0; i < P; ++i) {
+      int slot = ((base + i) % P + P) % P;
+      planar_cmac(fdlc(c) + (size_t)slot * S, hs + (size_t)i * S, acc, B + 8, B + 8);
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void* tanref_create(int L, int B, int C, int threads) {
+  if (L <= 0 || B <= 0 || C <= 0 || (B & (B - 1)) != 0 || B < 8) return nullptr;
+  RefConv* r = new RefConv();
+  r->L = L;
+  r->B = B;
+  r->C = C;
+  r->threads = threads > 0 ? threads : 1;
+  int len = 1;
+  while (len < L) len <<= 1;
+  r->length = len;
+  r->P = len / B;
+  if (r->P < 1) r->P = 1;
+  r->S = 2 * B + kPad;
+  r->N = 2 * B;
+  r->fft.init(r->N);
+  size_t per = (size_t)r->P * r->S;
+  r->H[0].assign(per * C, 0.f);
+  r->H[1].assign(per * C, 0.f);
+  r->active.assign(C, 0);
+  r->pending.assign(C, 0);
+  r->fdl.assign(per * C, 0.f);
+  r->overlap.assign((size_t)B * C, 0.f);
+  r->tail.assign((size_t)r->S * C, 0.f);
+  r->work.assign((size_t)r->threads * 8 * r->S, 0.f);
+  r->cur = 0;
+  r->tailLeft.assign(C, 0);
+  r->available.assign(C, 0);
+  r->flushed.assign(C, 0);
+  return r;
+}
+
+void tanref_destroy(void* h) { delete static_cast<RefConv*>(h); }
+
+int tanref_partitions(void* h) { return static_cast<RefConv*>(h)->P; }
+
+// UpdateResponseTD (ConvolutionImpl.cpp:407-557 + the update thread's
+// partition/transform, :2080-2141), done synchronously.
+int tanref_update_td(void* hh, const float* const* ir, size_t n, const uint32_t* flags) {
+  RefConv* r = static_cast<RefConv*>(hh);
+  if (!ir) return kInvalidArg;
+  if (n > (size_t)r->L) return kInvalidArg;
+  for (int c = 0; c < r->C; ++c)
+    if (flags && (flags[c] & kFlushStream)) r->flush(c);
+  std::vector<float> td((size_t)r->P * r->B + r->B, 0.f);
+  for (int c = 0; c < r->C; ++c) {
+    if (flags && (flags[c] & kStopInput)) continue;
+    int slot = 1 - r->active[c];
+    float* hs = r->h(slot, c);
+    std::fill(td.begin(), td.end(), 0.f);
+    std::memcpy(td.data(), ir[c], sizeof(float) * n);
+    std::vector<float> frame(r->N), zr(r->B), zi(r->B);
+    for (int i = 0; i < r->P; ++i) {
+      std::fill(frame.begin(), frame.end(), 0.f);
+      std::memcpy(frame.data(), td.data() + (size_t)i * r->B, sizeof(float) * r->B);
+      float* part = hs + (size_t)i * r->S;
+      std::memset(part, 0, sizeof(float) * r->S);
+      r->fft.forward(frame.data(), part, part + r->B + 8, zr.data(), zi.data());
+    }
+    r->pending[c] = 1;
+  }
+  return kOk;
+}
+
+// Process(float**, float**, ...) for FFT_PARTITIONED_UNIFORM on the CPU:
+// state machine (ConvolutionImpl.cpp:848-1043), ProcessInternal's channel
+// flags (:2839-2931), head (:2380-2535) and tail (:2539-2643).
+int tanref_process(void* hh, const float* const* in, float* const* out, size_t n,
+                   const uint32_t* flags, size_t* done) {
+  RefConv* r = static_cast<RefConv*>(hh);
+  if (!in || !out) return kInvalidArg;
+  if (done) *done = 0;
+  const int B = r->B, S = r->S, P = r->P, C = r->C;
+  size_t nblocks = n / (size_t)B;
+  for (size_t blk = 0; blk < nblocks; ++blk) {
+    // channel flags
+    std::vector<uint8_t> run(C, 0);
+    int nrun = 0;
+    for (int c = 0; c < C; ++c) {
+      uint32_t f = flags ? flags[c] : 0u;
+      if (!flags) {
+        r->available[c] = 0;
+        r->tailLeft[c] = r->length;
+      } else if (f & kStopInput) {
+        if (f & kFlushStream) {
+          r->available[c] = 1;
+          r->tailLeft[c] = 0;
+        } else if (r->tailLeft[c] > 0) {
+          r->available[c] = 0;
+          r->tailLeft[c] -= B;
+          if (r->tailLeft[c] <= 0) r->flush(c);
+        } else {
+          r->available[c] = 1;
+          r->tailLeft[c] = 0;
+        }
+      } else {
+        r->available[c] = 0;
+        r->tailLeft[c] = r->length;
+      }
+      if (flags && (f & kFlushStream)) {
+        if (!r->flushed[c]) r->flush(c);
+        r->flushed[c] = 1;
+      } else {
+        r->flushed[c] = 0;
+      }
+      run[c] = !r->available[c];
+      nrun += run[c];
+    }
+    if (nrun == 0) return kWrongState;
+
+    const int prev = r->cur;               // newest slot before this block
+    const int cur = (prev - 1 + P) % P;    // slot for this block's spectrum
+    r->cur = cur;
+
+#pragma omp parallel for num_threads(r->threads) schedule(static)
+    for (int c = 0; c < C; ++c) {
+      if (!run[c]) continue;
+      int t = omp_get_thread_num();
+      float* w = r->work.data() + (size_t)t * 8 * S;
+      float* accA = w;            // old / only IR accumulator
+      float* accB = w + S;        // new IR accumulator (swap block)
+      float* ovlN = w + 2 * S;    // new IR overlap (swap block)
+      float* tA = w + 3 * S;      // time-domain scratch (2B)
+      float* tB = w + 4 * S;
+      float* zr = w + 5 * S;
+      float* zi = w + 6 * S;
+      const float* x = in[c] + blk * B;
+      float* y = out[c] + blk * B;
+      const bool swap = r->pending[c] != 0;
+      const float* hOld = r->h(r->active[c], c);
+      const float* hNew = r->h(1 - r->active[c], c);
+
+      if (swap) {
+        // New IR's overlap: upper half of C2R(sum_{i=0}^{P-1} X_{k-1-i} H'_i),
+        // and new IR's tail for this block, both from the delay line before
+        // this block's spectrum is inserted.
+        r->fdl_mac(c, hNew, prev, 0, accB);
+        r->fft.inverse(accB, accB + B + 8, tB, zr, zi);
+        std::memcpy(ovlN, tB + B, sizeof(float) * B);
+        r->fdl_mac(c, hNew, prev - 1, 1, accB);
+      }
+
+      // newest slot <- R2C([x_k, 0^B])
+      float* part = r->fdlc(c) + (size_t)cur * S;
+      std::memset(tA, 0, sizeof(float) * 2 * B);
+      std::memcpy(tA, x, sizeof(float) * B);
+      std::memset(part, 0, sizeof(float) * S);
+      r->fft.forward(tA, part, part + B + 8, zr, zi);
+
+      // head: acc = tail + X_k * H_0
+      std::memcpy(accA, r->tail.data() + (size_t)c * S, sizeof(float) * S);
+      planar_cmac(part, hOld, accA, B + 8, B + 8);
+      r->fft.inverse(accA, accA + B + 8, tA, zr, zi);
+      float* ovl = r->overlap.data() + (size_t)c * B;
+      if (!swap) {
+        for (int i = 0; i < B; ++i) y[i] = tA[i] + ovl[i];
+        std::memcpy(ovl, tA + B, sizeof(float) * B);
+      } else {
+        planar_cmac(part, hNew, accB, B + 8, B + 8);
+        r->fft.inverse(accB, accB + B + 8, tB, zr, zi);
+        const float step = 1.0f / (float)B;
+        for (int i = 0; i < B; ++i) {
+          float yo = tA[i] + ovl[i];
+          float yn = tB[i] + ovlN[i];
+          float w1 = step * (float)i;
+          float w2 = step * (float)(B - i);
+          y[i] = yn * w1 + yo * w2;
+        }
+        std::memcpy(ovl, tB + B, sizeof(float) * B);
+        r->active[c] = 1 - r->active[c];
+        r->pending[c] = 0;
+      }
+      // tail for the next block: sum_{i=1}^{P-1} FDL[(cur+i-1) mod P] * H_i
+      r->fdl_mac(c, r->h(r->active[c], c), cur - 1, 1, r->tail.data() + (size_t)c * S);
+    }
+    if (done) *done += B;
+  }
+  return kOk;
+}
+
+// GetNextFreeChannel (ConvolutionImpl.cpp:1084-1110)
+int tanref_next_free_channel(void* hh, uint32_t* idx, const uint32_t* flags) {
+  RefConv* r = static_cast<RefConv*>(hh);
+  if (!idx) return kInvalidArg;
+  *idx = 0xFFFFFFFFu;
+  if (!flags) return kNotFound;
+  for (int c = 0; c < r->C; ++c) {
+    if ((flags[c] & kStopInput) && r->tailLeft[c] <= 0) {
+      *idx = (uint32_t)c;
+      return kOk;
+    }
+  }
+  return kNotFound;
+}
+
+// Plain forward/inverse real FFT, exposed for the oracle's own tests.
+int tanref_rfft(int N, const float* x, float* re, float* im) {
+  RealFFT f;
+  f.init(N);
+  std::vector<float> zr(N / 2), zi(N / 2);
+  f.forward(x, re, im, zr.data(), zi.data());
+  return kOk;
+}
+
+int tanref_irfft(int N, const float* re, const float* im, float* y) {
+  RealFFT f;
+  f.init(N);
+  std::vector<float> zr(N / 2), zi(N / 2);
+  f.inverse(re, im, y, zr.data(), zi.data());
+  return kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,291 @@
+"""Python mirror of amf::TANConvolution over the C ABI in libtanb.so.
+
+Method names, argument meaning and AMF_RESULT return codes follow
+tan/tanlibrary/include/TrueAudioNext.h:125-253; sample buffers are numpy arrays
+shaped (channels, samples) (or any sequence of per-channel 1-D float32 arrays)
+for the host overloads and CUDA tensors (anything with .data_ptr()) for the
+device overloads. Every call goes to the CUDA path; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtanb.so")
+
+# AMF_RESULT (amf/public/include/core/Result.h:43-125)
+AMF_OK = 0
+AMF_FAIL = 1
+AMF_UNEXPECTED = 2
+AMF_INVALID_ARG = 4
+AMF_OUT_OF_MEMORY = 6
+AMF_INVALID_POINTER = 7
+AMF_NOT_IMPLEMENTED = 9
+AMF_NOT_SUPPORTED = 10
+AMF_NOT_FOUND = 11
+AMF_ALREADY_INITIALIZED = 12
+AMF_NOT_INITIALIZED = 13
+AMF_WRONG_STATE = 15
+AMF_NO_DEVICE = 17
+AMF_TAN_UNSUPPORTED_VERSION = 43
+
+# TAN_CONVOLUTION_METHOD (TrueAudioNext.h:81-99)
+TAN_CONVOLUTION_METHOD_FFT_OVERLAP_ADD = 0
+TAN_CONVOLUTION_METHOD_FFT_PARTITIONED_UNIFORM = 1
+TAN_CONVOLUTION_METHOD_FFT_PARTITIONED_NONUNIFORM = 2
+TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED = 3
+TAN_CONVOLUTION_METHOD_FHT_UNIFORM_PARTITIONED = 4
+TAN_CONVOLUTION_METHOD_FFT_UNIFORM_HEAD_TAIL = 5
+TAN_CONVOLUTION_METHOD_FHT_UNIFORM_HEAD_TAIL = 6
+TAN_CONVOLUTION_METHOD_TIME_DOMAIN = 7
+TAN_CONVOLUTION_METHOD_FHT_NONUNIFORM_PARTITIONED = 8
+TAN_CONVOLUTION_METHOD_FFT_NONUNIFORM_PARTITIONED = 9
+TAN_CONVOLUTION_METHOD_USE_PROCESS_FINALIZE = 0x8000
+TAN_CONVOLUTION_METHOD_USE_PROCESS_TAILTHREAD = 0xC000
+
+# TAN_CONVOLUTION_CHANNEL_FLAG (TrueAudioNext.h:105-110)
+TAN_CONVOLUTION_CHANNEL_FLAG_PROCESS = 0
+TAN_CONVOLUTION_CHANNEL_FLAG_STOP_INPUT = 0x01
+TAN_CONVOLUTION_CHANNEL_FLAG_FLUSH_STREAM = 0x02
+
+# TAN_CONVOLUTION_OPERATION_FLAG (TrueAudioNext.h:116-120)
+TAN_CONVOLUTION_OPERATION_FLAG_NONE = 0x00
+TAN_CONVOLUTION_OPERATION_FLAG_BLOCK_UNTIL_READY = 0x01
+
+TAN_FULL_VERSION = (1 << 48) | (3 << 32) | (1 << 16) | 1
+
+# Every symbol include/tanb.h declares, with its ctypes signature.
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_u32 = ctypes.c_uint32
+_sz = ctypes.c_size_t
+_pp = ctypes.POINTER(ctypes.c_void_p)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_szp = ctypes.POINTER(ctypes.c_size_t)
+SIGNATURES = {
+    "tanb_create_context": (_i32, [ctypes.c_uint64, _i32, ctypes.POINTER(_vp)]),
+    "tanb_context_release": (_i32, [_vp]),
+    "tanb_create_convolution": (_i32, [_vp, ctypes.POINTER(_vp)]),
+    "tanb_convolution_release": (_i32, [_vp]),
+    "tanb_convolution_init": (_i32, [_vp, _u32, _u32, _u32, _u32]),
+    "tanb_convolution_terminate": (_i32, [_vp]),
+    "tanb_convolution_update_response_td": (_i32, [_vp, _pp, _sz, _u32p, _u32]),
+    "tanb_convolution_update_response_td_device": (_i32, [_vp, _pp, _sz, _u32p, _u32]),
+    "tanb_convolution_update_response_fd": (_i32, [_vp, _pp, _sz, _u32p, _u32]),
+    "tanb_convolution_process": (_i32, [_vp, _pp, _pp, _sz, _u32p, _szp]),
+    "tanb_convolution_process_host_to_device": (_i32, [_vp, _pp, _pp, _sz, _u32p, _szp]),
+    "tanb_convolution_process_device": (_i32, [_vp, _pp, _pp, _sz, _u32p, _szp]),
+    "tanb_convolution_process_direct": (_i32, [_vp, _pp, _pp, _pp, _sz, _szp, ctypes.POINTER(ctypes.c_int32)]),
+    "tanb_convolution_process_finalize": (_i32, [_vp]),
+    "tanb_convolution_get_next_free_channel": (_i32, [_vp, _u32p, _u32p]),
+    "tanb_convolution_synchronize": (_i32, [_vp]),
+    "tanb_convolution_stream": (_vp, [_vp]),
+    "tanb_convolution_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "tanb_last_error": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libtanb.so; raises if it was not built (there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m tan_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().tanb_last_error().decode()
+
+
+class TANError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        super().__init__(f"{where} failed with AMF_RESULT {code}: {last_error()}")
+        self.code = code
+
+
+def _rows_host(buf, channels: int):
+    """Per-channel float32 row pointers of a host buffer; returns (keepalive, ptr array)."""
+    if isinstance(buf, np.ndarray) and buf.ndim == 2:
+        if buf.dtype != np.float32 or not buf.flags.c_contiguous:
+            raise TypeError("host buffers must be C-contiguous float32 (channels, samples)")
+        rows = [buf[c] for c in range(buf.shape[0])]
+    else:
+        rows = list(buf)
+        for r in rows:
+            if r is not None and (not isinstance(r, np.ndarray) or r.dtype != np.float32 or not r.flags.c_contiguous):
+                raise TypeError("host rows must be C-contiguous float32 arrays")
+    if len(rows) != channels:
+        raise ValueError(f"expected {channels} channel rows, got {len(rows)}")
+    arr = (ctypes.c_void_p * channels)(*[(r.ctypes.data if r is not None else None) for r in rows])
+    return rows, arr
+
+
+def _rows_device(buf, channels: int):
+    """Per-channel row pointers of a device buffer (tensor with .data_ptr() and rows)."""
+    if hasattr(buf, "data_ptr") and getattr(buf, "dim", lambda: 0)() == 2:
+        if not buf.is_contiguous():
+            raise TypeError("device buffers must be contiguous")
+        stride = buf.stride(0) * buf.element_size()
+        base = buf.data_ptr()
+        ptrs = [base + c * stride for c in range(buf.shape[0])]
+    else:
+        ptrs = [(r.data_ptr() if hasattr(r, "data_ptr") else r) for r in buf]
+    if len(ptrs) != channels:
+        raise ValueError(f"expected {channels} channel rows, got {len(ptrs)}")
+    return buf, (ctypes.c_void_p * channels)(*ptrs)
+
+
+def _flags(flags, channels: int):
+    if flags is None:
+        return None, None
+    f = np.ascontiguousarray(np.asarray(flags, dtype=np.uint32))
+    if f.size != channels:
+        raise ValueError("one flag mask per channel")
+    return f, f.ctypes.data_as(_u32p)
+
+
+class TANContext:
+    """TANCreateContext (TrueAudioNext.h:647): a context bound to one CUDA device."""
+
+    def __init__(self, device: int = 0, version: int = TAN_FULL_VERSION):
+        h = ctypes.c_void_p()
+        rc = lib().tanb_create_context(version, device, ctypes.byref(h))
+        if rc != AMF_OK:
+            raise TANError(rc, "TANCreateContext")
+        self._h = h
+        self.device = device
+
+    def Release(self):
+        if self._h:
+            lib().tanb_context_release(self._h)
+            self._h = None
+
+
+class TANConvolution:
+    """TANCreateConvolution + the TANConvolution interface (TrueAudioNext.h:125-253)."""
+
+    def __init__(self, context: TANContext):
+        h = ctypes.c_void_p()
+        rc = lib().tanb_create_convolution(context._h, ctypes.byref(h))
+        if rc != AMF_OK:
+            raise TANError(rc, "TANCreateConvolution")
+        self._ctx = context
+        self._h = h
+        self.channels = 0
+        self.block = 0
+
+    # -- lifetime -----------------------------------------------------------
+    def Init(self, method: int, responseLengthInSamples: int, bufferSizeInSamples: int, channels: int) -> int:
+        rc = lib().tanb_convolution_init(self._h, method, responseLengthInSamples, bufferSizeInSamples, channels)
+        if rc == AMF_OK:
+            self.channels, self.block = channels, bufferSizeInSamples
+        return rc
+
+    InitGpu = Init
+    InitCpu = Init
+
+    def Terminate(self) -> int:
+        return lib().tanb_convolution_terminate(self._h)
+
+    def Release(self):
+        if self._h:
+            lib().tanb_convolution_release(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.Release()
+        except Exception:
+            pass
+
+    # -- IR updates ---------------------------------------------------------
+    def UpdateResponseTD(self, ppBuffer, numOfSamplesToProcess: int, flagMasks=None, operationFlags: int = 0) -> int:
+        keep, rows = _rows_host(ppBuffer, self.channels)
+        fk, fp = _flags(flagMasks, self.channels)
+        return lib().tanb_convolution_update_response_td(self._h, rows, numOfSamplesToProcess, fp, operationFlags)
+
+    def UpdateResponseTDDevice(self, ppBuffer, numOfSamplesToProcess: int, flagMasks=None,
+                               operationFlags: int = 0) -> int:
+        keep, rows = _rows_device(ppBuffer, self.channels)
+        fk, fp = _flags(flagMasks, self.channels)
+        return lib().tanb_convolution_update_response_td_device(self._h, rows, numOfSamplesToProcess, fp,
+                                                                operationFlags)
+
+    def UpdateResponseFD(self, ppBuffer, numOfSamplesToProcess: int, flagMasks=None, operationFlags: int = 0) -> int:
+        rows = (ctypes.c_void_p * max(1, self.channels))()
+        return lib().tanb_convolution_update_response_fd(self._h, rows, numOfSamplesToProcess, None, operationFlags)
+
+    # -- processing ---------------------------------------------------------
+    def Process(self, ppBufferInput, ppBufferOutput, numOfSamplesToProcess: int, flagMasks=None):
+        """Host buffers. Returns (AMF_RESULT, samples processed)."""
+        ki, rin = _rows_host(ppBufferInput, self.channels)
+        ko, rout = _rows_host(ppBufferOutput, self.channels)
+        fk, fp = _flags(flagMasks, self.channels)
+        done = ctypes.c_size_t(0)
+        rc = lib().tanb_convolution_process(self._h, rin, rout, numOfSamplesToProcess, fp, ctypes.byref(done))
+        return rc, done.value
+
+    def ProcessHostToDevice(self, ppBufferInput, ppDeviceOutput, numOfSamplesToProcess: int, flagMasks=None):
+        ki, rin = _rows_host(ppBufferInput, self.channels)
+        ko, rout = _rows_device(ppDeviceOutput, self.channels)
+        fk, fp = _flags(flagMasks, self.channels)
+        done = ctypes.c_size_t(0)
+        rc = lib().tanb_convolution_process_host_to_device(self._h, rin, rout, numOfSamplesToProcess, fp,
+                                                           ctypes.byref(done))
+        return rc, done.value
+
+    def ProcessDevice(self, ppDeviceInput, ppDeviceOutput, numOfSamplesToProcess: int, flagMasks=None):
+        """Device buffers; asynchronous on the object's stream (see Synchronize)."""
+        ki, rin = _rows_device(ppDeviceInput, self.channels)
+        ko, rout = _rows_device(ppDeviceOutput, self.channels)
+        fk, fp = _flags(flagMasks, self.channels)
+        done = ctypes.c_size_t(0)
+        rc = lib().tanb_convolution_process_device(self._h, rin, rout, numOfSamplesToProcess, fp, ctypes.byref(done))
+        return rc, done.value
+
+    def ProcessDirect(self, ppImpulseResponse, ppBufferInput, ppBufferOutput, numOfSamplesToProcess: int,
+                      nzFirstLast=None):
+        kr, rir = _rows_host(ppImpulseResponse, self.channels)
+        ki, rin = _rows_host(ppBufferInput, self.channels)
+        ko, rout = _rows_host(ppBufferOutput, self.channels)
+        nz = None
+        if nzFirstLast is not None:
+            nzk = np.ascontiguousarray(np.asarray(nzFirstLast, dtype=np.int32))
+            nz = nzk.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        done = ctypes.c_size_t(0)
+        rc = lib().tanb_convolution_process_direct(self._h, rir, rin, rout, numOfSamplesToProcess,
+                                                   ctypes.byref(done), nz)
+        return rc, done.value
+
+    def ProcessFinalize(self) -> int:
+        return lib().tanb_convolution_process_finalize(self._h)
+
+    def GetNextFreeChannel(self, flagMasks=None):
+        idx = ctypes.c_uint32(0)
+        fk, fp = _flags(flagMasks, self.channels)
+        rc = lib().tanb_convolution_get_next_free_channel(self._h, ctypes.byref(idx), fp)
+        return rc, idx.value
+
+    # -- extras (no reference counterpart) ---------------------------------
+    def Synchronize(self) -> int:
+        return lib().tanb_convolution_synchronize(self._h)
+
+    def stream(self) -> int:
+        return lib().tanb_convolution_stream(self._h) or 0
+
+    def info(self) -> dict:
+        out = (ctypes.c_int64 * 4)()
+        lib().tanb_convolution_info(self._h, out)
+        return {"partitions": out[0], "block": out[1], "channels": out[2], "device_bytes": out[3]}

@@ -1,0 +1,623 @@
+// Host engine behind include/tanb.h: the TANConvolution state machine of the
+// reference (tan/tanlibrary/src/TrueAudioNext/convolution/ConvolutionImpl.cpp)
+// driving the sm_100a kernels of tanb_kernels.cu on one CUDA stream per object.
+//
+// Per Process call the host
+//   1. runs the channel-flag bookkeeping per block (ConvolutionImpl.cpp:2867-2907),
+//   2. writes one descriptor per block (per-channel run / swap / IR slots and
+//      the input and output row pointers) and the input samples into pinned
+//      staging, copied to the device in one transfer,
+//   3. enqueues head + tail kernels per block, the output copy before the last
+//      tail, and waits only for the output copy.
+// UpdateResponseTD transforms the new IR into the idle slot and precomputes
+// that IR's tail, so the swap block costs the same device time as any other.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tanb.h"
+#include "tanb_internal.h"
+
+using tanb::ChanCtl;
+using tanb::DevState;
+using tanb::MacTiling;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int32_t fail(int32_t code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define TANB_CUDA(expr)                                                                   \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(e_ == cudaErrorMemoryAllocation ? TANB_OUT_OF_MEMORY : TANB_FAIL,       \
+                  "%s failed: %s", #expr, cudaGetErrorString(e_));                       \
+  } while (0)
+
+constexpr int kMaxBlocksPerChunk = 8;
+constexpr uint32_t kStopInput = TANB_CHANNEL_FLAG_STOP_INPUT;
+constexpr uint32_t kFlush = TANB_CHANNEL_FLAG_FLUSH_STREAM;
+
+enum class Mem { Host, Device };
+
+}  // namespace
+
+struct tanb_context {
+  int device = 0;
+};
+
+struct tanb_convolution {
+  tanb_context* ctx = nullptr;
+  std::mutex mu;
+  bool initialized = false;
+  bool terminated = false;
+  bool finalize_mode = false;
+  bool finalize_due = false;
+  uint32_t method = 0;
+  int L = 0, B = 0, C = 0, P = 0, length = 0;
+  cudaStream_t stream = nullptr;
+  DevState ds{};
+  float2* d_tw = nullptr;
+  MacTiling tiling{32, 8};
+  size_t dev_bytes = 0;
+
+  // host mirror of the per-channel state
+  std::vector<int> active, pending, slot_new, tail_left;
+  std::vector<uint8_t> available, flushed;
+  int cur = 0;  // delay-line slot of the newest spectrum
+
+  // Process staging: [kMaxBlocksPerChunk] descriptors, then inputs
+  size_t desc_bytes = 0;
+  uint8_t* h_stage = nullptr;
+  uint8_t* d_stage = nullptr;
+  float* h_out = nullptr;
+  float* d_out = nullptr;
+  const ChanCtl* last_desc = nullptr;  // device descriptor of the last head (for ProcessFinalize)
+  int last_cur = 0;
+
+  // UpdateResponseTD staging: IR rows [C][P*B], then ChanCtl[C] + int[C]
+  float* h_ir = nullptr;
+  float* d_ir = nullptr;
+  uint8_t* h_uctl = nullptr;
+  uint8_t* d_uctl = nullptr;
+
+  cudaEvent_t ev_stage = nullptr, ev_ir = nullptr, ev_out = nullptr;
+
+  // descriptor accessors
+  ChanCtl* desc_ctl(uint8_t* base, int b) { return reinterpret_cast<ChanCtl*>(base + b * desc_bytes); }
+  const float** desc_in(uint8_t* base, int b) {
+    return reinterpret_cast<const float**>(base + b * desc_bytes + sizeof(ChanCtl) * C);
+  }
+  float** desc_out(uint8_t* base, int b) {
+    return reinterpret_cast<float**>(base + b * desc_bytes + (sizeof(ChanCtl) + sizeof(void*)) * C);
+  }
+  float* stage_in(uint8_t* base, int b, int c) {
+    return reinterpret_cast<float*>(base + kMaxBlocksPerChunk * desc_bytes) + ((size_t)b * C + c) * B;
+  }
+};
+
+namespace {
+
+void free_all(tanb_convolution* v) {
+  if (v->stream) cudaStreamSynchronize(v->stream);
+  cudaFree(v->ds.H);
+  cudaFree(v->ds.fdl);
+  cudaFree(v->ds.prev);
+  cudaFree(v->ds.tail);
+  cudaFree(v->d_tw);
+  cudaFree(v->d_stage);
+  cudaFree(v->d_out);
+  cudaFree(v->d_ir);
+  cudaFree(v->d_uctl);
+  cudaFreeHost(v->h_stage);
+  cudaFreeHost(v->h_out);
+  cudaFreeHost(v->h_ir);
+  cudaFreeHost(v->h_uctl);
+  if (v->ev_stage) cudaEventDestroy(v->ev_stage);
+  if (v->ev_ir) cudaEventDestroy(v->ev_ir);
+  if (v->ev_out) cudaEventDestroy(v->ev_out);
+  if (v->stream) cudaStreamDestroy(v->stream);
+  v->ds = DevState{};
+  v->d_tw = nullptr;
+  v->d_stage = v->h_stage = nullptr;
+  v->d_out = v->h_out = nullptr;
+  v->d_ir = v->h_ir = nullptr;
+  v->d_uctl = v->h_uctl = nullptr;
+  v->ev_stage = v->ev_ir = v->ev_out = nullptr;
+  v->stream = nullptr;
+  v->last_desc = nullptr;
+  v->dev_bytes = 0;
+}
+
+template <typename T>
+cudaError_t dev_alloc(tanb_convolution* v, T** p, size_t count) {
+  size_t bytes = count * sizeof(T);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), bytes);
+  if (e == cudaSuccess) {
+    v->dev_bytes += bytes;
+    e = cudaMemsetAsync(*p, 0, bytes, v->stream);
+  }
+  return e;
+}
+
+MacTiling default_tiling(int B, int P) {
+  const int U = B / 2;
+  if (P >= 256 && U >= 32) return {32, 16};
+  if (U >= 32) return {32, 8};
+  return {16, 16};
+}
+
+// Zeroes one channel's delay line, history and tails (intended flush semantics;
+// the reference's CPU flush is ConvolutionImpl.cpp:1261-1351).
+cudaError_t flush_channel(tanb_convolution* v, int c) {
+  cudaError_t e;
+  const size_t B = v->B, P = v->P;
+  if ((e = cudaMemsetAsync(v->ds.fdl + (size_t)c * P * B, 0, P * B * sizeof(float2), v->stream)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemsetAsync(v->ds.prev + (size_t)c * B, 0, B * sizeof(float), v->stream)) != cudaSuccess) return e;
+  return cudaMemsetAsync(v->ds.tail + (size_t)c * 2 * B, 0, 2 * B * sizeof(float2), v->stream);
+}
+
+int32_t run_pending_finalize(tanb_convolution* v) {
+  if (!v->finalize_due) return TANB_OK;
+  v->finalize_due = false;
+  TANB_CUDA(tanb::launch_tail(v->ds, v->last_desc, 0, v->last_cur, v->tiling, v->stream));
+  return TANB_OK;
+}
+
+int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags,
+                      uint32_t op) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "UpdateResponseTD before Init");
+  if (!ir) return fail(TANB_INVALID_ARG, "ppBuffer == NULL");
+  if (n > (size_t)v->L) return fail(TANB_INVALID_ARG, "IR length %zu exceeds Init length %d", n, v->L);
+  TANB_CUDA(cudaSetDevice(v->ctx->device));
+  if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
+
+  const int C = v->C, PB = v->P * v->B;
+  std::vector<int> chans;
+  for (int c = 0; c < C; ++c) {
+    if (flags && (flags[c] & kFlush)) TANB_CUDA(flush_channel(v, c));
+    if (flags && (flags[c] & kStopInput)) continue;
+    if (!ir[c] && n > 0) return fail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", c);
+    chans.push_back(c);
+  }
+  if (chans.empty()) return TANB_OK;
+
+  TANB_CUDA(cudaEventSynchronize(v->ev_ir));
+  const int nch = (int)chans.size();
+  if (mem == Mem::Host) {
+    for (int j = 0; j < nch; ++j) {
+      float* row = v->h_ir + (size_t)j * PB;
+      if (n) std::memcpy(row, ir[chans[j]], n * sizeof(float));
+      std::memset(row + n, 0, (PB - n) * sizeof(float));
+    }
+    TANB_CUDA(cudaMemcpyAsync(v->d_ir, v->h_ir, (size_t)nch * PB * sizeof(float), cudaMemcpyHostToDevice,
+                              v->stream));
+  } else {
+    for (int j = 0; j < nch; ++j) {
+      float* row = v->d_ir + (size_t)j * PB;
+      if (n)
+        TANB_CUDA(cudaMemcpyAsync(row, ir[chans[j]], n * sizeof(float), cudaMemcpyDeviceToDevice, v->stream));
+      TANB_CUDA(cudaMemsetAsync(row + n, 0, (PB - n) * sizeof(float), v->stream));
+    }
+  }
+  for (int c : chans) {
+    if (!v->pending[c]) {
+      v->slot_new[c] = 1 - v->active[c];
+      v->pending[c] = 1;
+    }
+  }
+  ChanCtl* uctl = reinterpret_cast<ChanCtl*>(v->h_uctl);
+  int* uch = reinterpret_cast<int*>(v->h_uctl + sizeof(ChanCtl) * C);
+  for (int c = 0; c < C; ++c) uctl[c] = ChanCtl{v->pending[c], v->pending[c], v->active[c], v->slot_new[c]};
+  for (int j = 0; j < nch; ++j) uch[j] = chans[j];
+  TANB_CUDA(cudaMemcpyAsync(v->d_uctl, v->h_uctl, (sizeof(ChanCtl) + sizeof(int)) * C, cudaMemcpyHostToDevice,
+                            v->stream));
+  TANB_CUDA(cudaEventRecord(v->ev_ir, v->stream));
+  const ChanCtl* d_uctl = reinterpret_cast<const ChanCtl*>(v->d_uctl);
+  const int* d_uch = reinterpret_cast<const int*>(v->d_uctl + sizeof(ChanCtl) * C);
+  TANB_CUDA(tanb::launch_ir_spectrum(v->ds, v->d_ir, d_uch, nch, d_uctl, v->stream));
+  // tail of the pending IR for the next block, from the current delay line
+  TANB_CUDA(tanb::launch_tail(v->ds, d_uctl, 1, v->cur, v->tiling, v->stream));
+  if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) TANB_CUDA(cudaStreamSynchronize(v->stream));
+  return TANB_OK;
+}
+
+// Per-block channel-flag bookkeeping, ConvolutionImpl.cpp:2867-2907 with
+// per-channel state. Returns the number of running channels; fills run[] and
+// flush[] (channels whose state is cleared before this block).
+int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_t>& run,
+                  std::vector<uint8_t>& flush) {
+  int nrun = 0;
+  for (int c = 0; c < v->C; ++c) {
+    flush[c] = 0;
+    const uint32_t f = flags ? flags[c] : 0u;
+    if (!flags) {
+      v->available[c] = 0;
+      v->tail_left[c] = v->length;
+    } else if (f & kStopInput) {
+      if (f & kFlush) {
+        v->available[c] = 1;
+        v->tail_left[c] = 0;
+      } else if (v->tail_left[c] > 0) {
+        v->available[c] = 0;
+        v->tail_left[c] -= v->B;
+        if (v->tail_left[c] <= 0) flush[c] = 1;
+      } else {
+        v->available[c] = 1;
+        v->tail_left[c] = 0;
+      }
+    } else {
+      v->available[c] = 0;
+      v->tail_left[c] = v->length;
+    }
+    if (flags && (f & kFlush)) {
+      if (!v->flushed[c]) flush[c] = 1;
+      v->flushed[c] = 1;
+    } else {
+      v->flushed[c] = 0;
+    }
+    run[c] = !v->available[c];
+    nrun += run[c];
+  }
+  return nrun;
+}
+
+int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
+                       size_t n, const uint32_t* flags, size_t* done) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (done) *done = 0;
+  if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "Process before Init");
+  if (!in) return fail(TANB_INVALID_ARG, "ppBufferInput == NULL");
+  if (!out) return fail(TANB_INVALID_ARG, "ppBufferOutput == NULL");
+  TANB_CUDA(cudaSetDevice(v->ctx->device));
+  if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
+
+  const int B = v->B, C = v->C, P = v->P;
+  size_t nblocks = n / (size_t)B;
+  size_t processed = 0;
+  int32_t status = TANB_OK;
+  std::vector<uint8_t> run(C), flush(C);
+  std::vector<std::vector<uint8_t>> run_b(kMaxBlocksPerChunk, std::vector<uint8_t>(C));
+  std::vector<std::vector<int>> flush_b(kMaxBlocksPerChunk);
+  std::vector<int> cur_b(kMaxBlocksPerChunk);
+
+  while (processed < nblocks && status == TANB_OK) {
+    int nb = (int)std::min<size_t>(kMaxBlocksPerChunk, nblocks - processed);
+    TANB_CUDA(cudaEventSynchronize(v->ev_stage));
+    TANB_CUDA(cudaEventSynchronize(v->ev_out));
+    int filled = 0;
+    for (int b = 0; b < nb; ++b) {
+      const size_t blk = processed + b;
+      int nrun = channel_flags(v, flags, run, flush);
+      if (nrun == 0) {
+        status = fail(TANB_WRONG_STATE, "no running channels");
+        break;
+      }
+      ChanCtl* ctl = v->desc_ctl(v->h_stage, b);
+      const float** din = v->desc_in(v->h_stage, b);
+      float** dout = v->desc_out(v->h_stage, b);
+      flush_b[b].clear();
+      for (int c = 0; c < C; ++c) {
+        if (flush[c]) flush_b[b].push_back(c);
+        const int sw = (v->pending[c] && run[c]) ? 1 : 0;
+        ctl[c] = ChanCtl{run[c], sw, v->active[c], v->slot_new[c]};
+        if (sw) {
+          v->active[c] = v->slot_new[c];
+          v->pending[c] = 0;
+        }
+        // A null row reads as silence and its output is discarded.
+        if (in_mem == Mem::Host) {
+          din[c] = in[c] ? v->stage_in(v->d_stage, b, c) : nullptr;
+          if (run[c] && in[c]) std::memcpy(v->stage_in(v->h_stage, b, c), in[c] + blk * B, B * sizeof(float));
+        } else {
+          din[c] = in[c] ? in[c] + blk * B : nullptr;
+        }
+        if (out_mem == Mem::Host) {
+          dout[c] = v->d_out + ((size_t)b * C + c) * B;
+        } else {
+          dout[c] = out[c] ? out[c] + blk * B : nullptr;
+        }
+      }
+      run_b[b] = run;
+      v->cur = (v->cur - 1 + P) % P;
+      cur_b[b] = v->cur;
+      ++filled;
+    }
+    nb = filled;
+    if (nb == 0) break;
+    TANB_CUDA(cudaMemcpyAsync(v->d_stage, v->h_stage, nb * v->desc_bytes, cudaMemcpyHostToDevice, v->stream));
+    if (in_mem == Mem::Host)
+      TANB_CUDA(cudaMemcpyAsync(v->stage_in(v->d_stage, 0, 0), v->stage_in(v->h_stage, 0, 0),
+                                (size_t)nb * C * B * sizeof(float), cudaMemcpyHostToDevice, v->stream));
+    TANB_CUDA(cudaEventRecord(v->ev_stage, v->stream));
+    for (int b = 0; b < nb; ++b) {
+      for (int c : flush_b[b]) TANB_CUDA(flush_channel(v, c));
+      const ChanCtl* dctl = v->desc_ctl(v->d_stage, b);
+      TANB_CUDA(tanb::launch_head_ptrs(v->ds, dctl, v->desc_in(v->d_stage, b), v->desc_out(v->d_stage, b),
+                                       cur_b[b], v->stream));
+      const bool last = (b == nb - 1);
+      if (last) {
+        if (out_mem == Mem::Host)
+          TANB_CUDA(cudaMemcpyAsync(v->h_out, v->d_out, (size_t)nb * C * B * sizeof(float),
+                                    cudaMemcpyDeviceToHost, v->stream));
+        TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
+        v->last_desc = dctl;
+        v->last_cur = cur_b[b];
+        if (v->finalize_mode) {
+          v->finalize_due = true;
+        } else {
+          TANB_CUDA(tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream));
+        }
+      } else {
+        TANB_CUDA(tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream));
+      }
+    }
+    if (out_mem == Mem::Host) {
+      TANB_CUDA(cudaEventSynchronize(v->ev_out));
+      for (int b = 0; b < nb; ++b)
+        for (int c = 0; c < C; ++c)
+          if (run_b[b][c] && out[c])
+            std::memcpy(out[c] + (processed + b) * B, v->h_out + ((size_t)b * C + c) * B, B * sizeof(float));
+    }
+    processed += nb;
+    if (v->finalize_mode && processed < nblocks && status == TANB_OK) {
+      if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
+    }
+  }
+  if (done) *done = processed * B;
+  return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tanb_last_error(void) { return g_last_error.c_str(); }
+
+int32_t tanb_create_context(uint64_t version, int32_t device, tanb_context** ctx) {
+  if (!ctx) return fail(TANB_INVALID_POINTER, "ppContext == NULL");
+  *ctx = nullptr;
+  if ((version >> 48) != 1) return fail(TANB_TAN_UNSUPPORTED_VERSION, "unsupported version %llu", (unsigned long long)(version >> 48));
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    return fail(TANB_NO_DEVICE, "no CUDA device available");
+  if (device < 0 || device >= count) return fail(TANB_INVALID_ARG, "device %d out of range", device);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return fail(TANB_NO_DEVICE, "device query failed");
+  if (prop.major != 10) return fail(TANB_NO_DEVICE, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+  tanb_context* c = new tanb_context();
+  c->device = device;
+  *ctx = c;
+  return TANB_OK;
+}
+
+int32_t tanb_context_release(tanb_context* ctx) {
+  delete ctx;
+  return TANB_OK;
+}
+
+int32_t tanb_create_convolution(tanb_context* ctx, tanb_convolution** conv) {
+  if (!ctx) return fail(TANB_INVALID_POINTER, "pContext == NULL");
+  if (!conv) return fail(TANB_INVALID_POINTER, "ppConvolution == NULL");
+  tanb_convolution* v = new tanb_convolution();
+  v->ctx = ctx;
+  *conv = v;
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_terminate(tanb_convolution* v) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (v->initialized) cudaSetDevice(v->ctx->device);
+  free_all(v);
+  v->initialized = false;
+  v->terminated = true;
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_release(tanb_convolution* v) {
+  if (!v) return TANB_OK;
+  tanb_convolution_terminate(v);
+  delete v;
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, uint32_t B, uint32_t C) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (v->terminated) return fail(TANB_WRONG_STATE, "Cannot initialize after termination");
+  if (L == 0) return fail(TANB_INVALID_ARG, "lengthInSamples == 0");
+  if (B == 0) return fail(TANB_INVALID_ARG, "bufferSizeInSamples == 0");
+  if (C == 0) return fail(TANB_INVALID_ARG, "channels == 0");
+  if ((B & (B - 1)) != 0) return fail(TANB_INVALID_ARG, "bufferSizeInSamples must be power of 2");
+  if (B < 32 || B > 8192) return fail(TANB_INVALID_ARG, "bufferSizeInSamples must be in [32, 8192]");
+  if (v->initialized) return fail(TANB_ALREADY_INITIALIZED, "Already initialized");
+  const uint32_t extra = method & 0xC000u;
+  const uint32_t base = method & ~0xC000u;
+  if (base > TANB_METHOD_FFT_NONUNIFORM_PARTITIONED) return fail(TANB_NOT_SUPPORTED, "convolutionMethod isn't supported");
+  if (base == TANB_METHOD_TIME_DOMAIN) return fail(TANB_NOT_SUPPORTED, "TIME_DOMAIN is not available in this build");
+  v->method = base;
+  v->finalize_mode = (extra == TANB_METHOD_USE_PROCESS_FINALIZE);
+  v->finalize_due = false;
+  v->L = (int)L;
+  v->B = (int)B;
+  v->C = (int)C;
+  v->P = (int)((L + B - 1) / B);
+  if (v->P < 1) v->P = 1;
+  int len = 1;
+  while ((uint32_t)len < L) len <<= 1;
+  v->length = len;
+  int log2B = 0;
+  while ((1 << log2B) < (int)B) ++log2B;
+
+  cudaError_t e = cudaSetDevice(v->ctx->device);
+  if (e != cudaSuccess) return fail(TANB_NO_DEVICE, "cudaSetDevice: %s", cudaGetErrorString(e));
+  if ((e = tanb::prepare_kernels()) != cudaSuccess) return fail(TANB_FAIL, "kernel setup: %s", cudaGetErrorString(e));
+  if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(TANB_FAIL, "stream: %s", cudaGetErrorString(e));
+  const size_t Cs = C, Bs = B, Ps = v->P;
+  v->desc_bytes = (sizeof(ChanCtl) + 2 * sizeof(void*)) * Cs;
+  const size_t stage_bytes = kMaxBlocksPerChunk * (v->desc_bytes + Cs * Bs * sizeof(float));
+  const size_t out_floats = kMaxBlocksPerChunk * Cs * Bs;
+  const size_t uctl_bytes = (sizeof(ChanCtl) + sizeof(int)) * Cs;
+  do {
+    if ((e = dev_alloc(v, &v->ds.H, Cs * 2 * Ps * Bs)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->ds.fdl, Cs * Ps * Bs)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->ds.prev, Cs * Bs)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->ds.tail, Cs * 2 * Bs)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_tw, 2 * Bs)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_stage, stage_bytes)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_out, out_floats)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_ir, Cs * Ps * Bs)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_uctl, uctl_bytes)) != cudaSuccess) break;
+    if ((e = cudaMallocHost(&v->h_stage, stage_bytes)) != cudaSuccess) break;
+    if ((e = cudaMallocHost(&v->h_out, out_floats * sizeof(float))) != cudaSuccess) break;
+    if ((e = cudaMallocHost(&v->h_ir, Cs * Ps * Bs * sizeof(float))) != cudaSuccess) break;
+    if ((e = cudaMallocHost(&v->h_uctl, uctl_bytes)) != cudaSuccess) break;
+    if ((e = cudaEventCreateWithFlags(&v->ev_stage, cudaEventDisableTiming)) != cudaSuccess) break;
+    if ((e = cudaEventCreateWithFlags(&v->ev_ir, cudaEventDisableTiming)) != cudaSuccess) break;
+    if ((e = cudaEventCreateWithFlags(&v->ev_out, cudaEventDisableTiming)) != cudaSuccess) break;
+  } while (0);
+  if (e != cudaSuccess) {
+    free_all(v);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? TANB_OUT_OF_MEMORY : TANB_FAIL, "allocation failed: %s",
+                cudaGetErrorString(e));
+  }
+  std::memset(v->h_stage, 0, stage_bytes);
+  std::vector<float2> tw(2 * Bs);
+  tanb::make_twiddles(2 * B, tw.data());
+  e = cudaMemcpyAsync(v->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, v->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(v->ev_stage, v->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(v->ev_ir, v->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(v->ev_out, v->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
+  if (e != cudaSuccess) {
+    free_all(v);
+    return fail(TANB_FAIL, "init upload: %s", cudaGetErrorString(e));
+  }
+  v->ds.B = B;
+  v->ds.log2B = log2B;
+  v->ds.P = v->P;
+  v->ds.C = C;
+  v->ds.tw = v->d_tw;
+  v->tiling = default_tiling(B, v->P);
+  v->active.assign(C, 0);
+  v->pending.assign(C, 0);
+  v->slot_new.assign(C, 1);
+  v->tail_left.assign(C, 0);
+  v->available.assign(C, 0);
+  v->flushed.assign(C, 0);
+  v->cur = 0;
+  v->initialized = true;
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_update_response_td(tanb_convolution* v, const float* const* ir, size_t n,
+                                            const uint32_t* flags, uint32_t op) {
+  return update_common(v, Mem::Host, ir, n, flags, op);
+}
+
+int32_t tanb_convolution_update_response_td_device(tanb_convolution* v, const float* const* ir, size_t n,
+                                                   const uint32_t* flags, uint32_t op) {
+  return update_common(v, Mem::Device, ir, n, flags, op);
+}
+
+int32_t tanb_convolution_update_response_fd(tanb_convolution* v, const float* const*, size_t, const uint32_t*,
+                                            uint32_t) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "not initialized");
+  return fail(TANB_NOT_SUPPORTED, "UpdateResponseFD is not supported");
+}
+
+int32_t tanb_convolution_process(tanb_convolution* v, const float* const* in, float* const* out, size_t n,
+                                 const uint32_t* flags, size_t* done) {
+  return process_common(v, Mem::Host, in, Mem::Host, out, n, flags, done);
+}
+
+int32_t tanb_convolution_process_host_to_device(tanb_convolution* v, const float* const* in, float* const* out,
+                                                size_t n, const uint32_t* flags, size_t* done) {
+  int32_t r = process_common(v, Mem::Host, in, Mem::Device, out, n, flags, done);
+  if (r == TANB_OK && v->initialized) {
+    cudaError_t e = cudaEventSynchronize(v->ev_out);
+    if (e != cudaSuccess) return fail(TANB_FAIL, "sync: %s", cudaGetErrorString(e));
+  }
+  return r;
+}
+
+int32_t tanb_convolution_process_device(tanb_convolution* v, const float* const* in, float* const* out, size_t n,
+                                        const uint32_t* flags, size_t* done) {
+  return process_common(v, Mem::Device, in, Mem::Device, out, n, flags, done);
+}
+
+int32_t tanb_convolution_process_direct(tanb_convolution* v, const float* const*, const float* const*,
+                                        float* const*, size_t, size_t* done, const int32_t*) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  if (done) *done = 0;
+  return fail(TANB_NOT_SUPPORTED, "ProcessDirect requires the TIME_DOMAIN method");
+}
+
+int32_t tanb_convolution_process_finalize(tanb_convolution* v) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (!v->initialized) return TANB_OK;
+  TANB_CUDA(cudaSetDevice(v->ctx->device));
+  return run_pending_finalize(v);
+}
+
+int32_t tanb_convolution_get_next_free_channel(tanb_convolution* v, uint32_t* idx, const uint32_t* flags) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "not initialized");
+  if (!idx) return fail(TANB_INVALID_ARG, "pChannelIndex == NULL");
+  *idx = 0xFFFFFFFFu;
+  if (!flags) return TANB_NOT_FOUND;
+  for (int c = 0; c < v->C; ++c) {
+    if ((flags[c] & kStopInput) && v->tail_left[c] <= 0) {
+      *idx = (uint32_t)c;
+      return TANB_OK;
+    }
+  }
+  return TANB_NOT_FOUND;
+}
+
+int32_t tanb_convolution_synchronize(tanb_convolution* v) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (!v->initialized) return TANB_OK;
+  TANB_CUDA(cudaSetDevice(v->ctx->device));
+  TANB_CUDA(cudaStreamSynchronize(v->stream));
+  return TANB_OK;
+}
+
+void* tanb_convolution_stream(tanb_convolution* v) { return v ? (void*)v->stream : nullptr; }
+
+int32_t tanb_convolution_info(tanb_convolution* v, int64_t out[4]) {
+  if (!v || !out) return fail(TANB_INVALID_POINTER, "null argument");
+  out[0] = v->P;
+  out[1] = v->B;
+  out[2] = v->C;
+  out[3] = (int64_t)v->dev_bytes;
+  return v->initialized ? TANB_OK : TANB_NOT_INITIALIZED;
+}
+
+}  // extern "C"

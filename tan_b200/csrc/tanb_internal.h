@@ -1,0 +1,76 @@
+// Internal interface between the host engine (tanb_convolution.cpp) and the
+// sm_100a kernels (tanb_kernels.cu). Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tanb {
+
+// Per-channel control word for one audio block, uploaded with the block's input.
+//   run       channel is processed this block (reference: !m_availableChannels[c])
+//   swap      a new IR takes effect this block (crossfade from slot_cur to slot_new)
+//   slot_cur  IR slot in use before this block
+//   slot_new  IR slot holding the pending IR
+struct ChanCtl {
+  int32_t run;
+  int32_t swap;
+  int32_t slot_cur;
+  int32_t slot_new;
+};
+
+// Device-resident state of one convolution object.
+// Spectra are "packed" half spectra of a 2B-point real FFT: B complex bins,
+// bin 0 holding (X[0].re, X[B].re) -- both are real.
+struct DevState {
+  int B;          // block size (power of two)
+  int log2B;
+  int P;          // partitions = ceil(L / B), at least 1
+  int C;          // channels
+  float2* H;      // IR spectra      [C][2 slots][P][B]
+  float2* fdl;    // delay line      [C][P][B]  (slot (cur + i) mod P holds X_{k-i})
+  float* prev;    // previous input  [C][B]     (overlap-save history)
+  float2* tail;   // tails           [C][2][B]  ([0]: active IR, [1]: pending IR)
+  const float2* tw;  // W_N^j, N = 2B, j in [0, N)
+};
+
+__host__ __device__ inline size_t h_index(const DevState& s, int c, int slot, int part) {
+  return (((size_t)c * 2 + slot) * s.P + part) * s.B;
+}
+
+// Tiling of the tail multiply-accumulate: UX units (float4 = 2 bins) by SY
+// partition splits per CTA; UX * SY threads.
+struct MacTiling {
+  int ux;
+  int sy;
+};
+
+// R2C of each IR partition into slot `slot_new` of the channels listed in
+// `chans` (device array of nch channel indices). `ir` is [nch][P*B] floats,
+// row j holding the zero-padded IR of channel chans[j].
+cudaError_t launch_ir_spectrum(const DevState& s, const float* ir, const int* chans, int nch,
+                               const ChanCtl* ctl, cudaStream_t st);
+
+// Head of one block for every running channel: FFT of [prev, x], insert into
+// delay-line slot `cur`, multiply with partition 0, add the precomputed tail,
+// inverse FFT, overlap-save output (and the crossfade on swap channels).
+// `in[c]` / `out[c]` are device pointers to channel c's B input / output samples.
+cudaError_t launch_head_ptrs(const DevState& s, const ChanCtl* ctl, const float* const* in,
+                             float* const* out, int cur, cudaStream_t st);
+
+// Tail multiply-accumulate for the block after the one whose spectrum sits in
+// delay-line slot `cur`:
+//   tail[c][which] = sum_{i=1}^{P-1} FDL[c][(cur + i - 1) mod P] * H[c][slot][i]
+// which = 0: running channels, slot = swap ? slot_new : slot_cur
+// which = 1: channels with swap set (pending IR), slot = slot_new
+cudaError_t launch_tail(const DevState& s, const ChanCtl* ctl, int which, int cur,
+                        MacTiling t, cudaStream_t st);
+
+// Sets the shared-memory attributes of every kernel (once per process).
+cudaError_t prepare_kernels();
+
+// Fills the twiddle table W_N^j = exp(-2 pi i j / N) on the host, computed in
+// double and rounded to float, exact at multiples of pi/2.
+void make_twiddles(int N, float2* out);
+
+}  // namespace tanb
