@@ -204,6 +204,17 @@ void* tanb_convolution_stream(tanb_convolution* conv);
  * out[3] = device bytes held by the object. */
 int32_t tanb_convolution_info(tanb_convolution* conv, int64_t out[4]);
 
+/* No reference counterpart: per-kernel device-time accounting. With enable
+ * != 0 every kernel this object launches is bracketed by a CUDA event pair on
+ * its stream. */
+int32_t tanb_convolution_profile(tanb_convolution* conv, int32_t enable);
+
+/* No reference counterpart: reads and resets the accounting --
+ * counts[0..2] = launches of the head, tail and IR-spectrum kernels since the
+ * last read, counts[3..5] = how many of those were timed, ms[0..2] = their
+ * summed device milliseconds. Waits for the timed launches to finish. */
+int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6], double ms[3]);
+
 /* No reference counterpart: text of the last error raised on this thread. */
 const char* tanb_last_error(void);
 

@@ -266,12 +266,14 @@ int tanref_update_td(void* hh, const float* const* ir, size_t n, const uint32_t*
   if (n > (size_t)r->L) return kInvalidArg;
   for (int c = 0; c < r->C; ++c)
     if (flags && (flags[c] & kFlushStream)) r->flush(c);
-  std::vector<float> td((size_t)r->P * r->B + r->B, 0.f);
+  // one forward transform per partition per channel, OpenMP over channels as
+  // in TANFFTImpl::TransformImplCpuOMP (FFTImpl.cpp:1091-1096)
+#pragma omp parallel for num_threads(r->threads) schedule(static)
   for (int c = 0; c < r->C; ++c) {
     if (flags && (flags[c] & kStopInput)) continue;
     int slot = 1 - r->active[c];
     float* hs = r->h(slot, c);
-    std::fill(td.begin(), td.end(), 0.f);
+    std::vector<float> td((size_t)r->P * r->B + r->B, 0.f);
     std::memcpy(td.data(), ir[c], sizeof(float) * n);
     std::vector<float> frame(r->N), zr(r->B), zi(r->B);
     for (int i = 0; i < r->P; ++i) {

@@ -84,6 +84,8 @@ SIGNATURES = {
     "tanb_convolution_synchronize": (_i32, [_vp]),
     "tanb_convolution_stream": (_vp, [_vp]),
     "tanb_convolution_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "tanb_convolution_profile": (_i32, [_vp, _i32]),
+    "tanb_convolution_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_last_error": (ctypes.c_char_p, []),
 }
 
@@ -284,6 +286,17 @@ class TANConvolution:
 
     def stream(self) -> int:
         return lib().tanb_convolution_stream(self._h) or 0
+
+    def profile(self, enable: bool) -> int:
+        return lib().tanb_convolution_profile(self._h, 1 if enable else 0)
+
+    def profile_read(self) -> dict:
+        """Launch counts and device ms per kernel since the last read."""
+        counts = (ctypes.c_int64 * 6)()
+        ms = (ctypes.c_double * 3)()
+        lib().tanb_convolution_profile_read(self._h, counts, ms)
+        names = ("head", "tail", "ir_spectrum")
+        return {n: {"launches": counts[i], "timed": counts[3 + i], "ms": ms[i]} for i, n in enumerate(names)}
 
     def info(self) -> dict:
         out = (ctypes.c_int64 * 4)()

@@ -98,6 +98,19 @@ struct tanb_convolution {
 
   cudaEvent_t ev_stage = nullptr, ev_ir = nullptr, ev_out = nullptr;
 
+  // kernel accounting: launch counts always, device time when profiling is on
+  enum Kind { kHead = 0, kTail = 1, kIr = 2, kKinds = 3 };
+  int64_t launches[kKinds] = {0, 0, 0};
+  bool profiling = false;
+  struct Timed {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Timed> timed;          // recorded, not yet read
+  std::vector<cudaEvent_t> ev_pool;  // free events
+  double ms[kKinds] = {0, 0, 0};
+  int64_t timed_count[kKinds] = {0, 0, 0};
+
   // descriptor accessors
   ChanCtl* desc_ctl(uint8_t* base, int b) { return reinterpret_cast<ChanCtl*>(base + b * desc_bytes); }
   const float** desc_in(uint8_t* base, int b) {
@@ -113,8 +126,49 @@ struct tanb_convolution {
 
 namespace {
 
+cudaEvent_t pool_event(tanb_convolution* v) {
+  if (!v->ev_pool.empty()) {
+    cudaEvent_t e = v->ev_pool.back();
+    v->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Runs `launch` on the object's stream, counting it and, when profiling, timing
+// it with an event pair on the same stream.
+template <typename F>
+cudaError_t counted(tanb_convolution* v, int kind, F&& launch) {
+  v->launches[kind] += 1;
+  if (!v->profiling) return launch();
+  cudaEvent_t a = pool_event(v), b = pool_event(v);
+  cudaEventRecord(a, v->stream);
+  cudaError_t e = launch();
+  cudaEventRecord(b, v->stream);
+  v->timed.push_back({kind, a, b});
+  return e;
+}
+
+void drain_timed(tanb_convolution* v) {
+  for (auto& t : v->timed) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+      v->ms[t.kind] += ms;
+      v->timed_count[t.kind] += 1;
+    }
+    v->ev_pool.push_back(t.a);
+    v->ev_pool.push_back(t.b);
+  }
+  v->timed.clear();
+}
+
 void free_all(tanb_convolution* v) {
   if (v->stream) cudaStreamSynchronize(v->stream);
+  drain_timed(v);
+  for (cudaEvent_t e : v->ev_pool) cudaEventDestroy(e);
+  v->ev_pool.clear();
   cudaFree(v->ds.H);
   cudaFree(v->ds.fdl);
   cudaFree(v->ds.prev);
@@ -176,7 +230,9 @@ cudaError_t flush_channel(tanb_convolution* v, int c) {
 int32_t run_pending_finalize(tanb_convolution* v) {
   if (!v->finalize_due) return TANB_OK;
   v->finalize_due = false;
-  TANB_CUDA(tanb::launch_tail(v->ds, v->last_desc, 0, v->last_cur, v->tiling, v->stream));
+  if (v->P <= 1) return TANB_OK;
+  TANB_CUDA(counted(v, tanb_convolution::kTail,
+                    [&] { return tanb::launch_tail(v->ds, v->last_desc, 0, v->last_cur, v->tiling, v->stream); }));
   return TANB_OK;
 }
 
@@ -233,9 +289,12 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   TANB_CUDA(cudaEventRecord(v->ev_ir, v->stream));
   const ChanCtl* d_uctl = reinterpret_cast<const ChanCtl*>(v->d_uctl);
   const int* d_uch = reinterpret_cast<const int*>(v->d_uctl + sizeof(ChanCtl) * C);
-  TANB_CUDA(tanb::launch_ir_spectrum(v->ds, v->d_ir, d_uch, nch, d_uctl, v->stream));
+  TANB_CUDA(counted(v, tanb_convolution::kIr,
+                    [&] { return tanb::launch_ir_spectrum(v->ds, v->d_ir, d_uch, nch, d_uctl, v->stream); }));
   // tail of the pending IR for the next block, from the current delay line
-  TANB_CUDA(tanb::launch_tail(v->ds, d_uctl, 1, v->cur, v->tiling, v->stream));
+  if (v->P > 1)
+    TANB_CUDA(counted(v, tanb_convolution::kTail,
+                      [&] { return tanb::launch_tail(v->ds, d_uctl, 1, v->cur, v->tiling, v->stream); }));
   if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) TANB_CUDA(cudaStreamSynchronize(v->stream));
   return TANB_OK;
 }
@@ -352,8 +411,10 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     for (int b = 0; b < nb; ++b) {
       for (int c : flush_b[b]) TANB_CUDA(flush_channel(v, c));
       const ChanCtl* dctl = v->desc_ctl(v->d_stage, b);
-      TANB_CUDA(tanb::launch_head_ptrs(v->ds, dctl, v->desc_in(v->d_stage, b), v->desc_out(v->d_stage, b),
-                                       cur_b[b], v->stream));
+      TANB_CUDA(counted(v, tanb_convolution::kHead, [&] {
+        return tanb::launch_head_ptrs(v->ds, dctl, v->desc_in(v->d_stage, b), v->desc_out(v->d_stage, b),
+                                      cur_b[b], v->stream);
+      }));
       const bool last = (b == nb - 1);
       if (last) {
         if (out_mem == Mem::Host)
@@ -364,11 +425,13 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         v->last_cur = cur_b[b];
         if (v->finalize_mode) {
           v->finalize_due = true;
-        } else {
-          TANB_CUDA(tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream));
+        } else if (P > 1) {
+          TANB_CUDA(counted(v, tanb_convolution::kTail,
+                            [&] { return tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream); }));
         }
-      } else {
-        TANB_CUDA(tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream));
+      } else if (P > 1) {
+        TANB_CUDA(counted(v, tanb_convolution::kTail,
+                          [&] { return tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream); }));
       }
     }
     if (out_mem == Mem::Host) {
@@ -610,6 +673,29 @@ int32_t tanb_convolution_synchronize(tanb_convolution* v) {
 }
 
 void* tanb_convolution_stream(tanb_convolution* v) { return v ? (void*)v->stream : nullptr; }
+
+int32_t tanb_convolution_profile(tanb_convolution* v, int32_t enable) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  v->profiling = enable != 0;
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_profile_read(tanb_convolution* v, int64_t counts[6], double ms[3]) {
+  if (!v || !counts || !ms) return fail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (v->initialized) cudaSetDevice(v->ctx->device);
+  drain_timed(v);
+  for (int k = 0; k < tanb_convolution::kKinds; ++k) {
+    counts[k] = v->launches[k];
+    counts[3 + k] = v->timed_count[k];
+    ms[k] = v->ms[k];
+    v->launches[k] = 0;
+    v->timed_count[k] = 0;
+    v->ms[k] = 0.0;
+  }
+  return TANB_OK;
+}
 
 int32_t tanb_convolution_info(tanb_convolution* v, int64_t out[4]) {
   if (!v || !out) return fail(TANB_INVALID_POINTER, "null argument");
