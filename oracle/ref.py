@@ -43,6 +43,12 @@ def lib() -> ctypes.CDLL:
         L.tanref_process.restype = i32
         L.tanref_next_free_channel.argtypes = [vp, u32p, u32p]
         L.tanref_next_free_channel.restype = i32
+        L.tanref_td_create.restype = vp
+        L.tanref_td_create.argtypes = [i32, i32]
+        L.tanref_td_destroy.argtypes = [vp]
+        L.tanref_td_process_direct.restype = i32
+        L.tanref_td_process_direct.argtypes = [vp, fpp, fpp, fpp, sz, ctypes.POINTER(sz),
+                                               ctypes.POINTER(ctypes.c_int32)]
         fp = ctypes.c_void_p
         L.tanref_rfft.argtypes = [i32, fp, fp, fp]
         L.tanref_irfft.argtypes = [i32, fp, fp, fp]
@@ -106,6 +112,38 @@ class RefConvolution:
         fl = _flags(flags, self.C)
         rc = lib().tanref_next_free_channel(self._h, ctypes.byref(idx), fl[1] if fl else None)
         return rc, idx.value
+
+
+class RefTimeDomain:
+    """Mirror of TANConvolution::ProcessDirect for TIME_DOMAIN over the restatement."""
+
+    def __init__(self, length: int, channels: int):
+        self.L, self.C = length, channels
+        self._h = lib().tanref_td_create(length, channels)
+        if not self._h:
+            raise ValueError("invalid oracle configuration")
+
+    def close(self):
+        if self._h:
+            lib().tanref_td_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def process_direct(self, ir: np.ndarray, x: np.ndarray, nz=None):
+        ir = np.ascontiguousarray(ir, dtype=np.float32)
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.zeros_like(x)
+        nzp = None
+        if nz is not None:
+            nzk = np.ascontiguousarray(np.asarray(nz, dtype=np.int32))
+            nzp = nzk.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        done = ctypes.c_size_t(0)
+        rc = lib().tanref_td_process_direct(self._h, _ptrs([ir[c] for c in range(self.C)]),
+                                            _ptrs([x[c] for c in range(self.C)]),
+                                            _ptrs([out[c] for c in range(self.C)]), x.shape[1],
+                                            ctypes.byref(done), nzp)
+        return rc, out, done.value
 
 
 def rfft(x: np.ndarray):

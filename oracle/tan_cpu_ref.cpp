@@ -40,6 +40,8 @@
 //  * Per-channel state is indexed by channel, not by running-channel rank, and
 //    a flush also clears the precomputed tail (the reference's CPU flush
 //    dereferences an unallocated state array, ConvolutionImpl.cpp:1284-1325).
+//  * A free channel (rung out or stopped+flushed) that runs again starts from
+//    silence; the reference keeps whatever its last ring-out block left.
 #include <immintrin.h>
 #include <omp.h>
 
@@ -304,6 +306,7 @@ int tanref_process(void* hh, const float* const* in, float* const* out, size_t n
     int nrun = 0;
     for (int c = 0; c < C; ++c) {
       uint32_t f = flags ? flags[c] : 0u;
+      const bool was_free = r->available[c] != 0;
       if (!flags) {
         r->available[c] = 0;
         r->tailLeft[c] = r->length;
@@ -330,6 +333,8 @@ int tanref_process(void* hh, const float* const* in, float* const* out, size_t n
         r->flushed[c] = 0;
       }
       run[c] = !r->available[c];
+      // a free channel that starts running again starts from silence
+      if (was_free && run[c]) r->flush(c);
       nrun += run[c];
     }
     if (nrun == 0) return kWrongState;
@@ -417,6 +422,57 @@ int tanref_next_free_channel(void* hh, uint32_t* idx, const uint32_t* flags) {
     }
   }
   return kNotFound;
+}
+
+// TIME_DOMAIN method: ProcessDirect (ConvolutionImpl.cpp:721-762) over
+// ovlTimeDomainCPU (:2757-2782). One circular history of nextpow2(L) samples
+// per channel; each call appends n <= nextpow2(L) samples and computes
+//   out[j] = sum_{k=first}^{last-1} hist[(pos + j - k) mod len] * ir[k]
+// accumulating in float in increasing k.
+struct RefTD {
+  int L = 0, C = 0, length = 0;
+  std::vector<float> hist;  // [C][length]
+  std::vector<int> pos;     // per channel
+};
+
+void* tanref_td_create(int L, int C) {
+  if (L <= 0 || C <= 0) return nullptr;
+  RefTD* r = new RefTD();
+  r->L = L;
+  r->C = C;
+  int len = 1;
+  while (len < L) len <<= 1;
+  r->length = len;
+  r->hist.assign((size_t)C * len, 0.f);
+  r->pos.assign(C, 0);
+  return r;
+}
+
+void tanref_td_destroy(void* h) { delete static_cast<RefTD*>(h); }
+
+int tanref_td_process_direct(void* hh, const float* const* ir, const float* const* in, float* const* out,
+                             size_t n, size_t* done, const int* nz) {
+  RefTD* r = static_cast<RefTD*>(hh);
+  const int len = r->length;
+  if (n > (size_t)len) n = len;
+  for (int c = 0; c < r->C; ++c) {
+    int first = 0, last = len;
+    if (nz) {
+      first = nz[2 * c];
+      last = nz[2 * c + 1];
+    }
+    float* hist = r->hist.data() + (size_t)c * len;
+    const int p = r->pos[c] % len;
+    for (size_t i = 0; i < n; ++i) hist[(p + i) % len] = in[c][i];
+    for (size_t j = 0; j < n; ++j) {
+      float acc = 0.f;
+      for (int k = first; k < last; ++k) acc += hist[((size_t)p + j - k + len) % len] * ir[c][k];
+      out[c][j] = acc;
+    }
+    r->pos[c] += (int)n;
+  }
+  if (done) *done = n;
+  return kOk;
 }
 
 // Plain forward/inverse real FFT, exposed for the oracle's own tests.

@@ -98,6 +98,19 @@ struct tanb_convolution {
 
   cudaEvent_t ev_stage = nullptr, ev_ir = nullptr, ev_out = nullptr;
 
+  // TIME_DOMAIN method state (history of `length` samples per channel)
+  bool td = false;
+  float* td_hist = nullptr;    // [C][length]
+  float* td_ir = nullptr;      // [2 slots][C][length]  (Process IRs)
+  float* td_dir = nullptr;     // [C][length]           (ProcessDirect per-call IRs)
+  float* td_io = nullptr;      // [2][C][length]        (device in / out staging)
+  float* h_td = nullptr;       // pinned [3][C][length] (IR, in, out staging)
+  tanb::TdChan* d_tdchan = nullptr;
+  tanb::TdChan* h_tdchan = nullptr;
+  std::vector<int> td_pos;
+  int td_fade = -1;            // crossfade sample index, -1 when none
+  std::vector<int> td_swapping;
+
   // kernel accounting: launch counts always, device time when profiling is on
   enum Kind { kHead = 0, kTail = 1, kIr = 2, kKinds = 3 };
   int64_t launches[kKinds] = {0, 0, 0};
@@ -182,6 +195,15 @@ void free_all(tanb_convolution* v) {
   cudaFreeHost(v->h_out);
   cudaFreeHost(v->h_ir);
   cudaFreeHost(v->h_uctl);
+  cudaFree(v->td_hist);
+  cudaFree(v->td_ir);
+  cudaFree(v->td_dir);
+  cudaFree(v->td_io);
+  cudaFree(v->d_tdchan);
+  cudaFreeHost(v->h_td);
+  cudaFreeHost(v->h_tdchan);
+  v->td_hist = v->td_ir = v->td_dir = v->td_io = v->h_td = nullptr;
+  v->d_tdchan = v->h_tdchan = nullptr;
   if (v->ev_stage) cudaEventDestroy(v->ev_stage);
   if (v->ev_ir) cudaEventDestroy(v->ev_ir);
   if (v->ev_out) cudaEventDestroy(v->ev_out);
@@ -236,6 +258,13 @@ int32_t run_pending_finalize(tanb_convolution* v) {
   return TANB_OK;
 }
 
+int32_t td_update(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags,
+                  uint32_t op);
+int32_t td_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
+                   size_t n, const uint32_t* flags, size_t* done);
+int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_t>& run,
+                  std::vector<uint8_t>& flush);
+
 int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags,
                       uint32_t op) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
@@ -244,6 +273,7 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   if (!ir) return fail(TANB_INVALID_ARG, "ppBuffer == NULL");
   if (n > (size_t)v->L) return fail(TANB_INVALID_ARG, "IR length %zu exceeds Init length %d", n, v->L);
   TANB_CUDA(cudaSetDevice(v->ctx->device));
+  if (v->td) return td_update(v, mem, ir, n, flags, op);
   if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
 
   const int C = v->C, PB = v->P * v->B;
@@ -308,6 +338,7 @@ int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_
   for (int c = 0; c < v->C; ++c) {
     flush[c] = 0;
     const uint32_t f = flags ? flags[c] : 0u;
+    const bool was_free = v->available[c] != 0;
     if (!flags) {
       v->available[c] = 0;
       v->tail_left[c] = v->length;
@@ -334,6 +365,8 @@ int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_
       v->flushed[c] = 0;
     }
     run[c] = !v->available[c];
+    // a free channel that starts running again starts from silence
+    if (was_free && run[c]) flush[c] = 1;
     nrun += run[c];
   }
   return nrun;
@@ -348,6 +381,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   if (!in) return fail(TANB_INVALID_ARG, "ppBufferInput == NULL");
   if (!out) return fail(TANB_INVALID_ARG, "ppBufferOutput == NULL");
   TANB_CUDA(cudaSetDevice(v->ctx->device));
+  if (v->td) return td_process(v, in_mem, in, out_mem, out, n, flags, done);
   if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
 
   const int B = v->B, C = v->C, P = v->P;
@@ -450,6 +484,183 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   return status;
 }
 
+// ---------------------------------------------------------------------------
+// TIME_DOMAIN method (ConvolutionImpl.cpp:407-468, 721-762, 2645-2782)
+// ---------------------------------------------------------------------------
+
+cudaError_t td_alloc(tanb_convolution* v) {
+  const size_t C = v->C, len = v->length;
+  cudaError_t e;
+  if ((e = dev_alloc(v, &v->td_hist, C * len)) != cudaSuccess) return e;
+  if ((e = dev_alloc(v, &v->td_ir, 2 * C * len)) != cudaSuccess) return e;
+  if ((e = dev_alloc(v, &v->td_dir, C * len)) != cudaSuccess) return e;
+  if ((e = dev_alloc(v, &v->td_io, 2 * C * len)) != cudaSuccess) return e;
+  if ((e = dev_alloc(v, &v->d_tdchan, C)) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&v->h_td, 3 * C * len * sizeof(float))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&v->h_tdchan, C * sizeof(tanb::TdChan))) != cudaSuccess) return e;
+  v->td_pos.assign(C, 0);
+  v->td_fade = -1;
+  v->td_swapping.assign(C, 0);
+  return cudaSuccess;
+}
+
+float* td_ir_row(tanb_convolution* v, int slot, int c) {
+  return v->td_ir + ((size_t)slot * v->C + c) * v->length;
+}
+
+int32_t td_update(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags,
+                  uint32_t op) {
+  const size_t len = v->length;
+  TANB_CUDA(cudaStreamSynchronize(v->stream));  // pinned IR staging is reused
+  for (int c = 0; c < v->C; ++c) {
+    if (flags && (flags[c] & kFlush)) {
+      TANB_CUDA(cudaMemsetAsync(v->td_hist + (size_t)c * len, 0, len * sizeof(float), v->stream));
+      v->td_pos[c] = 0;
+    }
+    if (flags && (flags[c] & kStopInput)) continue;
+    if (!ir[c] && n > 0) return fail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", c);
+    if (!v->pending[c]) {
+      v->slot_new[c] = 1 - v->active[c];
+      v->pending[c] = 1;
+    }
+    float* dst = td_ir_row(v, v->slot_new[c], c);
+    if (mem == Mem::Host) {
+      float* row = v->h_td + (size_t)c * len;
+      if (n) std::memcpy(row, ir[c], n * sizeof(float));
+      std::memset(row + n, 0, (len - n) * sizeof(float));
+      TANB_CUDA(cudaMemcpyAsync(dst, row, len * sizeof(float), cudaMemcpyHostToDevice, v->stream));
+    } else {
+      if (n) TANB_CUDA(cudaMemcpyAsync(dst, ir[c], n * sizeof(float), cudaMemcpyDeviceToDevice, v->stream));
+      TANB_CUDA(cudaMemsetAsync(dst + n, 0, (len - n) * sizeof(float), v->stream));
+    }
+  }
+  if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) TANB_CUDA(cudaStreamSynchronize(v->stream));
+  return TANB_OK;
+}
+
+// Runs one TIME_DOMAIN call: the descriptors in h_tdchan are filled; inputs
+// are staged (host) or referenced (device); outputs go to staging (host).
+int32_t td_launch(tanb_convolution* v, int n, bool host_in, bool host_out, float* const* out) {
+  const size_t C = v->C, len = v->length;
+  float* h_in = v->h_td + C * len;
+  float* h_out = v->h_td + 2 * C * len;
+  if (host_in)
+    TANB_CUDA(cudaMemcpyAsync(v->td_io, h_in, C * len * sizeof(float), cudaMemcpyHostToDevice, v->stream));
+  TANB_CUDA(cudaMemcpyAsync(v->d_tdchan, v->h_tdchan, C * sizeof(tanb::TdChan), cudaMemcpyHostToDevice,
+                            v->stream));
+  TANB_CUDA(counted(v, tanb_convolution::kTail,
+                    [&] { return tanb::launch_td(v->td_hist, (int)len, v->d_tdchan, (int)C, n, v->B, v->stream); }));
+  if (host_out) {
+    TANB_CUDA(cudaMemcpyAsync(h_out, v->td_io + C * len, C * len * sizeof(float), cudaMemcpyDeviceToHost,
+                              v->stream));
+  }
+  TANB_CUDA(cudaStreamSynchronize(v->stream));
+  if (host_out)
+    for (size_t c = 0; c < C; ++c)
+      if (v->h_tdchan[c].run && out[c]) std::memcpy(out[c], h_out + c * len, n * sizeof(float));
+  return TANB_OK;
+}
+
+int32_t td_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
+                   size_t n, const uint32_t* flags, size_t* done) {
+  const size_t C = v->C, len = v->length;
+  const int ns = (int)std::min<size_t>(n, (size_t)v->B);
+  if (ns == 0) return TANB_OK;
+  std::vector<uint8_t> run(C), flush(C);
+  if (channel_flags(v, flags, run, flush) == 0) return fail(TANB_WRONG_STATE, "no running channels");
+  TANB_CUDA(cudaStreamSynchronize(v->stream));
+  for (size_t c = 0; c < C; ++c)
+    if (flush[c]) {
+      TANB_CUDA(cudaMemsetAsync(v->td_hist + c * len, 0, len * sizeof(float), v->stream));
+      v->td_pos[c] = 0;
+    }
+  if (v->td_fade < 0) {
+    bool any = false;
+    for (size_t c = 0; c < C; ++c) {
+      v->td_swapping[c] = v->pending[c] && run[c];
+      any = any || v->td_swapping[c];
+    }
+    if (any) v->td_fade = 0;
+  }
+  float* h_in = v->h_td + C * len;
+  for (size_t c = 0; c < C; ++c) {
+    tanb::TdChan& t = v->h_tdchan[c];
+    t = tanb::TdChan{};
+    t.run = run[c];
+    t.pos = v->td_pos[c];
+    t.first = 0;
+    t.last = (int)len;
+    t.ir = td_ir_row(v, v->active[c], c);
+    t.ir_new = td_ir_row(v, v->slot_new[c], c);
+    t.swap = (v->td_fade >= 0 && v->td_swapping[c]) ? 1 : 0;
+    t.fade0 = v->td_fade < 0 ? 0 : v->td_fade;
+    if (in_mem == Mem::Host) {
+      t.in = in[c] ? v->td_io + c * len : nullptr;
+      if (in[c] && run[c]) std::memcpy(h_in + c * len, in[c], ns * sizeof(float));
+    } else {
+      t.in = in[c];
+    }
+    t.out = out_mem == Mem::Host ? v->td_io + (C + c) * len : out[c];
+  }
+  int32_t r = td_launch(v, ns, in_mem == Mem::Host, out_mem == Mem::Host, out);
+  if (r != TANB_OK) return r;
+  for (size_t c = 0; c < C; ++c)
+    if (run[c]) v->td_pos[c] = (int)((v->td_pos[c] + ns) % len);
+  if (v->td_fade >= 0) {
+    v->td_fade += ns;
+    if (v->td_fade >= v->B) {
+      for (size_t c = 0; c < C; ++c)
+        if (v->td_swapping[c]) {
+          v->active[c] = v->slot_new[c];
+          v->pending[c] = 0;
+          v->td_swapping[c] = 0;
+        }
+      v->td_fade = -1;
+    }
+  }
+  if (done) *done = ns;
+  return TANB_OK;
+}
+
+int32_t td_process_direct(tanb_convolution* v, const float* const* ir, const float* const* in, float* const* out,
+                          size_t n, size_t* done, const int32_t* nz) {
+  const size_t C = v->C, len = v->length;
+  if (n > len) n = len;
+  for (size_t c = 0; c < C; ++c) {
+    const int first = nz ? nz[2 * c] : 0, last = nz ? nz[2 * c + 1] : (int)len;
+    if (first < 0 || last > (int)len || first > last)
+      return fail(TANB_INVALID_ARG, "nzFirstLast[%zu] = [%d, %d) outside [0, %zu]", c, first, last, len);
+    if (!in[c] || !out[c] || (!ir[c] && last > first)) return fail(TANB_INVALID_ARG, "null buffer for channel %zu", c);
+  }
+  if (n == 0) return TANB_OK;
+  TANB_CUDA(cudaStreamSynchronize(v->stream));
+  float* h_in = v->h_td + C * len;
+  for (size_t c = 0; c < C; ++c) {
+    const int first = nz ? nz[2 * c] : 0, last = nz ? nz[2 * c + 1] : (int)len;
+    float* row = v->h_td + c * len;
+    if (last > first) {
+      std::memcpy(row + first, ir[c] + first, (last - first) * sizeof(float));
+      TANB_CUDA(cudaMemcpyAsync(v->td_dir + c * len + first, row + first, (last - first) * sizeof(float),
+                                cudaMemcpyHostToDevice, v->stream));
+    }
+    std::memcpy(h_in + c * len, in[c], n * sizeof(float));
+    tanb::TdChan& t = v->h_tdchan[c];
+    t = tanb::TdChan{};
+    t.run = 1;
+    t.pos = v->td_pos[c];
+    t.first = first;
+    t.last = last;
+    t.ir = v->td_dir + c * len;
+    t.in = v->td_io + c * len;
+    t.out = v->td_io + (C + c) * len;
+  }
+  int32_t r = td_launch(v, (int)n, true, true, out);
+  if (r != TANB_OK) return r;
+  for (size_t c = 0; c < C; ++c) v->td_pos[c] = (int)((v->td_pos[c] + n) % len);
+  if (done) *done = n;
+  return TANB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -517,7 +728,6 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
   const uint32_t extra = method & 0xC000u;
   const uint32_t base = method & ~0xC000u;
   if (base > TANB_METHOD_FFT_NONUNIFORM_PARTITIONED) return fail(TANB_NOT_SUPPORTED, "convolutionMethod isn't supported");
-  if (base == TANB_METHOD_TIME_DOMAIN) return fail(TANB_NOT_SUPPORTED, "TIME_DOMAIN is not available in this build");
   v->method = base;
   v->finalize_mode = (extra == TANB_METHOD_USE_PROCESS_FINALIZE);
   v->finalize_due = false;
@@ -538,6 +748,25 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
   if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess)
     return fail(TANB_FAIL, "stream: %s", cudaGetErrorString(e));
   const size_t Cs = C, Bs = B, Ps = v->P;
+  v->td = (base == TANB_METHOD_TIME_DOMAIN);
+  if (v->td) {
+    e = td_alloc(v);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
+    if (e != cudaSuccess) {
+      free_all(v);
+      cudaGetLastError();
+      return fail(e == cudaErrorMemoryAllocation ? TANB_OUT_OF_MEMORY : TANB_FAIL, "allocation failed: %s",
+                  cudaGetErrorString(e));
+    }
+    v->active.assign(C, 0);
+    v->pending.assign(C, 0);
+    v->slot_new.assign(C, 1);
+    v->tail_left.assign(C, 0);
+    v->available.assign(C, 0);
+    v->flushed.assign(C, 0);
+    v->initialized = true;
+    return TANB_OK;
+  }
   v->desc_bytes = (sizeof(ChanCtl) + 2 * sizeof(void*)) * Cs;
   const size_t stage_bytes = kMaxBlocksPerChunk * (v->desc_bytes + Cs * Bs * sizeof(float));
   const size_t out_floats = kMaxBlocksPerChunk * Cs * Bs;
@@ -632,11 +861,16 @@ int32_t tanb_convolution_process_device(tanb_convolution* v, const float* const*
   return process_common(v, Mem::Device, in, Mem::Device, out, n, flags, done);
 }
 
-int32_t tanb_convolution_process_direct(tanb_convolution* v, const float* const*, const float* const*,
-                                        float* const*, size_t, size_t* done, const int32_t*) {
+int32_t tanb_convolution_process_direct(tanb_convolution* v, const float* const* ir, const float* const* in,
+                                        float* const* out, size_t n, size_t* done, const int32_t* nz) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
   if (done) *done = 0;
-  return fail(TANB_NOT_SUPPORTED, "ProcessDirect requires the TIME_DOMAIN method");
+  if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "ProcessDirect before Init");
+  if (!v->td) return fail(TANB_NOT_SUPPORTED, "ProcessDirect requires the TIME_DOMAIN method");
+  if (!ir || !in || !out) return fail(TANB_INVALID_ARG, "null buffer array");
+  TANB_CUDA(cudaSetDevice(v->ctx->device));
+  return td_process_direct(v, ir, in, out, n, done, nz);
 }
 
 int32_t tanb_convolution_process_finalize(tanb_convolution* v) {

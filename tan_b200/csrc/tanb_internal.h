@@ -66,6 +66,24 @@ cudaError_t launch_head_ptrs(const DevState& s, const ChanCtl* ctl, const float*
 cudaError_t launch_tail(const DevState& s, const ChanCtl* ctl, int which, int cur,
                         MacTiling t, cudaStream_t st);
 
+// Per-channel descriptor of one TIME_DOMAIN call.
+struct TdChan {
+  const float* in;      // device row of n input samples (null: silence)
+  float* out;           // device row of n outputs (null: discarded)
+  const float* ir;      // device IR row, taps [first, last) valid
+  const float* ir_new;  // second IR on a crossfade call
+  int32_t pos;          // history position before this call
+  int32_t first, last;  // tap range
+  int32_t run;          // channel processed
+  int32_t swap;         // crossfade ir -> ir_new
+  int32_t fade0;        // crossfade sample index of this call's first output
+  int32_t pad[2];
+};
+
+// TIME_DOMAIN: append n input samples to each running channel's circular
+// history (len samples, [C][len]) and compute n direct-FIR outputs.
+cudaError_t launch_td(float* hist, int len, const TdChan* ch, int C, int n, int fade_len, cudaStream_t st);
+
 // Sets the shared-memory attributes of every kernel (once per process).
 cudaError_t prepare_kernels();
 

@@ -119,3 +119,28 @@ def test_restatement_stop_input_ring_out_and_free_channel():
     conv2 = ref.RefConvolution(L, B, 1)
     rc, _, _ = conv2.process(H.noise(g, 1, B), np.array([3], np.uint32))
     assert rc == 15
+
+
+def test_restatement_free_channel_restarts_from_silence():
+    """Stop -> ring-out (input still applied) -> flushed on the last ring-out
+    block -> free (output untouched) -> running again from silence."""
+    g = H.rng(12)
+    C, B, L, nb = 2, 128, 500, 24  # nextpow2(L) = 512: ring-out of 4 blocks
+    x = H.noise(g, C, nb * B)
+    h = H.irs(g, C, L)
+    flags = [np.array([1 if 5 <= k < 15 else 0, 0], np.uint32) for k in range(nb)]
+    conv = ref.RefConvolution(L, B, C)
+    assert conv.update_response_td(h) == 0
+    y = np.full((C, nb * B), 9.0, np.float32)
+    for k in range(nb):
+        ys = y[:, k * B:(k + 1) * B].copy()
+        rc, ys, _ = conv.process(np.ascontiguousarray(x[:, k * B:(k + 1) * B]), flags[k], ys)
+        assert rc == 0
+        y[:, k * B:(k + 1) * B] = ys
+    # ring-out blocks 5..8, flush before block 8, free 9..14, restart (flush) at 15
+    exp = fp64.stream_fp64(x, B, [(0, {0: h[0], 1: h[1]})], flush_events=[(8, [0]), (15, [0])])
+    live = np.ones(nb * B, bool)
+    live[9 * B:15 * B] = False
+    assert np.all(y[0, ~live] == 9.0)
+    assert fp64.error_db(y[0, live], exp[0, live]) < -120
+    assert fp64.error_db(y[1], exp[1]) < -120
