@@ -215,6 +215,65 @@ int32_t tanb_convolution_profile(tanb_convolution* conv, int32_t enable);
  * summed device milliseconds. Waits for the timed launches to finish. */
 int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6], double ms[3]);
 
+/* ---------------------------------------------------------------------------
+ * Batched engine. No single reference counterpart: it is the serving form of
+ * the same path -- many TANConvolution-equivalent sessions (C channels, IR
+ * length L each) processed together, one head and one tail launch per block
+ * for all of them, the role the reference's GPU engine plays with its channel
+ * maps (tan/tanlibrary/src/Graal/GraalConv.cpp:644-704, 1883-2145).
+ * ------------------------------------------------------------------------- */
+typedef struct tanb_engine tanb_engine;
+
+enum { TANB_SPECTRUM_FP32 = 0, TANB_SPECTRUM_FP16 = 1, TANB_SPECTRUM_BF16 = 2 };
+
+/* Creates an engine for blocks of `block` samples (power of two in
+ * [128, 2048]). IR spectra are stored as `spectrum` (FP16 / BF16 with a
+ * power-of-two scale per partition; accumulation is FP32). Sessions are
+ * admitted while their device memory fits in `budget_bytes`; at most
+ * `max_channels` channel slots. `partitions_per_item` (0: 32) sets the size of
+ * the tail's work items. */
+int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum, uint64_t budget_bytes,
+                           uint32_t max_channels, uint32_t partitions_per_item, tanb_engine** engine);
+int32_t tanb_engine_release(tanb_engine* engine);
+
+/* Admits a session of `channels` channels and IR length `ir_length`; its
+ * channels occupy slots [*first_slot, *first_slot + channels) of the I/O
+ * buffers. AMF_OUT_OF_MEMORY when the budget or the slot table is exhausted.
+ * The session starts with an all-zero IR. */
+int32_t tanb_engine_open_session(tanb_engine* engine, uint32_t channels, uint32_t ir_length, int32_t* session,
+                                 uint32_t* first_slot);
+int32_t tanb_engine_close_session(tanb_engine* engine, int32_t session);
+
+/* UpdateResponseTD for one session (host IR rows, n <= ir_length): the new IR
+ * takes effect with a one-block crossfade on the next processed block. */
+int32_t tanb_engine_update_response_td(tanb_engine* engine, int32_t session, const float* const* ir, size_t n);
+
+/* Pinned host I/O buffers [max_channels][block]: write slot s's input block at
+ * in[s * block], read its output at out[s * block] after tanb_engine_process. */
+int32_t tanb_engine_io(tanb_engine* engine, float** in, float** out);
+
+/* One block for every open session through the host buffers; returns when the
+ * output is in the pinned output buffer (the tail for the next block runs on). */
+int32_t tanb_engine_process(tanb_engine* engine);
+
+/* One block with device-resident I/O: slot s reads in[s * ld] (null: silence)
+ * and writes out[s * ld]. Asynchronous on the engine's stream. */
+int32_t tanb_engine_process_device(tanb_engine* engine, const float* in, float* out, uint32_t ld);
+
+int32_t tanb_engine_synchronize(tanb_engine* engine);
+void* tanb_engine_stream(tanb_engine* engine);
+
+/* out[0] sessions, out[1] channels, out[2] slot high-water mark, out[3] work
+ * items high-water mark, out[4] arena bytes in use, out[5] budget, out[6]
+ * algorithmic tail bytes per block, out[7] tail grid size. */
+int32_t tanb_engine_info(tanb_engine* engine, int64_t out[8]);
+
+/* Device-time accounting of tanb_engine_process_device: counts[0] heads,
+ * counts[1] tails, counts[2] IR updates, counts[3] timed blocks; ms[0] head,
+ * ms[1] tail device milliseconds. Reading resets. */
+int32_t tanb_engine_profile(tanb_engine* engine, int32_t enable);
+int32_t tanb_engine_profile_read(tanb_engine* engine, int64_t counts[4], double ms[2]);
+
 /* No reference counterpart: text of the last error raised on this thread. */
 const char* tanb_last_error(void);
 

@@ -86,6 +86,20 @@ SIGNATURES = {
     "tanb_convolution_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_convolution_profile": (_i32, [_vp, _i32]),
     "tanb_convolution_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
+    "tanb_engine_create": (_i32, [_vp, _u32, _u32, ctypes.c_uint64, _u32, _u32, ctypes.POINTER(_vp)]),
+    "tanb_engine_release": (_i32, [_vp]),
+    "tanb_engine_open_session": (_i32, [_vp, _u32, _u32, ctypes.POINTER(ctypes.c_int32), _u32p]),
+    "tanb_engine_close_session": (_i32, [_vp, _i32]),
+    "tanb_engine_update_response_td": (_i32, [_vp, _i32, _pp, _sz]),
+    "tanb_engine_io": (_i32, [_vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
+                              ctypes.POINTER(ctypes.POINTER(ctypes.c_float))]),
+    "tanb_engine_process": (_i32, [_vp]),
+    "tanb_engine_process_device": (_i32, [_vp, _vp, _vp, _u32]),
+    "tanb_engine_synchronize": (_i32, [_vp]),
+    "tanb_engine_stream": (_vp, [_vp]),
+    "tanb_engine_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "tanb_engine_profile": (_i32, [_vp, _i32]),
+    "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_last_error": (ctypes.c_char_p, []),
 }
 

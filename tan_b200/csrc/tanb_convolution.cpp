@@ -31,6 +31,12 @@ namespace {
 
 thread_local std::string g_last_error;
 
+}  // namespace
+
+void tanb::set_last_error(const char* msg) { g_last_error = msg; }
+
+namespace {
+
 int32_t fail(int32_t code, const char* fmt, ...) {
   char buf[512];
   va_list ap;
@@ -56,10 +62,6 @@ constexpr uint32_t kFlush = TANB_CHANNEL_FLAG_FLUSH_STREAM;
 enum class Mem { Host, Device };
 
 }  // namespace
-
-struct tanb_context {
-  int device = 0;
-};
 
 struct tanb_convolution {
   tanb_context* ctx = nullptr;

@@ -1,0 +1,583 @@
+// Batched engine behind the tanb_engine_* entry points of include/tanb.h.
+//
+// Many sessions (each the equivalent of one TANConvolution object: C channels,
+// IR length L) share one block size and one CUDA stream. A session's IR spectra,
+// delay line, overlap-save history and tail partial sums live in a
+// device-memory arena sized by the caller's budget; opening a session that does
+// not fit is refused with AMF_OUT_OF_MEMORY (admission by memory budget).
+//
+// Per audio block one CUDA graph runs: input copy (pinned -> device), the head
+// kernel over every channel slot, output copy, then the persistent tail kernel
+// over every work item for the next block. The graph is re-instantiated only
+// when the high-water marks of channel slots or work items change.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tanb.h"
+#include "tanb_engine.h"
+#include "tanb_internal.h"
+
+using tanb::EngChan;
+using tanb::EngItem;
+using tanb::EngUpd;
+
+namespace {
+
+int32_t efail(int32_t code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  tanb::set_last_error(buf);
+  return code;
+}
+
+#define ENG_CUDA(expr)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return efail(e_ == cudaErrorMemoryAllocation ? TANB_OUT_OF_MEMORY : TANB_FAIL,      \
+                   "%s failed: %s", #expr, cudaGetErrorString(e_));                      \
+  } while (0)
+
+constexpr size_t kAlign = 256;
+
+size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+// First-fit range allocator with coalescing (offsets in arbitrary units).
+class RangeAlloc {
+ public:
+  void reset(size_t size) {
+    free_.clear();
+    if (size) free_[0] = size;
+    size_ = size;
+  }
+  bool alloc(size_t n, size_t* off) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= n) {
+        *off = it->first;
+        size_t rest = it->second - n;
+        size_t start = it->first + n;
+        free_.erase(it);
+        if (rest) free_[start] = rest;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t n) {
+    if (!n) return;
+    auto it = free_.emplace(off, n).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) {
+      it->second += next->second;
+      free_.erase(next);
+    }
+    if (it != free_.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) {
+        prev->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  // one past the highest allocated unit
+  size_t high_water() const {
+    if (free_.empty()) return size_;
+    auto last = std::prev(free_.end());
+    return (last->first + last->second == size_) ? last->first : size_;
+  }
+
+ private:
+  std::map<size_t, size_t> free_;
+  size_t size_ = 0;
+};
+
+struct Session {
+  int id = -1;
+  int C = 0, L = 0, P = 0, nitem = 0;
+  size_t slot0 = 0, item0 = 0;
+  size_t arena_off = 0, arena_bytes = 0;
+};
+
+}  // namespace
+
+struct tanb_engine {
+  tanb_context* ctx = nullptr;
+  std::mutex mu;
+  int B = 0, log2B = 0, spec = 0, Q = 32;
+  size_t budget = 0, max_channels = 0, max_items = 0;
+  cudaStream_t stream = nullptr;
+  char* arena = nullptr;
+  RangeAlloc arena_alloc, slot_alloc, item_alloc;
+  EngChan* d_chans = nullptr;
+  EngChan* h_chans = nullptr;
+  EngItem* d_items = nullptr;
+  EngItem* h_items = nullptr;
+  float* h_in = nullptr;
+  float* h_out = nullptr;
+  float* d_in = nullptr;
+  float* d_out = nullptr;
+  float* h_ir = nullptr;
+  float* d_ir = nullptr;
+  size_t ir_cap = 0;
+  EngUpd* h_upd = nullptr;
+  EngUpd* d_upd = nullptr;
+  float2* d_tw = nullptr;
+  int tail_grid = 0;
+  size_t nslots_hwm = 0, nitems_hwm = 0;
+  size_t graph_slots = (size_t)-1, graph_items = (size_t)-1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaEvent_t ev_out = nullptr;
+  std::map<int, Session> sessions;
+  int next_id = 1;
+  // accounting
+  bool profiling = false;
+  cudaEvent_t pa = nullptr, pb = nullptr, pc = nullptr;
+  double ms_head = 0, ms_tail = 0;
+  int64_t n_head = 0, n_tail = 0, n_ir = 0, n_timed = 0;
+};
+
+namespace {
+
+size_t spec_bytes(int spec) { return spec == tanb::kSpecFP32 ? 8 : 4; }
+
+size_t session_bytes(const tanb_engine* e, int C, int P, int nitem) {
+  const size_t B = e->B;
+  size_t per = align_up(2 * (size_t)P * B * spec_bytes(e->spec));        // H
+  if (e->spec != tanb::kSpecFP32) per += align_up(2 * (size_t)P * 4);     // scales
+  per += align_up((size_t)P * B * 8);                                    // fdl
+  per += align_up(B * 4);                                                // prev
+  per += align_up(2 * (size_t)nitem * B * 8);                            // partials
+  return per * C;
+}
+
+void destroy_graph(tanb_engine* e) {
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->graph_exec = nullptr;
+  e->graph = nullptr;
+  e->graph_slots = e->graph_items = (size_t)-1;
+}
+
+void free_engine(tanb_engine* e) {
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  destroy_graph(e);
+  cudaFree(e->arena);
+  cudaFree(e->d_chans);
+  cudaFree(e->d_items);
+  cudaFree(e->d_in);
+  cudaFree(e->d_out);
+  cudaFree(e->d_ir);
+  cudaFree(e->d_upd);
+  cudaFree(e->d_tw);
+  cudaFreeHost(e->h_chans);
+  cudaFreeHost(e->h_items);
+  cudaFreeHost(e->h_in);
+  cudaFreeHost(e->h_out);
+  cudaFreeHost(e->h_ir);
+  cudaFreeHost(e->h_upd);
+  if (e->ev_out) cudaEventDestroy(e->ev_out);
+  if (e->pa) cudaEventDestroy(e->pa);
+  if (e->pb) cudaEventDestroy(e->pb);
+  if (e->pc) cudaEventDestroy(e->pc);
+  if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+cudaError_t upload_chans(tanb_engine* e, size_t first, size_t n) {
+  if (!n) return cudaSuccess;
+  return cudaMemcpyAsync(e->d_chans + first, e->h_chans + first, n * sizeof(EngChan), cudaMemcpyHostToDevice,
+                         e->stream);
+}
+
+cudaError_t upload_items(tanb_engine* e, size_t first, size_t n) {
+  if (!n) return cudaSuccess;
+  return cudaMemcpyAsync(e->d_items + first, e->h_items + first, n * sizeof(EngItem), cudaMemcpyHostToDevice,
+                         e->stream);
+}
+
+void update_hwm(tanb_engine* e) {
+  e->nslots_hwm = e->slot_alloc.high_water();
+  e->nitems_hwm = e->item_alloc.high_water();
+}
+
+// Enqueues one block: head over all slots, output copy (host mode), tail.
+cudaError_t enqueue_block(tanb_engine* e, const float* in, float* out, size_t ld, bool host) {
+  cudaError_t r;
+  if (host && e->nslots_hwm) {
+    r = cudaMemcpyAsync(e->d_in, e->h_in, e->nslots_hwm * e->B * sizeof(float), cudaMemcpyHostToDevice, e->stream);
+    if (r != cudaSuccess) return r;
+  }
+  r = tanb::eng_launch_head(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, in, out, (int)ld, e->d_tw,
+                            e->stream);
+  if (r != cudaSuccess) return r;
+  if (host && e->nslots_hwm) {
+    r = cudaMemcpyAsync(e->h_out, e->d_out, e->nslots_hwm * e->B * sizeof(float), cudaMemcpyDeviceToHost,
+                        e->stream);
+    if (r != cudaSuccess) return r;
+  }
+  if ((r = cudaEventRecord(e->ev_out, e->stream)) != cudaSuccess) return r;
+  return tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, 0, (int)e->nitems_hwm, 0, e->tail_grid,
+                               e->stream);
+}
+
+cudaError_t ensure_graph(tanb_engine* e) {
+  if (e->graph_exec && e->graph_slots == e->nslots_hwm && e->graph_items == e->nitems_hwm) return cudaSuccess;
+  destroy_graph(e);
+  cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+  if (r != cudaSuccess) return r;
+  cudaError_t r2 = enqueue_block(e, e->d_in, e->d_out, e->B, true);
+  r = cudaStreamEndCapture(e->stream, &e->graph);
+  if (r2 != cudaSuccess) return r2;
+  if (r != cudaSuccess) return r;
+  r = cudaGraphInstantiate(&e->graph_exec, e->graph, 0);
+  if (r != cudaSuccess) return r;
+  e->graph_slots = e->nslots_hwm;
+  e->graph_items = e->nitems_hwm;
+  return cudaSuccess;
+}
+
+// Host mirror of what the head kernel does to the channel table.
+void advance_mirror(tanb_engine* e) {
+  for (auto& kv : e->sessions) {
+    const Session& s = kv.second;
+    for (int j = 0; j < s.C; ++j) {
+      EngChan& ch = e->h_chans[s.slot0 + j];
+      ch.cur = (ch.cur - 1 + ch.P) % ch.P;
+      if (ch.pending) {
+        ch.active = 1 - ch.active;
+        ch.pending = 0;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum, uint64_t budget_bytes,
+                           uint32_t max_channels, uint32_t partitions_per_item, tanb_engine** out) {
+  if (!ctx || !out) return efail(TANB_INVALID_POINTER, "null argument");
+  *out = nullptr;
+  if (block < 128 || block > 2048 || (block & (block - 1)))
+    return efail(TANB_INVALID_ARG, "engine block must be a power of two in [128, 2048]");
+  if (spectrum > tanb::kSpecBF16) return efail(TANB_INVALID_ARG, "unknown spectrum type %u", spectrum);
+  if (max_channels == 0) return efail(TANB_INVALID_ARG, "max_channels == 0");
+  if (partitions_per_item == 0) partitions_per_item = 32;
+  tanb_engine* e = new tanb_engine();
+  e->ctx = ctx;
+  e->B = (int)block;
+  while ((1 << e->log2B) < e->B) ++e->log2B;
+  e->spec = (int)spectrum;
+  e->Q = (int)partitions_per_item;
+  e->budget = budget_bytes;
+  e->max_channels = max_channels;
+  e->max_items = (size_t)max_channels * 64;
+  cudaError_t r = cudaSetDevice(ctx->device);
+  if (r == cudaSuccess) r = tanb::eng_prepare();
+  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  const size_t io = e->max_channels * e->B;
+  if (r == cudaSuccess) r = cudaMalloc(&e->arena, std::max<size_t>(budget_bytes, kAlign));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_chans, e->max_channels * sizeof(EngChan));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_items, e->max_items * sizeof(EngItem));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_in, io * sizeof(float));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_out, io * sizeof(float));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_upd, e->max_channels * sizeof(EngUpd));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_tw, 2 * e->B * sizeof(float2));
+  if (r == cudaSuccess) r = cudaMallocHost(&e->h_chans, e->max_channels * sizeof(EngChan));
+  if (r == cudaSuccess) r = cudaMallocHost(&e->h_items, e->max_items * sizeof(EngItem));
+  if (r == cudaSuccess) r = cudaMallocHost(&e->h_in, io * sizeof(float));
+  if (r == cudaSuccess) r = cudaMallocHost(&e->h_out, io * sizeof(float));
+  if (r == cudaSuccess) r = cudaMallocHost(&e->h_upd, e->max_channels * sizeof(EngUpd));
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreate(&e->pa);
+  if (r == cudaSuccess) r = cudaEventCreate(&e->pb);
+  if (r == cudaSuccess) r = cudaEventCreate(&e->pc);
+  if (r != cudaSuccess) {
+    free_engine(e);
+    delete e;
+    cudaGetLastError();
+    return efail(r == cudaErrorMemoryAllocation ? TANB_OUT_OF_MEMORY : TANB_FAIL, "engine setup: %s",
+                 cudaGetErrorString(r));
+  }
+  std::memset(e->h_chans, 0, e->max_channels * sizeof(EngChan));
+  for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0};
+  std::memset(e->h_in, 0, io * sizeof(float));
+  e->arena_alloc.reset(budget_bytes / kAlign);
+  e->slot_alloc.reset(e->max_channels);
+  e->item_alloc.reset(e->max_items);
+  std::vector<float2> tw(2 * e->B);
+  tanb::make_twiddles(2 * e->B, tw.data());
+  r = cudaMemcpyAsync(e->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, e->stream);
+  if (r == cudaSuccess) r = cudaMemsetAsync(e->d_chans, 0, e->max_channels * sizeof(EngChan), e->stream);
+  if (r == cudaSuccess) r = upload_items(e, 0, e->max_items);
+  if (r == cudaSuccess) r = cudaMemsetAsync(e->d_in, 0, io * sizeof(float), e->stream);
+  if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
+  int sms = 148, per_sm = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  per_sm = std::max(1, 2048 / (e->B / 2));
+  e->tail_grid = sms * per_sm;
+  if (r != cudaSuccess) {
+    free_engine(e);
+    delete e;
+    return efail(TANB_FAIL, "engine init: %s", cudaGetErrorString(r));
+  }
+  *out = e;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_release(tanb_engine* e) {
+  if (!e) return TANB_OK;
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    cudaSetDevice(e->ctx->device);
+    free_engine(e);
+  }
+  delete e;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, int32_t* session,
+                                 uint32_t* first_slot) {
+  if (!e || !session) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(e->mu);
+  if (channels == 0 || ir_length == 0) return efail(TANB_INVALID_ARG, "channels and IR length must be > 0");
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  Session s;
+  s.C = (int)channels;
+  s.L = (int)ir_length;
+  s.P = (int)std::max<uint32_t>(1, (ir_length + e->B - 1) / e->B);
+  s.nitem = s.P > 1 ? (s.P - 1 + e->Q - 1) / e->Q : 0;
+  s.arena_bytes = session_bytes(e, s.C, s.P, s.nitem);
+  if (!e->arena_alloc.alloc(s.arena_bytes / kAlign, &s.arena_off))
+    return efail(TANB_OUT_OF_MEMORY, "session of %u channels x %u taps needs %zu bytes; device budget exhausted",
+                 channels, ir_length, s.arena_bytes);
+  if (!e->slot_alloc.alloc(s.C, &s.slot0)) {
+    e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
+    return efail(TANB_OUT_OF_MEMORY, "no %u free channel slots", channels);
+  }
+  const size_t nit_total = (size_t)s.C * s.nitem;
+  if (nit_total && !e->item_alloc.alloc(nit_total, &s.item0)) {
+    e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
+    e->slot_alloc.release(s.slot0, s.C);
+    return efail(TANB_OUT_OF_MEMORY, "work-item table full");
+  }
+  ENG_CUDA(cudaStreamSynchronize(e->stream));  // pinned mirrors are rewritten below
+  char* base = e->arena + s.arena_off * kAlign;
+  ENG_CUDA(cudaMemsetAsync(base, 0, s.arena_bytes, e->stream));
+  const size_t B = e->B;
+  for (int j = 0; j < s.C; ++j) {
+    EngChan ch{};
+    ch.H = base;
+    base += align_up(2 * (size_t)s.P * B * spec_bytes(e->spec));
+    if (e->spec != tanb::kSpecFP32) {
+      ch.scale = reinterpret_cast<float*>(base);
+      base += align_up(2 * (size_t)s.P * 4);
+    }
+    ch.fdl = reinterpret_cast<float2*>(base);
+    base += align_up((size_t)s.P * B * 8);
+    ch.prev = reinterpret_cast<float*>(base);
+    base += align_up(B * 4);
+    ch.part = reinterpret_cast<float2*>(base);
+    base += align_up(2 * (size_t)s.nitem * B * 8);
+    ch.P = s.P;
+    ch.nitem = s.nitem;
+    ch.cur = 0;
+    ch.active = 0;
+    ch.pending = 0;
+    ch.run = 1;
+    e->h_chans[s.slot0 + j] = ch;
+    for (int r = 0; r < s.nitem; ++r) {
+      const int i0 = 1 + r * e->Q;
+      e->h_items[s.item0 + (size_t)j * s.nitem + r] = EngItem{(int)(s.slot0 + j), i0, std::min(s.P, i0 + e->Q), r};
+    }
+  }
+  ENG_CUDA(upload_chans(e, s.slot0, s.C));
+  ENG_CUDA(upload_items(e, s.item0, nit_total));
+  s.id = e->next_id++;
+  e->sessions[s.id] = s;
+  update_hwm(e);
+  *session = s.id;
+  if (first_slot) *first_slot = (uint32_t)s.slot0;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
+  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->sessions.find(session);
+  if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  ENG_CUDA(cudaStreamSynchronize(e->stream));
+  const Session s = it->second;
+  for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j] = EngChan{};
+  const size_t nit_total = (size_t)s.C * s.nitem;
+  for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0};
+  ENG_CUDA(upload_chans(e, s.slot0, s.C));
+  ENG_CUDA(upload_items(e, s.item0, nit_total));
+  e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
+  e->slot_alloc.release(s.slot0, s.C);
+  e->item_alloc.release(s.item0, nit_total);
+  e->sessions.erase(it);
+  update_hwm(e);
+  return TANB_OK;
+}
+
+int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const float* const* ir, size_t n) {
+  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->sessions.find(session);
+  if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
+  const Session& s = it->second;
+  if (!ir) return efail(TANB_INVALID_ARG, "ppBuffer == NULL");
+  if (n > (size_t)s.L) return efail(TANB_INVALID_ARG, "IR length %zu exceeds the session's %d", n, s.L);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  ENG_CUDA(cudaStreamSynchronize(e->stream));  // staging reuse
+  const size_t PB = (size_t)s.P * e->B;
+  const size_t need = PB * s.C;
+  if (need > e->ir_cap) {
+    cudaFree(e->d_ir);
+    cudaFreeHost(e->h_ir);
+    e->d_ir = nullptr;
+    e->h_ir = nullptr;
+    e->ir_cap = 0;
+    ENG_CUDA(cudaMalloc(&e->d_ir, need * sizeof(float)));
+    ENG_CUDA(cudaMallocHost(&e->h_ir, need * sizeof(float)));
+    e->ir_cap = need;
+  }
+  for (int j = 0; j < s.C; ++j) {
+    if (!ir[j] && n) return efail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", j);
+    float* row = e->h_ir + (size_t)j * PB;
+    if (n) std::memcpy(row, ir[j], n * sizeof(float));
+    std::memset(row + n, 0, (PB - n) * sizeof(float));
+    EngChan& ch = e->h_chans[s.slot0 + j];
+    e->h_upd[j] = EngUpd{(int)(s.slot0 + j), 1 - ch.active, (int64_t)PB};
+    ch.pending = 1;
+  }
+  ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, need * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+  ENG_CUDA(cudaMemcpyAsync(e->d_upd, e->h_upd, s.C * sizeof(EngUpd), cudaMemcpyHostToDevice, e->stream));
+  ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_ir, e->d_upd, s.C, s.P, e->d_tw, e->stream));
+  e->n_ir += 1;
+  // tail of the new IR for the coming block, from the current delay line
+  if (s.nitem)
+    ENG_CUDA(tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, s.C * s.nitem, 1,
+                                   std::min(e->tail_grid, s.C * s.nitem), e->stream));
+  return TANB_OK;
+}
+
+int32_t tanb_engine_io(tanb_engine* e, float** in, float** out) {
+  if (!e || !in || !out) return efail(TANB_INVALID_POINTER, "null argument");
+  *in = e->h_in;
+  *out = e->h_out;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_process(tanb_engine* e) {
+  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  std::lock_guard<std::mutex> lock(e->mu);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
+  ENG_CUDA(ensure_graph(e));
+  ENG_CUDA(cudaGraphLaunch(e->graph_exec, e->stream));
+  ENG_CUDA(cudaEventSynchronize(e->ev_out));
+  e->n_head += 1;
+  e->n_tail += e->nitems_hwm ? 1 : 0;
+  advance_mirror(e);
+  return TANB_OK;
+}
+
+int32_t tanb_engine_process_device(tanb_engine* e, const float* in, float* out, uint32_t ld) {
+  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  std::lock_guard<std::mutex> lock(e->mu);
+  if (!out) return efail(TANB_INVALID_ARG, "null output");
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
+  if (ld == 0) ld = e->B;
+  if (e->profiling) ENG_CUDA(cudaEventRecord(e->pa, e->stream));
+  ENG_CUDA(tanb::eng_launch_head(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, in, out, (int)ld, e->d_tw,
+                                 e->stream));
+  if (e->profiling) ENG_CUDA(cudaEventRecord(e->pb, e->stream));
+  ENG_CUDA(tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, 0, (int)e->nitems_hwm, 0,
+                                 e->tail_grid, e->stream));
+  if (e->profiling) {
+    ENG_CUDA(cudaEventRecord(e->pc, e->stream));
+    ENG_CUDA(cudaEventSynchronize(e->pc));
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, e->pa, e->pb);
+    cudaEventElapsedTime(&b, e->pb, e->pc);
+    e->ms_head += a;
+    e->ms_tail += b;
+    e->n_timed += 1;
+  }
+  e->n_head += 1;
+  e->n_tail += e->nitems_hwm ? 1 : 0;
+  advance_mirror(e);
+  return TANB_OK;
+}
+
+int32_t tanb_engine_synchronize(tanb_engine* e) {
+  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  std::lock_guard<std::mutex> lock(e->mu);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  ENG_CUDA(cudaStreamSynchronize(e->stream));
+  return TANB_OK;
+}
+
+void* tanb_engine_stream(tanb_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
+  if (!e || !out) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(e->mu);
+  int64_t chans = 0, bytes = 0, tail_bytes = 0;
+  for (auto& kv : e->sessions) {
+    const Session& s = kv.second;
+    chans += s.C;
+    bytes += (int64_t)s.arena_bytes;
+    // per block: (P-1) partitions x B bins of IR spectrum + delay line, plus partial rows
+    tail_bytes += (int64_t)s.C * ((int64_t)(s.P - 1) * e->B * (int64_t)(spec_bytes(e->spec) + 8) +
+                                  (int64_t)s.nitem * e->B * 8);
+  }
+  out[0] = (int64_t)e->sessions.size();
+  out[1] = chans;
+  out[2] = (int64_t)e->nslots_hwm;
+  out[3] = (int64_t)e->nitems_hwm;
+  out[4] = bytes;
+  out[5] = (int64_t)e->budget;
+  out[6] = tail_bytes;
+  out[7] = e->tail_grid;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_profile(tanb_engine* e, int32_t enable) {
+  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  std::lock_guard<std::mutex> lock(e->mu);
+  e->profiling = enable != 0;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_profile_read(tanb_engine* e, int64_t counts[4], double ms[2]) {
+  if (!e || !counts || !ms) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(e->mu);
+  counts[0] = e->n_head;
+  counts[1] = e->n_tail;
+  counts[2] = e->n_ir;
+  counts[3] = e->n_timed;
+  ms[0] = e->ms_head;
+  ms[1] = e->ms_tail;
+  e->n_head = e->n_tail = e->n_ir = e->n_timed = 0;
+  e->ms_head = e->ms_tail = 0;
+  return TANB_OK;
+}
+
+}  // extern "C"

@@ -5,7 +5,15 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// A TAN context: the CUDA device its objects run on.
+struct tanb_context {
+  int device = 0;
+};
+
 namespace tanb {
+
+// Records the text returned by tanb_last_error() on this thread.
+void set_last_error(const char* msg);
 
 // Per-channel control word for one audio block, uploaded with the block's input.
 //   run       channel is processed this block (reference: !m_availableChannels[c])

@@ -1,0 +1,105 @@
+"""Python mirror of the batched engine (tanb_engine_* in include/tanb.h).
+
+A session is the equivalent of one TANConvolution object (C channels, IR
+length L); every open session advances by one block per `process()` call, all
+of them in one head and one tail launch. I/O goes through the engine's pinned
+host buffers, exposed here as numpy views shaped (max_channels, block).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .convolution import AMF_OK, TANContext, TANError, lib
+
+SPECTRUM_FP32 = 0
+SPECTRUM_FP16 = 1
+SPECTRUM_BF16 = 2
+
+
+class Session:
+    def __init__(self, engine: "Engine", sid: int, first_slot: int, channels: int, ir_length: int):
+        self.engine, self.id, self.first_slot = engine, sid, first_slot
+        self.channels, self.ir_length = channels, ir_length
+
+    @property
+    def slots(self) -> slice:
+        return slice(self.first_slot, self.first_slot + self.channels)
+
+    def update_response_td(self, ir: np.ndarray) -> int:
+        ir = np.ascontiguousarray(ir, dtype=np.float32)
+        rows = (ctypes.c_void_p * self.channels)(*[ir[c].ctypes.data for c in range(self.channels)])
+        return lib().tanb_engine_update_response_td(self.engine._h, self.id, rows, ir.shape[1])
+
+    def close(self) -> int:
+        return lib().tanb_engine_close_session(self.engine._h, self.id)
+
+
+class Engine:
+    def __init__(self, ctx: TANContext, block: int, spectrum: int = SPECTRUM_FP32, budget_bytes: int = 1 << 30,
+                 max_channels: int = 1024, partitions_per_item: int = 32):
+        h = ctypes.c_void_p()
+        rc = lib().tanb_engine_create(ctx._h, block, spectrum, budget_bytes, max_channels, partitions_per_item,
+                                      ctypes.byref(h))
+        if rc != AMF_OK:
+            raise TANError(rc, "tanb_engine_create")
+        self._h = h
+        self._ctx = ctx
+        self.block = block
+        self.max_channels = max_channels
+        pin = ctypes.POINTER(ctypes.c_float)()
+        pout = ctypes.POINTER(ctypes.c_float)()
+        lib().tanb_engine_io(h, ctypes.byref(pin), ctypes.byref(pout))
+        n = max_channels * block
+        self.inp = np.ctypeslib.as_array(pin, shape=(n,)).reshape(max_channels, block)
+        self.out = np.ctypeslib.as_array(pout, shape=(n,)).reshape(max_channels, block)
+
+    def release(self):
+        if self._h:
+            lib().tanb_engine_release(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def open_session(self, channels: int, ir_length: int):
+        """Returns (AMF_RESULT, Session or None)."""
+        sid = ctypes.c_int32(0)
+        first = ctypes.c_uint32(0)
+        rc = lib().tanb_engine_open_session(self._h, channels, ir_length, ctypes.byref(sid), ctypes.byref(first))
+        if rc != AMF_OK:
+            return rc, None
+        return rc, Session(self, sid.value, first.value, channels, ir_length)
+
+    def process(self) -> int:
+        return lib().tanb_engine_process(self._h)
+
+    def process_device(self, d_in: int, d_out: int, ld: int = 0) -> int:
+        return lib().tanb_engine_process_device(self._h, d_in, d_out, ld)
+
+    def synchronize(self) -> int:
+        return lib().tanb_engine_synchronize(self._h)
+
+    def stream(self) -> int:
+        return lib().tanb_engine_stream(self._h) or 0
+
+    def info(self) -> dict:
+        out = (ctypes.c_int64 * 8)()
+        lib().tanb_engine_info(self._h, out)
+        keys = ("sessions", "channels", "slot_hwm", "item_hwm", "arena_bytes", "budget", "tail_bytes_per_block",
+                "tail_grid")
+        return dict(zip(keys, list(out)))
+
+    def profile(self, enable: bool) -> int:
+        return lib().tanb_engine_profile(self._h, 1 if enable else 0)
+
+    def profile_read(self) -> dict:
+        counts = (ctypes.c_int64 * 4)()
+        ms = (ctypes.c_double * 2)()
+        lib().tanb_engine_profile_read(self._h, counts, ms)
+        return {"heads": counts[0], "tails": counts[1], "ir_updates": counts[2], "timed": counts[3],
+                "head_ms": ms[0], "tail_ms": ms[1]}
