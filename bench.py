@@ -11,7 +11,7 @@ pre-generated IR sets are cycled). One step = one audio block of every channel.
 ours (default):
   value  GSamples/s with inputs and IRs resident in HBM (device-pointer Process
          and UpdateResponseTD), device time from CUDA events on the object's
-         stream, L2 flushed (256 MiB memset) before every timed step.
+         stream, L2 flushed (256 MiB write + read) before every timed step.
   e2e    the same metric through the host C ABI (tanb_convolution_process with
          host float* rows, H2D + D2H inside), wall clock per step including the
          tail kernel; p50/p99/p99.9 of the per-block latency (Process return).
@@ -261,6 +261,7 @@ def hbm_peak():
 def run_ours(args):
     import torch
 
+    from tan_b200 import autotune
     from tan_b200 import convolution as cv
 
     world, rank, local, pg = dist_setup(args)
@@ -273,15 +274,22 @@ def run_ours(args):
     ctx = cv.TANContext(dev)
 
     # ---- device-resident pass (value + roofline) --------------------------
-    conv = cv.TANConvolution(ctx)
-    rc = conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C)
-    assert rc == cv.AMF_OK, cv.last_error()
+    conv = autotune.tuned(ctx, cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C)
     P = conv.info()["partitions"]
+    tiling = conv.tiling()[1]
     stream = torch.cuda.ExternalStream(conv.stream(), device=dev)
     x_dev = torch.from_numpy(x).to(f"cuda:{dev}")
     y_dev = torch.zeros((C, B * 2), dtype=torch.float32, device=f"cuda:{dev}")
     ir_dev = [torch.from_numpy(h).to(f"cuda:{dev}") for h in irs]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    flush_r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{dev}")
+
+    def flush_l2():
+        # write one buffer larger than L2, then read another, so no dirty lines
+        # of the flush are written back inside the timed step
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            flush_r.sum()
     row = x_dev.stride(0) * 4
     yrow = y_dev.stride(0) * 4
     torch.cuda.synchronize()
@@ -296,8 +304,7 @@ def run_ours(args):
         assert rc == 0 and done == B, cv.last_error()
 
     for k in range(args.warmup):
-        with torch.cuda.stream(stream):
-            flush.zero_()
+        flush_l2()
         dev_step(k)
     conv.Synchronize()
     conv.profile_read()
@@ -308,8 +315,7 @@ def run_ours(args):
     conv.profile(True)
     with ClockSampler(dev) as clk:
         for k in range(args.warmup, nblocks):
-            with torch.cuda.stream(stream):
-                flush.zero_()
+            flush_l2()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -335,17 +341,26 @@ def run_ours(args):
     del x_dev, y_dev, ir_dev
 
     # ---- end-to-end pass through the host C ABI ----------------------------
-    conv = cv.TANConvolution(ctx)
-    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == 0
+    import ctypes
+
+    conv = autotune.tuned(ctx, cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C)
     stream = torch.cuda.ExternalStream(conv.stream(), device=dev)
+    lib = cv.lib()
     y = np.zeros((C, B), np.float32)
     xs_blocks = [np.ascontiguousarray(x[:, j * B:(j + 1) * B]) for j in range(xblocks)]
+    # host row-pointer arrays built once, as a C caller would keep them
+    in_rows = [(ctypes.c_void_p * C)(*[xb[c].ctypes.data for c in range(C)]) for xb in xs_blocks]
+    out_rows = (ctypes.c_void_p * C)(*[y[c].ctypes.data for c in range(C)])
+    ir_rows = [(ctypes.c_void_p * C)(*[h[c].ctypes.data for c in range(C)]) for h in irs]
+    done = ctypes.c_size_t(0)
 
     def host_step(k):
         if k % SWAP_EVERY == 0:
-            assert conv.UpdateResponseTD(irs[(k // SWAP_EVERY) % N_IR_SETS], L) == 0
-        rc, done = conv.Process(xs_blocks[k % xblocks], y, B)
-        assert rc == 0 and done == B
+            rc = lib.tanb_convolution_update_response_td(conv._h, ir_rows[(k // SWAP_EVERY) % N_IR_SETS], L,
+                                                         None, 0)
+            assert rc == 0
+        rc = lib.tanb_convolution_process(conv._h, in_rows[k % xblocks], out_rows, B, None, ctypes.byref(done))
+        assert rc == 0 and done.value == B
 
     for k in range(args.warmup):
         host_step(k)
@@ -354,8 +369,7 @@ def run_ours(args):
     if pg:
         pg.barrier()
     for k in range(args.warmup, nblocks):
-        with torch.cuda.stream(stream):
-            flush.zero_()
+        flush_l2()
         conv.Synchronize()
         t0 = time.perf_counter()
         host_step(k)
@@ -385,12 +399,12 @@ def run_ours(args):
                            "p999": float(np.percentile(lat_ms, 99.9)), "deadline": deadline_ms,
                            "what": "host Process() call, H2D + head + D2H, per block"},
             "realtime_factor_p99": deadline_ms / p99,
-            "l2": "flushed before every timed step (256 MiB memset on the object's stream)",
+            "l2": "flushed before every timed step (256 MiB write + 256 MiB read on the object's stream)",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": read_traffic(),
                          "kernel": "tail_kernel (partition MAC)", "peak_source": f"{peak_kind} hbm_gbs",
                          "bytes_per_launch": bytes_per_tail, "avg_launch_us": tail_ms_avg * 1e3,
-                         "launches_timed": tail["timed"]},
+                         "launches_timed": tail["timed"], "tiling": list(tiling)},
             "kernel_ms": {k: v["ms"] for k, v in prof.items()},
             "e2e": {"value": e2e_value, "unit": "GSamples/s", "h2d_bytes_per_step": C * B * 4 + 32 * C,
                     "d2h_bytes_per_step": C * B * 4,

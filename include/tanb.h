@@ -29,6 +29,7 @@ enum {
   TANB_FAIL = 1,
   TANB_UNEXPECTED = 2,
   TANB_INVALID_ARG = 4,
+  TANB_OUT_OF_RANGE = 5,
   TANB_OUT_OF_MEMORY = 6,
   TANB_INVALID_POINTER = 7,
   TANB_NOT_IMPLEMENTED = 9,
@@ -203,6 +204,12 @@ void* tanb_convolution_stream(tanb_convolution* conv);
  * out[0] = partitions P, out[1] = block B, out[2] = channels C,
  * out[3] = device bytes held by the object. */
 int32_t tanb_convolution_info(tanb_convolution* conv, int64_t out[4]);
+
+/* No reference counterpart: autotuner hook. index >= 0 selects entry `index`
+ * of the tail kernel's compiled tilings (TANB_OUT_OF_RANGE past the last);
+ * index < 0 only reads. out (nullable) gets the tiling in use: units of two
+ * bins per CTA row, partition splits per CTA, partitions in flight per thread. */
+int32_t tanb_convolution_tiling(tanb_convolution* conv, int32_t index, int32_t out[3]);
 
 /* No reference counterpart: per-kernel device-time accounting. With enable
  * != 0 every kernel this object launches is bracketed by a CUDA event pair on

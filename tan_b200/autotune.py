@@ -1,0 +1,123 @@
+"""Autotuner for the partition multiply-accumulate (the tail kernel).
+
+For one shape (block B, IR length L, channels C) it runs the convolution on the
+device with every compiled tail tiling, timing the tail kernel with CUDA events
+on the object's stream (L2 flushed before every timed block), and keeps the
+fastest. Results are cached in tuning.json next to this file, keyed by shape;
+TANConvolution objects created through `tuned()` apply the cached choice.
+
+    python -m tan_b200.autotune --block 512 --length 65536 --channels 64
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+import numpy as np
+
+from . import convolution as cv
+
+CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
+
+
+def key(B: int, L: int, C: int) -> str:
+    P = max(1, -(-L // B))
+    return f"B{B}_P{P}_C{C}"
+
+
+def load_cache() -> dict:
+    if os.path.exists(CACHE):
+        with open(CACHE) as f:
+            return json.load(f)
+    return {}
+
+
+def save_cache(d: dict) -> None:
+    with open(CACHE, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+
+
+def measure(ctx, B: int, L: int, C: int, steps: int = 40, warmup: int = 5, seed: int = 7):
+    """Returns [(index, (ux, sy, depth), mean tail us)] for every compiled tiling."""
+    import torch
+
+    g = np.random.Generator(np.random.PCG64(seed))
+    conv = cv.TANConvolution(ctx)
+    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == cv.AMF_OK, cv.last_error()
+    dev = ctx.device
+    h = torch.from_numpy((g.standard_normal((C, L)) * 0.01).astype(np.float32)).to(f"cuda:{dev}")
+    assert conv.UpdateResponseTDDevice(h, L) == 0
+    x = torch.from_numpy(g.uniform(-1, 1, (C, B)).astype(np.float32)).to(f"cuda:{dev}")
+    y = torch.zeros_like(x)
+    flush_w = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
+    flush_r = torch.ones(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
+    stream = torch.cuda.ExternalStream(conv.stream(), device=dev)
+    results = []
+    idx = 0
+    while True:
+        rc, tiling = conv.tiling(idx)
+        if rc != cv.AMF_OK:
+            break
+        if tiling[0] > B // 2:  # more units per CTA row than the block has bin pairs
+            idx += 1
+            continue
+        for k in range(warmup + steps):
+            if k == warmup:
+                conv.Synchronize()
+                conv.profile_read()
+                conv.profile(True)
+            with torch.cuda.stream(stream):
+                flush_w.zero_()
+                flush_r.sum()
+            rc, _ = conv.ProcessDevice(x, y, B)
+            assert rc == 0
+        conv.Synchronize()
+        conv.profile(False)
+        p = conv.profile_read()["tail"]
+        results.append((idx, tiling, 1000.0 * p["ms"] / max(1, p["timed"])))
+        idx += 1
+    conv.Release()
+    return results
+
+
+def tune(ctx, B: int, L: int, C: int, write: bool = True) -> dict:
+    res = measure(ctx, B, L, C)
+    best = min(res, key=lambda r: r[2])
+    P = max(1, -(-L // B))
+    bytes_per_launch = C * ((P - 1) * B * 16 + B * 8)
+    entry = {"index": best[0], "tiling": list(best[1]), "tail_us": best[2],
+             "gbs": bytes_per_launch / (best[2] * 1e-6) / 1e9,
+             "all": [{"index": i, "tiling": list(t), "tail_us": us} for i, t, us in res]}
+    if write:
+        d = load_cache()
+        d[key(B, L, C)] = entry
+        save_cache(d)
+    return entry
+
+
+def tuned(ctx, method: int, L: int, B: int, C: int) -> cv.TANConvolution:
+    """A TANConvolution initialised and set to the cached best tiling, if any."""
+    conv = cv.TANConvolution(ctx)
+    rc = conv.Init(method, L, B, C)
+    if rc != cv.AMF_OK:
+        raise cv.TANError(rc, "Init")
+    e = load_cache().get(key(B, L, C))
+    if e is not None:
+        conv.tiling(int(e["index"]))
+    return conv
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--block", type=int, default=512)
+    ap.add_argument("--length", type=int, default=65536)
+    ap.add_argument("--channels", type=int, default=64)
+    a = ap.parse_args()
+    ctx = cv.TANContext(0)
+    e = tune(ctx, a.block, a.length, a.channels)
+    print(json.dumps({key(a.block, a.length, a.channels): e}))
+
+
+if __name__ == "__main__":
+    main()

@@ -21,6 +21,7 @@ AMF_OK = 0
 AMF_FAIL = 1
 AMF_UNEXPECTED = 2
 AMF_INVALID_ARG = 4
+AMF_OUT_OF_RANGE = 5
 AMF_OUT_OF_MEMORY = 6
 AMF_INVALID_POINTER = 7
 AMF_NOT_IMPLEMENTED = 9
@@ -84,6 +85,7 @@ SIGNATURES = {
     "tanb_convolution_synchronize": (_i32, [_vp]),
     "tanb_convolution_stream": (_vp, [_vp]),
     "tanb_convolution_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "tanb_convolution_tiling": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_int32)]),
     "tanb_convolution_profile": (_i32, [_vp, _i32]),
     "tanb_convolution_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_engine_create": (_i32, [_vp, _u32, _u32, ctypes.c_uint64, _u32, _u32, ctypes.POINTER(_vp)]),
@@ -300,6 +302,12 @@ class TANConvolution:
 
     def stream(self) -> int:
         return lib().tanb_convolution_stream(self._h) or 0
+
+    def tiling(self, index: int = -1):
+        """Selects compiled tail tiling `index` (>= 0) and returns (AMF_RESULT, (ux, sy, depth))."""
+        out = (ctypes.c_int32 * 3)()
+        rc = lib().tanb_convolution_tiling(self._h, index, out)
+        return rc, tuple(out)
 
     def profile(self, enable: bool) -> int:
         return lib().tanb_convolution_profile(self._h, 1 if enable else 0)

@@ -95,6 +95,7 @@ struct tanb_convolution {
   // UpdateResponseTD staging: IR rows [C][P*B], then ChanCtl[C] + int[C]
   float* h_ir = nullptr;
   float* d_ir = nullptr;
+  int* h_err = nullptr;  // host-mapped error word written by kernels (DevState::err)
   uint8_t* h_uctl = nullptr;
   uint8_t* d_uctl = nullptr;
 
@@ -197,6 +198,8 @@ void free_all(tanb_convolution* v) {
   cudaFreeHost(v->h_out);
   cudaFreeHost(v->h_ir);
   cudaFreeHost(v->h_uctl);
+  cudaFreeHost(v->h_err);
+  v->h_err = nullptr;
   cudaFree(v->td_hist);
   cudaFree(v->td_ir);
   cudaFree(v->td_dir);
@@ -235,9 +238,9 @@ cudaError_t dev_alloc(tanb_convolution* v, T** p, size_t count) {
 
 MacTiling default_tiling(int B, int P) {
   const int U = B / 2;
-  if (P >= 256 && U >= 32) return {32, 16};
-  if (U >= 32) return {32, 8};
-  return {16, 16};
+  if (P >= 256 && U >= 32) return {32, 16, 4};
+  if (U >= 32) return {32, 8, 4};
+  return {16, 16, 4};
 }
 
 // Zeroes one channel's delay line, history and tails (intended flush semantics;
@@ -472,6 +475,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     }
     if (out_mem == Mem::Host) {
       TANB_CUDA(cudaEventSynchronize(v->ev_out));
+      if (*v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
       for (int b = 0; b < nb; ++b)
         for (int c = 0; c < C; ++c)
           if (run_b[b][c] && out[c])
@@ -787,6 +791,7 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
     if ((e = cudaMallocHost(&v->h_out, out_floats * sizeof(float))) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_ir, Cs * Ps * Bs * sizeof(float))) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_uctl, uctl_bytes)) != cudaSuccess) break;
+    if ((e = cudaHostAlloc(&v->h_err, sizeof(int), cudaHostAllocMapped)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_stage, cudaEventDisableTiming)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_ir, cudaEventDisableTiming)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_out, cudaEventDisableTiming)) != cudaSuccess) break;
@@ -814,6 +819,11 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
   v->ds.P = v->P;
   v->ds.C = C;
   v->ds.tw = v->d_tw;
+  *v->h_err = tanb::kErrNone;
+  if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&v->ds.err), v->h_err, 0)) != cudaSuccess) {
+    free_all(v);
+    return fail(TANB_FAIL, "mapped error word: %s", cudaGetErrorString(e));
+  }
   v->tiling = default_tiling(B, v->P);
   v->active.assign(C, 0);
   v->pending.assign(C, 0);
@@ -905,10 +915,24 @@ int32_t tanb_convolution_synchronize(tanb_convolution* v) {
   if (!v->initialized) return TANB_OK;
   TANB_CUDA(cudaSetDevice(v->ctx->device));
   TANB_CUDA(cudaStreamSynchronize(v->stream));
+  if (v->h_err && *v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
   return TANB_OK;
 }
 
 void* tanb_convolution_stream(tanb_convolution* v) { return v ? (void*)v->stream : nullptr; }
+
+int32_t tanb_convolution_tiling(tanb_convolution* v, int32_t index, int32_t out[3]) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (index >= tanb::mac_tiling_count()) return fail(TANB_OUT_OF_RANGE, "tiling index %d out of range", index);
+  if (index >= 0) v->tiling = tanb::mac_tiling(index);
+  if (out) {
+    out[0] = v->tiling.ux;
+    out[1] = v->tiling.sy;
+    out[2] = v->tiling.depth;
+  }
+  return TANB_OK;
+}
 
 int32_t tanb_convolution_profile(tanb_convolution* v, int32_t enable) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");

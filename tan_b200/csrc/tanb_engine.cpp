@@ -226,7 +226,9 @@ cudaError_t enqueue_block(tanb_engine* e, const float* in, float* out, size_t ld
                         e->stream);
     if (r != cudaSuccess) return r;
   }
-  if ((r = cudaEventRecord(e->ev_out, e->stream)) != cudaSuccess) return r;
+  // inside stream capture a plain record only marks a capture dependency; the
+  // external flag makes it an event-record node that fires on every launch
+  if ((r = cudaEventRecordWithFlags(e->ev_out, e->stream, cudaEventRecordExternal)) != cudaSuccess) return r;
   return tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, 0, (int)e->nitems_hwm, 0, e->tail_grid,
                                e->stream);
 }

@@ -25,16 +25,21 @@ __device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
 __device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
 
 // Threads per FFT block and complex values each thread holds per stage.
+// TW_SMEM: the 2M-entry twiddle table is staged in shared memory (it fits
+// beside two M-point work buffers up to M = 2048).
 template <int LOG2M>
 struct FftShape {
   static constexpr int M = 1 << LOG2M;
   static constexpr int T = (M / 4 > 1024) ? 1024 : M / 4;
   static constexpr int E = M / T;
+  static constexpr bool TW_SMEM = LOG2M <= 11;
+  // bin pairs (k, M-k), k in [0, M/2], handled per thread
+  static constexpr int KP = (M / 2 + 1 + T - 1) / T;
 };
 
 // In-place M-point complex FFT of s[0..M) (forward: exp(-i..), inverse:
-// exp(+i..), unscaled). Must be called by all FftShape<LOG2M>::T threads;
-// ends with a barrier.
+// exp(+i..), unscaled). `tw` may point to global or shared memory. Must be
+// called by all FftShape<LOG2M>::T threads; ends with a barrier.
 template <int LOG2M, bool INV>
 __device__ __forceinline__ void fft_inplace(float2* s, const float2* __restrict__ tw) {
   using S = FftShape<LOG2M>;
@@ -72,7 +77,7 @@ __device__ __forceinline__ void fft_inplace(float2* s, const float2* __restrict_
       v[4 * e] = s[j];
 #pragma unroll
       for (int r = 1; r < 4; ++r) {
-        float2 w = __ldg(tw + r * k * tstep);
+        float2 w = tw[r * k * tstep];
         if (INV) w.y = -w.y;
         v[4 * e + r] = c_mul(s[j + r * nb], w);
       }

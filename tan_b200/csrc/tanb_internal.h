@@ -40,18 +40,30 @@ struct DevState {
   float* prev;    // previous input  [C][B]     (overlap-save history)
   float2* tail;   // tails           [C][2][B]  ([0]: active IR, [1]: pending IR)
   const float2* tw;  // W_N^j, N = 2B, j in [0, N)
+  int* err;       // device-visible error word (host-mapped); nonzero after a
+                  // bounded wait in a kernel gave up (kErr* codes)
 };
+
+// Error codes a kernel writes to DevState::err.
+enum : int { kErrNone = 0, kErrBulkWaitTimeout = 1 };
 
 __host__ __device__ inline size_t h_index(const DevState& s, int c, int slot, int part) {
   return (((size_t)c * 2 + slot) * s.P + part) * s.B;
 }
 
 // Tiling of the tail multiply-accumulate: UX units (float4 = 2 bins) by SY
-// partition splits per CTA; UX * SY threads.
+// partition splits per CTA (UX * SY threads), each thread keeping `depth`
+// partitions' loads in flight.
 struct MacTiling {
-  int ux;
-  int sy;
+  int ux;         // kind 0: float4 units per CTA row; kind 1: bins per CTA / 2
+  int sy;         // kind 0: partition splits per CTA; kind 1: pipeline stages
+  int depth = 4;  // kind 0: partitions in flight per thread; kind 1: rows per stage
+  int kind = 0;   // 0: register loads (LDG.128); 1: cp.async.bulk into shared memory
 };
+
+// Tilings the tail kernel is compiled for (index -> MacTiling).
+int mac_tiling_count();
+MacTiling mac_tiling(int index);
 
 // R2C of each IR partition into slot `slot_new` of the channels listed in
 // `chans` (device array of nch channel indices). `ir` is [nch][P*B] floats,

@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
     head_kernel(DevState s, const ChanCtl* __restrict__ ctl, const float* const* __restrict__ inp,
                 float* const* __restrict__ outp, int cur) {
   using S = FftShape<LOG2M>;
-  constexpr int M = S::M, T = S::T;
+  constexpr int M = S::M, T = S::T, KP = S::KP;
   extern __shared__ float2 sm[];
   float2* z = sm;       // old / only IR
   float2* z2 = sm + M;  // new IR on a swap block
@@ -68,7 +68,33 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   const float* x = inp[c];
   float* y = outp[c];
   float* prev = s.prev + (size_t)c * M;
+  const float2* h0 = s.H + h_index(s, c, cc.slot_cur, 0);
+  const float2* h1 = s.H + h_index(s, c, cc.slot_new, 0);
+  const float2* t0 = s.tail + (size_t)c * 2 * M;
+  const float2* t1 = t0 + M;
 
+  // twiddles into shared memory (small transforms), coalesced float4 loads
+  const float2* tw = s.tw;
+  if constexpr (S::TW_SMEM) {
+    float2* tws = sm + 2 * M;
+    for (int j = threadIdx.x; j < M; j += T)
+      reinterpret_cast<float4*>(tws)[j] = __ldg(reinterpret_cast<const float4*>(s.tw) + j);
+    tw = tws;
+  }
+  // prefetch the tail and partition 0 of this thread's bin pairs; they do not
+  // depend on the transform, so their latency hides behind it
+  float2 pt[KP][2], ph[KP][2];
+#pragma unroll
+  for (int q = 0; q < KP; ++q) {
+    const int k = threadIdx.x + q * T;
+    if (k <= M / 2) {
+      const int km = (k == 0) ? 0 : M - k;
+      pt[q][0] = t0[k];
+      pt[q][1] = t0[km];
+      ph[q][0] = h0[k];
+      ph[q][1] = h0[km];
+    }
+  }
   // frame [x_{k-1}, x_k] packed as complex pairs
   for (int n = threadIdx.x; n < M; n += T) {
     const float* src = (n < M / 2) ? prev + 2 * n : (x ? x + 2 * (n - M / 2) : nullptr);
@@ -77,30 +103,29 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   __syncthreads();
   for (int n = threadIdx.x; n < M / 2; n += T) reinterpret_cast<float2*>(prev)[n] = z[n + M / 2];
 
-  fft_inplace<LOG2M, false>(z, s.tw);
+  fft_inplace<LOG2M, false>(z, tw);
 
   float2* F = s.fdl + ((size_t)c * s.P + cur) * M;
-  const float2* h0 = s.H + h_index(s, c, cc.slot_cur, 0);
-  const float2* h1 = s.H + h_index(s, c, cc.slot_new, 0);
-  const float2* t0 = s.tail + (size_t)c * 2 * M;
-  const float2* t1 = t0 + M;
   const float inv_n = 1.0f / (float)(2 * M);
-  for (int k = threadIdx.x; k <= M / 2; k += T) {
+#pragma unroll
+  for (int q = 0; q < KP; ++q) {
+    const int k = threadIdx.x + q * T;
+    if (k > M / 2) continue;
     if (k == 0) {
       const float2 X = rfft_post_dc(z[0]);
       F[0] = X;
-      z[0] = irfft_pre_dc(c_mac_dc(t0[0], X, h0[0]), inv_n);
+      z[0] = irfft_pre_dc(c_mac_dc(pt[q][0], X, ph[q][0]), inv_n);
       if (swap) z2[0] = irfft_pre_dc(c_mac_dc(t1[0], X, h1[0]), inv_n);
     } else {
       const int km = M - k;
-      const float2 wk = __ldg(s.tw + k), wm = __ldg(s.tw + km);
+      const float2 wk = tw[k], wm = tw[km];
       const float2 a = z[k], b = z[km];
       const float2 Xk = rfft_post(a, b, wk);
       const float2 Xm = rfft_post(b, a, wm);
       F[k] = Xk;
       if (km != k) F[km] = Xm;
-      const float2 Ak = c_mac(t0[k], Xk, h0[k]);
-      const float2 Am = c_mac(t0[km], Xm, h0[km]);
+      const float2 Ak = c_mac(pt[q][0], Xk, ph[q][0]);
+      const float2 Am = c_mac(pt[q][1], Xm, ph[q][1]);
       z[k] = irfft_pre(Ak, Am, wk, inv_n);
       if (km != k) z[km] = irfft_pre(Am, Ak, wm, inv_n);
       if (swap) {
@@ -112,8 +137,8 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
     }
   }
   __syncthreads();
-  fft_inplace<LOG2M, true>(z, s.tw);
-  if (swap) fft_inplace<LOG2M, true>(z2, s.tw);
+  fft_inplace<LOG2M, true>(z, tw);
+  if (swap) fft_inplace<LOG2M, true>(z2, tw);
 
   // overlap-save: samples [B, 2B) of the circular result are the output
   if (!y) return;
@@ -142,7 +167,7 @@ __device__ __forceinline__ float4 mac4(float4 acc, float4 f, float4 h, bool dc) 
   return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
 
-template <int UX, int SY>
+template <int UX, int SY, int D>
 __global__ void __launch_bounds__(UX* SY)
     tail_kernel(DevState s, const ChanCtl* __restrict__ ctl, int which, int cur) {
   const int c = blockIdx.y;
@@ -164,16 +189,16 @@ __global__ void __launch_bounds__(UX* SY)
     int fs = (cur + i0 - 1) % P;
     const bool dc = (u == 0);
     int i = i0;
-    for (; i + 4 <= i1; i += 4) {
-      float4 h[4], f[4];
+    for (; i + D <= i1; i += D) {
+      float4 h[D], f[D];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < D; ++q) {
         h[q] = __ldg(Hc + (size_t)(i + q) * U);
         f[q] = __ldg(Fc + (size_t)fs * U);
         fs = (fs + 1 == P) ? 0 : fs + 1;
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc = mac4(acc, f[q], h[q], dc);
+      for (int q = 0; q < D; ++q) acc = mac4(acc, f[q], h[q], dc);
     }
     for (; i < i1; ++i) {
       const float4 h = __ldg(Hc + (size_t)i * U);
@@ -199,12 +224,138 @@ __global__ void __launch_bounds__(UX* SY)
   if (u < U) reinterpret_cast<float4*>(s.tail + ((size_t)c * 2 + which) * s.B)[u] = acc;
 }
 
+// ---------------------------------------------------------------------------
+// Tail MAC with cp.async.bulk staging. One CTA per (channel, BR-bin slice):
+// thread 0 streams, for each chunk of RS partitions, the IR-spectrum and
+// delay-line row segments of the slice (BR x 8 bytes each, 16-byte aligned)
+// into stage (chunk mod NS) of a shared-memory ring and arms that stage's
+// mbarrier with the byte count; all BR/2 threads wait on the barrier, multiply
+// and accumulate their two bins from shared memory, then release the stage to
+// the next chunk. Up to NS x RS x BR x 16 bytes are in flight per CTA without
+// holding them in registers. Waits are bounded: on timeout the kernel records
+// kErrBulkWaitTimeout, waits (bounded) for its copies in flight and returns.
+// No multicast; every load reads this GPU's own memory.
+constexpr int kBulkWaitLimit = 1 << 20;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int it = 0; it < kBulkWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+template <int BR, int RS, int NS>
+__global__ void __launch_bounds__(BR / 2)
+    tail_bulk_kernel(DevState s, const ChanCtl* __restrict__ ctl, int which, int cur) {
+  constexpr int U = BR / 2;                     // threads = float4 units of the slice
+  constexpr uint32_t kRowBytes = BR * sizeof(float2);
+  extern __shared__ __align__(128) unsigned char bulk_smem[];
+  float4* hbuf = reinterpret_cast<float4*>(bulk_smem);             // [NS][RS][U]
+  float4* fbuf = hbuf + NS * RS * U;                                // [NS][RS][U]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(fbuf + NS * RS * U);  // [NS]
+  const int c = blockIdx.y;
+  const ChanCtl cc = ctl[c];
+  if (which == 0 ? !cc.run : !cc.swap) return;
+  const int slot = (which == 0) ? (cc.swap ? cc.slot_new : cc.slot_cur) : cc.slot_new;
+  const int P = s.P;
+  const int bin0 = blockIdx.x * BR;
+  const int tid = threadIdx.x;
+  const int nparts = P - 1;
+  const int nchunks = (nparts + RS - 1) / RS;
+  const float2* Hrow = s.H + h_index(s, c, slot, 0) + bin0;  // + i * B for partition i
+  const float2* Frow = s.fdl + (size_t)c * P * s.B + bin0;    // + slot * B
+
+  auto issue = [&](int q) {  // chunk q -> stage q % NS (thread 0 only)
+    const int st = q % NS;
+    const int i0 = 1 + q * RS;
+    const int rows = min(RS, P - i0);
+    const uint32_t bar = smem_addr(&bars[st]);
+    mbar_expect_tx(bar, 2u * rows * kRowBytes);
+    for (int r = 0; r < rows; ++r) {
+      const int i = i0 + r;
+      const int fs = (cur + i - 1) % P;
+      bulk_g2s(smem_addr(hbuf + (st * RS + r) * U), Hrow + (size_t)i * s.B, kRowBytes, bar);
+      bulk_g2s(smem_addr(fbuf + (st * RS + r) * U), Frow + (size_t)fs * s.B, kRowBytes, bar);
+    }
+  };
+
+  if (tid == 0) {
+    for (int st = 0; st < NS; ++st) mbar_init(smem_addr(&bars[st]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int q = 0; q < NS && q < nchunks; ++q) issue(q);
+
+  const bool dc = (bin0 == 0 && tid == 0);
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  bool ok = true;
+  int q = 0;
+  for (; q < nchunks; ++q) {
+    const int st = q % NS;
+    const uint32_t parity = (uint32_t)(q / NS) & 1u;
+    const bool landed = mbar_wait(smem_addr(&bars[st]), parity);
+    if (__syncthreads_or(!landed)) {  // CTA-uniform decision
+      ok = false;
+      break;
+    }
+    const int rows = min(RS, P - (1 + q * RS));
+    for (int r = 0; r < rows; ++r)
+      acc = mac4(acc, fbuf[(st * RS + r) * U + tid], hbuf[(st * RS + r) * U + tid], dc);
+    __syncthreads();  // every thread is done reading stage st
+    if (tid == 0 && q + NS < nchunks) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(q + NS);
+    }
+  }
+  if (!ok) {
+    // record the failure, then let copies already issued land before exiting
+    if (tid == 0) {
+      atomicExch(s.err, kErrBulkWaitTimeout);
+      for (int r = q; r < nchunks && r < q + NS; ++r) mbar_wait(smem_addr(&bars[r % NS]), (uint32_t)(r / NS) & 1u);
+    }
+    __syncthreads();
+    return;
+  }
+  reinterpret_cast<float4*>(s.tail + ((size_t)c * 2 + which) * s.B + bin0)[tid] = acc;
+}
+
+template <int BR, int RS, int NS>
+constexpr int bulk_smem_bytes() {
+  return 2 * NS * RS * BR * (int)sizeof(float2) + NS * 8;
+}
+
 template <int LOG2M>
 cudaError_t set_attrs() {
-  const int smem = 2 * (1 << LOG2M) * (int)sizeof(float2);
+  const int smem = (FftShape<LOG2M>::TW_SMEM ? 4 : 2) * (1 << LOG2M) * (int)sizeof(float2);
   cudaError_t e = cudaFuncSetAttribute(head_kernel<LOG2M>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(ir_spectrum_kernel<LOG2M>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem / 2);
+  return cudaFuncSetAttribute(ir_spectrum_kernel<LOG2M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (1 << LOG2M) * (int)sizeof(float2));
 }
 
 template <int LOG2M>
@@ -220,7 +371,7 @@ template <int LOG2M>
 cudaError_t launch_head_t(const DevState& s, const ChanCtl* ctl, const float* const* in, float* const* out,
                           int cur, cudaStream_t st) {
   using S = FftShape<LOG2M>;
-  head_kernel<LOG2M><<<s.C, S::T, 2 * S::M * sizeof(float2), st>>>(s, ctl, in, out, cur);
+  head_kernel<LOG2M><<<s.C, S::T, (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2), st>>>(s, ctl, in, out, cur);
   return cudaGetLastError();
 }
 
@@ -238,14 +389,46 @@ cudaError_t launch_head_t(const DevState& s, const ChanCtl* ctl, const float* co
     default: return cudaErrorInvalidValue;                       \
   }
 
-template <int UX, int SY>
+template <int UX, int SY, int D>
 cudaError_t launch_tail_t(const DevState& s, const ChanCtl* ctl, int which, int cur, cudaStream_t st) {
   const int U = s.B >> 1;
   dim3 grid((U + UX - 1) / UX, s.C);
   dim3 block(UX, SY);
-  tail_kernel<UX, SY><<<grid, block, 0, st>>>(s, ctl, which, cur);
+  tail_kernel<UX, SY, D><<<grid, block, 0, st>>>(s, ctl, which, cur);
   return cudaGetLastError();
 }
+
+template <int BR, int RS, int NS>
+cudaError_t launch_bulk_t(const DevState& s, const ChanCtl* ctl, int which, int cur, cudaStream_t st) {
+  if (s.B % BR != 0) return cudaErrorInvalidValue;
+  static cudaError_t attr = cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 bulk_smem_bytes<BR, RS, NS>());
+  if (attr != cudaSuccess) return attr;
+  dim3 grid(s.B / BR, s.C);
+  tail_bulk_kernel<BR, RS, NS><<<grid, BR / 2, bulk_smem_bytes<BR, RS, NS>(), st>>>(s, ctl, which, cur);
+  return cudaGetLastError();
+}
+
+using TailLauncher = cudaError_t (*)(const DevState&, const ChanCtl*, int, int, cudaStream_t);
+struct TailEntry {
+  MacTiling t;
+  TailLauncher fn;
+};
+// The tilings the autotuner chooses among.
+const TailEntry kTail[] = {
+    {{32, 8, 4}, launch_tail_t<32, 8, 4>},   {{16, 16, 4}, launch_tail_t<16, 16, 4>},
+    {{32, 8, 8}, launch_tail_t<32, 8, 8>},   {{32, 16, 4}, launch_tail_t<32, 16, 4>},
+    {{32, 16, 8}, launch_tail_t<32, 16, 8>}, {{64, 4, 4}, launch_tail_t<64, 4, 4>},
+    {{64, 8, 4}, launch_tail_t<64, 8, 4>},   {{64, 8, 8}, launch_tail_t<64, 8, 8>},
+    {{128, 2, 8}, launch_tail_t<128, 2, 8>}, {{32, 32, 4}, launch_tail_t<32, 32, 4>},
+    {{16, 32, 8}, launch_tail_t<16, 32, 8>}, {{64, 16, 2}, launch_tail_t<64, 16, 2>},
+    // cp.async.bulk pipelines: {BR/2, stages, rows per stage, kind 1}
+    {{32, 4, 8, 1}, launch_bulk_t<64, 8, 4>},   {{64, 4, 8, 1}, launch_bulk_t<128, 8, 4>},
+    {{64, 6, 4, 1}, launch_bulk_t<128, 4, 6>},  {{128, 4, 4, 1}, launch_bulk_t<256, 4, 4>},
+    {{64, 8, 8, 1}, launch_bulk_t<128, 8, 8>},  {{128, 3, 8, 1}, launch_bulk_t<256, 8, 3>},
+};
+constexpr int kTailCount = sizeof(kTail) / sizeof(kTail[0]);
 
 }  // namespace
 
@@ -279,14 +462,16 @@ cudaError_t launch_head_ptrs(const DevState& s, const ChanCtl* ctl, const float*
 cudaError_t launch_tail(const DevState& s, const ChanCtl* ctl, int which, int cur, MacTiling t,
                         cudaStream_t st) {
   if (s.P <= 1) return cudaSuccess;
-  if (t.ux == 16 && t.sy == 16) return launch_tail_t<16, 16>(s, ctl, which, cur, st);
-  if (t.ux == 32 && t.sy == 8) return launch_tail_t<32, 8>(s, ctl, which, cur, st);
-  if (t.ux == 64 && t.sy == 4) return launch_tail_t<64, 4>(s, ctl, which, cur, st);
-  if (t.ux == 128 && t.sy == 2) return launch_tail_t<128, 2>(s, ctl, which, cur, st);
-  if (t.ux == 32 && t.sy == 16) return launch_tail_t<32, 16>(s, ctl, which, cur, st);
-  if (t.ux == 64 && t.sy == 8) return launch_tail_t<64, 8>(s, ctl, which, cur, st);
+  for (int i = 0; i < kTailCount; ++i)
+    if (kTail[i].t.ux == t.ux && kTail[i].t.sy == t.sy && kTail[i].t.depth == t.depth &&
+        kTail[i].t.kind == t.kind)
+      return kTail[i].fn(s, ctl, which, cur, st);
   return cudaErrorInvalidValue;
 }
+
+int mac_tiling_count() { return kTailCount; }
+
+MacTiling mac_tiling(int index) { return kTail[index].t; }
 
 void make_twiddles(int N, float2* out) {
   const int q4 = N / 4;

@@ -1,0 +1,233 @@
+"""Serving loop over the batched engine, and real-time capacity of both forms.
+
+Sessions (each the equivalent of one TANConvolution: 1-8 channels, IR length
+log-uniform in [8192, 524288]) arrive as a Poisson process and live for
+exponential lifetimes; each receives IR swaps at a Poisson rate. Every audio
+block the loop admits arrivals while the device-memory budget allows (refused
+sessions are counted), retires departures, applies pending IR swaps, writes the
+block's input, runs one engine block and records the block latency against the
+block deadline B / fs. Time is simulated block by block as fast as the device
+allows; the latency of a block is the host wall time of everything done for it.
+
+`capacity()` measures the largest number of channels whose p99 block latency
+stays under the deadline, for the engine ("batched") and for one
+TANConvolution object per session processed in turn ("plain").
+
+    python -m tan_b200.serving --seconds 30 --rate 20 --spectrum fp32
+    python -m tan_b200.serving --capacity --ir-length 65536
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import convolution as cv
+from . import engine as eng
+
+FS = 48000
+
+
+class IRPool:
+    """Pre-generated exp-decayed Gaussian noise IRs (unit L2 norm per prefix use)."""
+
+    def __init__(self, g, n=8, length=524288, rt60=(0.2, 3.0)):
+        t = np.arange(length, dtype=np.float64)
+        self.irs = []
+        for _ in range(n):
+            r = g.uniform(*rt60)
+            h = g.standard_normal(length) * np.exp(-np.log(1000.0) * t / (r * FS))
+            self.irs.append(h.astype(np.float32))
+
+    def get(self, g, C, L):
+        out = np.empty((C, L), np.float32)
+        for c in range(C):
+            h = self.irs[int(g.integers(len(self.irs)))][:L]
+            out[c] = h / np.float32(np.linalg.norm(h))
+        return out
+
+
+def percentiles(lat_ms):
+    a = np.asarray(lat_ms)
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)),
+            "p999": float(np.percentile(a, 99.9)), "max": float(a.max())}
+
+
+def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256, spectrum=eng.SPECTRUM_FP32,
+          budget=150 << 30, max_channels=1 << 16, ch_range=(1, 8), len_range=(8192, 524288), seed=20261203 + 4,
+          prefill=True):
+    """Runs the serving loop; returns a dict of latency and occupancy statistics."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    pool = IRPool(g, length=len_range[1])
+    e = eng.Engine(ctx, block, spectrum, budget_bytes=budget, max_channels=max_channels)
+    deadline_ms = 1000.0 * block / FS
+    nblocks = int(seconds * FS / block)
+    dt = block / FS
+    live = {}  # id -> (session, end_time, next_swap_time)
+    refused = 0
+    admitted = 0
+    lat, chans = [], []
+    t = 0.0
+    next_arrival = g.exponential(1.0 / rate)
+
+    def new_session(now):
+        nonlocal refused, admitted
+        C = int(g.integers(ch_range[0], ch_range[1] + 1))
+        L = int(np.exp(g.uniform(np.log(len_range[0]), np.log(len_range[1]))))
+        rc, s = e.open_session(C, L)
+        if rc != cv.AMF_OK:
+            refused += 1
+            return
+        admitted += 1
+        s.update_response_td(pool.get(g, C, L))
+        live[s.id] = [s, now + g.exponential(lifetime), now + g.exponential(1.0 / swap_rate)]
+
+    if prefill:  # start in steady state: rate x lifetime sessions already running
+        for _ in range(int(rate * lifetime)):
+            new_session(0.0)
+    x = g.uniform(-1.0, 1.0, (max_channels, block)).astype(np.float32)
+    for k in range(nblocks):
+        t0 = time.perf_counter()
+        while next_arrival <= t:
+            new_session(t)
+            next_arrival += g.exponential(1.0 / rate)
+        for sid in [sid for sid, v in live.items() if v[1] <= t]:
+            live.pop(sid)[0].close()
+        for v in live.values():
+            if v[2] <= t:
+                s = v[0]
+                s.update_response_td(pool.get(g, s.channels, s.ir_length))
+                v[2] = t + g.exponential(1.0 / swap_rate)
+        info_ch = 0
+        for v in live.values():
+            s = v[0]
+            e.inp[s.slots] = x[s.slots]
+            info_ch += s.channels
+        rc = e.process() if live else cv.AMF_OK
+        assert rc == cv.AMF_OK, cv.last_error()
+        lat.append(1000.0 * (time.perf_counter() - t0))
+        chans.append(info_ch)
+        t += dt
+    e.synchronize()
+    e.release()
+    lat = np.asarray(lat)
+    return {"blocks": nblocks, "deadline_ms": deadline_ms, "latency_ms": percentiles(lat),
+            "deadline_misses": int((lat > deadline_ms).sum()), "concurrent_channels_mean": float(np.mean(chans)),
+            "concurrent_channels_max": int(np.max(chans)), "admitted": admitted, "refused": refused,
+            "spectrum": ["fp32", "fp16", "bf16"][spectrum]}
+
+
+def _block_latencies_batched(ctx, nsess, C, L, block, spectrum, blocks, g, pool):
+    e = eng.Engine(ctx, block, spectrum, budget_bytes=170 << 30, max_channels=nsess * C + 8)
+    sess = []
+    for _ in range(nsess):
+        rc, s = e.open_session(C, L)
+        if rc != cv.AMF_OK:
+            e.release()
+            return None
+        s.update_response_td(pool.get(g, C, L))
+        sess.append(s)
+    x = g.uniform(-1, 1, (nsess * C + 8, block)).astype(np.float32)
+    lat = []
+    for k in range(blocks + 5):
+        t0 = time.perf_counter()
+        e.inp[: nsess * C] = x[: nsess * C]
+        assert e.process() == cv.AMF_OK
+        if k >= 5:
+            lat.append(1000.0 * (time.perf_counter() - t0))
+    e.release()
+    return np.asarray(lat)
+
+
+def _block_latencies_plain(ctx, nsess, C, L, block, blocks, g, pool):
+    convs = []
+    for _ in range(nsess):
+        conv = cv.TANConvolution(ctx)
+        if conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, block, C) != cv.AMF_OK:
+            for c in convs:
+                c.Release()
+            return None
+        conv.UpdateResponseTD(pool.get(g, C, L), L)
+        convs.append(conv)
+    x = g.uniform(-1, 1, (C, block)).astype(np.float32)
+    y = np.zeros_like(x)
+    import ctypes
+
+    lib = cv.lib()
+    rin = (ctypes.c_void_p * C)(*[x[c].ctypes.data for c in range(C)])
+    rout = (ctypes.c_void_p * C)(*[y[c].ctypes.data for c in range(C)])
+    done = ctypes.c_size_t(0)
+    lat = []
+    for k in range(blocks + 5):
+        t0 = time.perf_counter()
+        for conv in convs:
+            rc = lib.tanb_convolution_process(conv._h, rin, rout, block, None, ctypes.byref(done))
+            assert rc == cv.AMF_OK
+        if k >= 5:
+            lat.append(1000.0 * (time.perf_counter() - t0))
+    for c in convs:
+        c.Release()
+    return np.asarray(lat)
+
+
+def capacity(ctx, form="batched", C=4, L=65536, block=256, spectrum=eng.SPECTRUM_FP32, blocks=200,
+             seed=20261203 + 5, start=4):
+    """Largest channel count (sessions of C channels, IR length L) whose p99 block
+    latency is under the deadline; doubling then bisection on the session count."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    pool = IRPool(g, n=4, length=L)
+    deadline = 1000.0 * block / FS
+
+    def ok(n):
+        if form == "batched":
+            lat = _block_latencies_batched(ctx, n, C, L, block, spectrum, blocks, g, pool)
+        else:
+            lat = _block_latencies_plain(ctx, n, C, L, block, blocks, g, pool)
+        if lat is None:
+            return False, None
+        p99 = float(np.percentile(lat, 99))
+        return p99 < deadline, p99
+
+    lo, hi = 0, start
+    last = {}
+    while True:
+        good, p99 = ok(hi)
+        last[hi] = p99
+        if not good:
+            break
+        lo, hi = hi, hi * 2
+        if hi * C > (1 << 17):
+            break
+    while hi - lo > max(1, lo // 16):
+        mid = (lo + hi) // 2
+        good, p99 = ok(mid)
+        last[mid] = p99
+        lo, hi = (mid, hi) if good else (lo, mid)
+    return {"form": form, "max_realtime_channels": lo * C, "sessions": lo, "channels_per_session": C,
+            "ir_length": L, "block": block, "deadline_ms": deadline, "p99_at": {str(k): v for k, v in last.items()}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--seconds", type=float, default=30.0)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--spectrum", choices=["fp32", "fp16", "bf16"], default="fp32")
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--capacity", action="store_true")
+    ap.add_argument("--form", choices=["batched", "plain"], default="batched")
+    ap.add_argument("--ir-length", type=int, default=65536)
+    ap.add_argument("--channels", type=int, default=4)
+    a = ap.parse_args()
+    spec = {"fp32": eng.SPECTRUM_FP32, "fp16": eng.SPECTRUM_FP16, "bf16": eng.SPECTRUM_BF16}[a.spectrum]
+    ctx = cv.TANContext(0)
+    if a.capacity:
+        r = capacity(ctx, a.form, a.channels, a.ir_length, spectrum=spec)
+    else:
+        r = serve(ctx, a.seconds, a.rate, spectrum=spec, budget=int(a.budget_gb * (1 << 30)))
+    print(json.dumps(r))
+
+
+if __name__ == "__main__":
+    main()

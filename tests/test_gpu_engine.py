@@ -1,0 +1,137 @@
+"""Batched engine on the GPU: sessions with different channel counts and IR
+lengths (uneven partition counts) processed together must give, per session,
+the same output as that session alone through the single-object path
+(tolerance 1e-5 x rms), also when sessions open and close mid-stream; FP16 /
+BF16 spectra are measured against the FP64 statement in dB; admission is by
+the device-memory budget."""
+import numpy as np
+import pytest
+
+from oracle import fp64
+from tan_b200 import convolution as cv
+from tan_b200 import engine as eng
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def alone(ctx, x, B, events):
+    """The session run by itself through TANConvolution (the plain path)."""
+    C, T = x.shape
+    L = max(ir.shape[1] for ir in events.values())
+    conv = cv.TANConvolution(ctx)
+    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_PARTITIONED_UNIFORM, L, B, C) == 0
+    y, codes = H.run_stream(conv, x, B, {k: (ir, None) for k, ir in events.items()})
+    conv.Release()
+    return y
+
+
+def run_engine(engine, sessions, nb, close_at=None, open_late=None):
+    """sessions: list of dict(C, L, x, events, start); returns outputs per session."""
+    B = engine.block
+    outs = [None] * len(sessions)
+    live = {}
+    for k in range(nb):
+        for i, s in enumerate(sessions):
+            if s["start"] == k:
+                rc, sess = engine.open_session(s["C"], s["L"])
+                assert rc == 0, cv.last_error()
+                live[i] = sess
+                outs[i] = np.zeros((s["C"], (nb - k) * B), np.float32)
+            if close_at and close_at.get(i) == k and i in live:
+                assert live.pop(i).close() == 0
+        for i, sess in live.items():
+            s = sessions[i]
+            kk = k - s["start"]
+            if kk in s["events"]:
+                assert sess.update_response_td(s["events"][kk]) == 0
+            engine.inp[sess.slots] = s["x"][:, kk * B:(kk + 1) * B]
+        assert engine.process() == 0, cv.last_error()
+        for i, sess in live.items():
+            kk = k - sessions[i]["start"]
+            outs[i][:, kk * B:(kk + 1) * B] = engine.out[sess.slots]
+    return outs
+
+
+def make_sessions(g, B, specs, nb):
+    sessions = []
+    for (C, L, start, swaps) in specs:
+        n = nb - start
+        x = H.noise(g, C, n * B)
+        events = {k: H.irs(g, C, L, (0.2, 1.5)) for k in swaps}
+        sessions.append({"C": C, "L": L, "x": x, "events": events, "start": start})
+    return sessions
+
+
+def test_engine_mix_equals_alone(tan_ctx):
+    g = H.rng(31)
+    B, nb = 256, 40
+    specs = [(2, 3000, 0, [0, 17]), (1, 20000, 0, [0, 9, 30]), (3, 65536, 3, [0, 11]), (4, 700, 5, [0]),
+             (2, 256, 0, [0, 20])]
+    sessions = make_sessions(g, B, specs, nb)
+    engine = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=1 << 30, max_channels=64, partitions_per_item=16)
+    outs = run_engine(engine, sessions, nb)
+    for s, y in zip(sessions, outs):
+        ya = alone(tan_ctx, s["x"], B, s["events"])
+        rms = np.sqrt(np.mean(ya.astype(np.float64) ** 2))
+        assert np.max(np.abs(y - ya)) <= TOL * rms
+        exp = fp64.stream_fp64(s["x"], B, [(k, {c: ir[c] for c in range(s["C"])}) for k, ir in s["events"].items()])
+        for c in range(s["C"]):
+            assert fp64.error_db(y[c], exp[c]) < -120
+    engine.release()
+
+
+def test_engine_churn_does_not_disturb_other_sessions(tan_ctx):
+    g = H.rng(32)
+    B, nb = 256, 36
+    specs = [(2, 5000, 0, [0, 13]), (1, 9000, 2, [0]), (2, 30000, 4, [0, 20]), (3, 1000, 10, [0, 4])]
+    sessions = make_sessions(g, B, specs, nb)
+    engine = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=256 << 20, max_channels=16, partitions_per_item=8)
+    # session 1 closes at block 12, freeing slots/memory that session 3 (opens at 10) and later reuse
+    outs = run_engine(engine, sessions, nb, close_at={1: 12})
+    for i, (s, y) in enumerate(zip(sessions, outs)):
+        if i == 1:
+            continue
+        ya = alone(tan_ctx, s["x"], B, s["events"])
+        rms = np.sqrt(np.mean(ya.astype(np.float64) ** 2))
+        assert np.max(np.abs(y - ya)) <= TOL * rms, i
+    engine.release()
+
+
+@pytest.mark.parametrize("spectrum,limit_db", [(eng.SPECTRUM_FP16, -60.0), (eng.SPECTRUM_BF16, -40.0)])
+def test_engine_reduced_precision_spectra_error_db(tan_ctx, spectrum, limit_db):
+    g = H.rng(33 + spectrum)
+    B, nb = 256, 24
+    specs = [(2, 8192, 0, [0]), (2, 40000, 0, [0, 10])]
+    sessions = make_sessions(g, B, specs, nb)
+    engine = eng.Engine(tan_ctx, B, spectrum, budget_bytes=1 << 28, max_channels=16)
+    outs = run_engine(engine, sessions, nb)
+    worst = -np.inf
+    for s, y in zip(sessions, outs):
+        exp = fp64.stream_fp64(s["x"], B, [(k, {c: ir[c] for c in range(s["C"])}) for k, ir in s["events"].items()])
+        for c in range(s["C"]):
+            worst = max(worst, fp64.error_db(y[c], exp[c]))
+    print(f"spectrum {spectrum}: worst channel error vs FP64 {worst:.1f} dB")
+    assert worst < limit_db
+    engine.release()
+
+
+def test_engine_admission_by_budget(tan_ctx):
+    B = 256
+    engine = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=32 << 20, max_channels=64)
+    opened = []
+    while True:
+        rc, s = engine.open_session(2, 65536)
+        if rc != 0:
+            assert rc == cv.AMF_OUT_OF_MEMORY
+            break
+        opened.append(s)
+    assert 1 <= len(opened) < 20
+    assert engine.info()["arena_bytes"] <= 32 << 20
+    assert opened[0].close() == 0
+    rc, s = engine.open_session(2, 65536)
+    assert rc == 0
+    assert engine.process() == 0
+    engine.release()

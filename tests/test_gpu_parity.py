@@ -269,3 +269,32 @@ def test_full_size_cfg2_properties(tan_ctx):
     assert T > 40000
     assert np.max(np.abs(y[:, 40000:] - x1[:, : T - 40000])) < 1e-6
     conv.Release()
+
+
+@pytest.mark.parametrize("B,L", [(256, 5000), (512, 20000), (1024, 9000)])
+def test_every_tail_tiling_matches_restatement(tan_ctx, B, L):
+    """Every compiled tail tiling (register-load and cp.async.bulk pipelines)
+    gives the restatement's output within tolerance, swaps included."""
+    g = H.rng(B + L)
+    C, nb = 3, 10
+    x = H.noise(g, C, nb * B)
+    events = {0: (H.irs(g, C, L), None), 6: (H.irs(g, C, L), None)}
+    oracle = ref.RefConvolution(L, B, C, threads=4)
+    yr, _ = H.run_stream(oracle, x, B, events)
+    idx = 0
+    tested = 0
+    while True:
+        conv = make(tan_ctx, L, B, C)
+        rc, tiling = conv.tiling(idx)
+        if rc != cv.AMF_OK:
+            conv.Release()
+            break
+        if tiling[0] <= B // 2:
+            y, codes = H.run_stream(conv, x, B, events, per_call_blocks=3)
+            assert all(c == 0 for c in codes), (tiling, cv.last_error())
+            assert conv.Synchronize() == 0
+            assert H.rel_err(y, yr) < TOL, tiling
+            tested += 1
+        conv.Release()
+        idx += 1
+    assert tested >= 10
