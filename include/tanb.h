@@ -281,6 +281,25 @@ int32_t tanb_engine_info(tanb_engine* engine, int64_t out[8]);
 int32_t tanb_engine_profile(tanb_engine* engine, int32_t enable);
 int32_t tanb_engine_profile_read(tanb_engine* engine, int64_t counts[4], double ms[2]);
 
+/* No reference counterpart. One-shot convolution that allocates no device
+ * memory, for callers that cannot call cudaMalloc on this path -- e.g. a
+ * plugin inside a host application's real-time audio callback, where an
+ * allocation can block for milliseconds, or a host that gives the library a
+ * fixed memory budget. out[c * samples + i] = sum_k ir[c * ir_length + k] *
+ * in[c * samples + i - k] for every channel c, i < samples (zero history
+ * before sample 0); in, ir, out are device arrays, samples a multiple of
+ * `block` (power of two in [32, 8192]), work enqueued on `stream`.
+ * All temporaries live in one library-owned device array of
+ * TANB_NO_ALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit; requests whose working set (about channels * ceil(ir_length / block)
+ * * block * 28 bytes plus small per-channel terms) exceeds it return
+ * TANB_INVALID_ARG. Calls share that array: calls that overlap on the GPU
+ * race, so serialise them. The first call on a device looks up the array's
+ * address; make it before any stream capture. */
+#define TANB_NO_ALLOC_SCRATCH_BYTES (32u << 20)
+int32_t tanb_convolve_no_alloc(const float* in, const float* ir, float* out, uint32_t channels, size_t samples,
+                               size_t ir_length, uint32_t block, void* stream);
+
 /* No reference counterpart: text of the last error raised on this thread. */
 const char* tanb_last_error(void);
 

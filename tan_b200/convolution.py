@@ -102,6 +102,7 @@ SIGNATURES = {
     "tanb_engine_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_engine_profile": (_i32, [_vp, _i32]),
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
+    "tanb_convolve_no_alloc": (_i32, [_vp, _vp, _vp, _u32, _sz, _sz, _u32, _vp]),
     "tanb_last_error": (ctypes.c_char_p, []),
 }
 
