@@ -254,6 +254,9 @@ int32_t tanb_engine_close_session(tanb_engine* engine, int32_t session);
 /* UpdateResponseTD for one session (host IR rows, n <= ir_length): the new IR
  * takes effect with a one-block crossfade on the next processed block. */
 int32_t tanb_engine_update_response_td(tanb_engine* engine, int32_t session, const float* const* ir, size_t n);
+/* Same with device-resident IR rows. */
+int32_t tanb_engine_update_response_td_device(tanb_engine* engine, int32_t session, const float* const* ir,
+                                              size_t n);
 
 /* Pinned host I/O buffers [max_channels][block]: write slot s's input block at
  * in[s * block], read its output at out[s * block] after tanb_engine_process. */

@@ -93,6 +93,7 @@ SIGNATURES = {
     "tanb_engine_open_session": (_i32, [_vp, _u32, _u32, ctypes.POINTER(ctypes.c_int32), _u32p]),
     "tanb_engine_close_session": (_i32, [_vp, _i32]),
     "tanb_engine_update_response_td": (_i32, [_vp, _i32, _pp, _sz]),
+    "tanb_engine_update_response_td_device": (_i32, [_vp, _i32, _pp, _sz]),
     "tanb_engine_io": (_i32, [_vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
                               ctypes.POINTER(ctypes.POINTER(ctypes.c_float))]),
     "tanb_engine_process": (_i32, [_vp]),

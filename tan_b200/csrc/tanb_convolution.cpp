@@ -91,6 +91,10 @@ struct tanb_convolution {
   float* d_out = nullptr;
   const ChanCtl* last_desc = nullptr;  // device descriptor of the last head (for ProcessFinalize)
   int last_cur = 0;
+  // per-block descriptors passed as kernel parameters (C <= kParamChannels)
+  std::vector<tanb::ParamDesc> pdesc;
+  tanb::ParamDesc last_pdesc{};
+  bool last_is_param = false;
 
   // UpdateResponseTD staging: IR rows [C][P*B], then ChanCtl[C] + int[C]
   float* h_ir = nullptr;
@@ -258,8 +262,13 @@ int32_t run_pending_finalize(tanb_convolution* v) {
   if (!v->finalize_due) return TANB_OK;
   v->finalize_due = false;
   if (v->P <= 1) return TANB_OK;
+  tanb::BlockRef ref;
+  if (v->last_is_param)
+    ref.param = &v->last_pdesc;
+  else
+    ref.ctl = v->last_desc;
   TANB_CUDA(counted(v, tanb_convolution::kTail,
-                    [&] { return tanb::launch_tail(v->ds, v->last_desc, 0, v->last_cur, v->tiling, v->stream); }));
+                    [&] { return tanb::launch_tail(v->ds, ref, 0, v->last_cur, v->tiling, v->stream); }));
   return TANB_OK;
 }
 
@@ -329,7 +338,11 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   // tail of the pending IR for the next block, from the current delay line
   if (v->P > 1)
     TANB_CUDA(counted(v, tanb_convolution::kTail,
-                      [&] { return tanb::launch_tail(v->ds, d_uctl, 1, v->cur, v->tiling, v->stream); }));
+                      [&] {
+                        tanb::BlockRef ref;
+                        ref.ctl = d_uctl;
+                        return tanb::launch_tail(v->ds, ref, 1, v->cur, v->tiling, v->stream);
+                      }));
   if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) TANB_CUDA(cudaStreamSynchronize(v->stream));
   return TANB_OK;
 }
@@ -398,6 +411,8 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   std::vector<std::vector<int>> flush_b(kMaxBlocksPerChunk);
   std::vector<int> cur_b(kMaxBlocksPerChunk);
 
+  const bool param = C <= tanb::kParamChannels;
+  if (param && v->pdesc.size() < (size_t)kMaxBlocksPerChunk) v->pdesc.resize(kMaxBlocksPerChunk);
   while (processed < nblocks && status == TANB_OK) {
     int nb = (int)std::min<size_t>(kMaxBlocksPerChunk, nblocks - processed);
     TANB_CUDA(cudaEventSynchronize(v->ev_stage));
@@ -410,9 +425,9 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         status = fail(TANB_WRONG_STATE, "no running channels");
         break;
       }
-      ChanCtl* ctl = v->desc_ctl(v->h_stage, b);
-      const float** din = v->desc_in(v->h_stage, b);
-      float** dout = v->desc_out(v->h_stage, b);
+      ChanCtl* ctl = param ? v->pdesc[b].ctl : v->desc_ctl(v->h_stage, b);
+      const float** din = param ? v->pdesc[b].in : v->desc_in(v->h_stage, b);
+      float** dout = param ? v->pdesc[b].out : v->desc_out(v->h_stage, b);
       flush_b[b].clear();
       for (int c = 0; c < C; ++c) {
         if (flush[c]) flush_b[b].push_back(c);
@@ -442,7 +457,8 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     }
     nb = filled;
     if (nb == 0) break;
-    TANB_CUDA(cudaMemcpyAsync(v->d_stage, v->h_stage, nb * v->desc_bytes, cudaMemcpyHostToDevice, v->stream));
+    if (!param)
+      TANB_CUDA(cudaMemcpyAsync(v->d_stage, v->h_stage, nb * v->desc_bytes, cudaMemcpyHostToDevice, v->stream));
     if (in_mem == Mem::Host)
       TANB_CUDA(cudaMemcpyAsync(v->stage_in(v->d_stage, 0, 0), v->stage_in(v->h_stage, 0, 0),
                                 (size_t)nb * C * B * sizeof(float), cudaMemcpyHostToDevice, v->stream));
@@ -450,10 +466,15 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     for (int b = 0; b < nb; ++b) {
       for (int c : flush_b[b]) TANB_CUDA(flush_channel(v, c));
       const ChanCtl* dctl = v->desc_ctl(v->d_stage, b);
-      TANB_CUDA(counted(v, tanb_convolution::kHead, [&] {
-        return tanb::launch_head_ptrs(v->ds, dctl, v->desc_in(v->d_stage, b), v->desc_out(v->d_stage, b),
-                                      cur_b[b], v->stream);
-      }));
+      tanb::BlockRef ref;
+      if (param) {
+        ref.param = &v->pdesc[b];
+      } else {
+        ref.ctl = dctl;
+        ref.in = v->desc_in(v->d_stage, b);
+        ref.out = v->desc_out(v->d_stage, b);
+      }
+      TANB_CUDA(counted(v, tanb_convolution::kHead, [&] { return tanb::launch_head(v->ds, ref, cur_b[b], v->stream); }));
       const bool last = (b == nb - 1);
       if (last) {
         if (out_mem == Mem::Host)
@@ -461,16 +482,18 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
                                     cudaMemcpyDeviceToHost, v->stream));
         TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
         v->last_desc = dctl;
+        v->last_is_param = param;
+        if (param) v->last_pdesc = v->pdesc[b];
         v->last_cur = cur_b[b];
         if (v->finalize_mode) {
           v->finalize_due = true;
         } else if (P > 1) {
           TANB_CUDA(counted(v, tanb_convolution::kTail,
-                            [&] { return tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream); }));
+                            [&] { return tanb::launch_tail(v->ds, ref, 0, cur_b[b], v->tiling, v->stream); }));
         }
       } else if (P > 1) {
         TANB_CUDA(counted(v, tanb_convolution::kTail,
-                          [&] { return tanb::launch_tail(v->ds, dctl, 0, cur_b[b], v->tiling, v->stream); }));
+                          [&] { return tanb::launch_tail(v->ds, ref, 0, cur_b[b], v->tiling, v->stream); }));
       }
     }
     if (out_mem == Mem::Host) {

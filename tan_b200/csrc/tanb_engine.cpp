@@ -436,7 +436,7 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   return TANB_OK;
 }
 
-int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const float* const* ir, size_t n) {
+static int32_t engine_update(tanb_engine* e, int32_t session, const float* const* ir, size_t n, bool device) {
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   std::lock_guard<std::mutex> lock(e->mu);
   auto it = e->sessions.find(session);
@@ -458,16 +458,24 @@ int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const fl
     ENG_CUDA(cudaMallocHost(&e->h_ir, need * sizeof(float)));
     e->ir_cap = need;
   }
-  for (int j = 0; j < s.C; ++j) {
+  for (int j = 0; j < s.C; ++j)
     if (!ir[j] && n) return efail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", j);
-    float* row = e->h_ir + (size_t)j * PB;
-    if (n) std::memcpy(row, ir[j], n * sizeof(float));
-    std::memset(row + n, 0, (PB - n) * sizeof(float));
+  for (int j = 0; j < s.C; ++j) {
+    if (device) {
+      float* row = e->d_ir + (size_t)j * PB;
+      if (n) ENG_CUDA(cudaMemcpyAsync(row, ir[j], n * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+      ENG_CUDA(cudaMemsetAsync(row + n, 0, (PB - n) * sizeof(float), e->stream));
+    } else {
+      float* row = e->h_ir + (size_t)j * PB;
+      if (n) std::memcpy(row, ir[j], n * sizeof(float));
+      std::memset(row + n, 0, (PB - n) * sizeof(float));
+    }
     EngChan& ch = e->h_chans[s.slot0 + j];
     e->h_upd[j] = EngUpd{(int)(s.slot0 + j), 1 - ch.active, (int64_t)PB};
     ch.pending = 1;
   }
-  ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, need * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+  if (!device)
+    ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, need * sizeof(float), cudaMemcpyHostToDevice, e->stream));
   ENG_CUDA(cudaMemcpyAsync(e->d_upd, e->h_upd, s.C * sizeof(EngUpd), cudaMemcpyHostToDevice, e->stream));
   ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_ir, e->d_upd, s.C, s.P, e->d_tw, e->stream));
   e->n_ir += 1;
@@ -476,6 +484,15 @@ int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const fl
     ENG_CUDA(tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, s.C * s.nitem, 1,
                                    std::min(e->tail_grid, s.C * s.nitem), e->stream));
   return TANB_OK;
+}
+
+int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const float* const* ir, size_t n) {
+  return engine_update(e, session, ir, n, false);
+}
+
+int32_t tanb_engine_update_response_td_device(tanb_engine* e, int32_t session, const float* const* ir,
+                                              size_t n) {
+  return engine_update(e, session, ir, n, true);
 }
 
 int32_t tanb_engine_io(tanb_engine* e, float** in, float** out) {

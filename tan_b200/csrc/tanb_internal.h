@@ -65,6 +65,25 @@ struct MacTiling {
 int mac_tiling_count();
 MacTiling mac_tiling(int index);
 
+// Per-block descriptors of up to kParamChannels channels, passed to the head
+// and tail kernels as a kernel parameter (no copy to device memory and no
+// dependent global load before a CTA knows its channel's state).
+constexpr int kParamChannels = 128;
+struct ParamDesc {
+  ChanCtl ctl[kParamChannels];
+  const float* in[kParamChannels];
+  float* out[kParamChannels];
+};
+
+// Where a launch finds its per-channel descriptors: a ParamDesc (host copy,
+// passed by value) or device arrays.
+struct BlockRef {
+  const ParamDesc* param = nullptr;
+  const ChanCtl* ctl = nullptr;
+  const float* const* in = nullptr;
+  float* const* out = nullptr;
+};
+
 // R2C of each IR partition into slot `slot_new` of the channels listed in
 // `chans` (device array of nch channel indices). `ir` is [nch][P*B] floats,
 // row j holding the zero-padded IR of channel chans[j].
@@ -75,16 +94,15 @@ cudaError_t launch_ir_spectrum(const DevState& s, const float* ir, const int* ch
 // delay-line slot `cur`, multiply with partition 0, add the precomputed tail,
 // inverse FFT, overlap-save output (and the crossfade on swap channels).
 // `in[c]` / `out[c]` are device pointers to channel c's B input / output samples.
-cudaError_t launch_head_ptrs(const DevState& s, const ChanCtl* ctl, const float* const* in,
-                             float* const* out, int cur, cudaStream_t st);
+cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st);
 
 // Tail multiply-accumulate for the block after the one whose spectrum sits in
 // delay-line slot `cur`:
 //   tail[c][which] = sum_{i=1}^{P-1} FDL[c][(cur + i - 1) mod P] * H[c][slot][i]
 // which = 0: running channels, slot = swap ? slot_new : slot_cur
 // which = 1: channels with swap set (pending IR), slot = slot_new
-cudaError_t launch_tail(const DevState& s, const ChanCtl* ctl, int which, int cur,
-                        MacTiling t, cudaStream_t st);
+cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, MacTiling t,
+                        cudaStream_t st);
 
 // Per-channel descriptor of one TIME_DOMAIN call.
 struct TdChan {

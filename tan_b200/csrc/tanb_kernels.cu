@@ -22,6 +22,22 @@
 namespace tanb {
 namespace {
 
+// Descriptor sources for the head and tail kernels.
+struct DevDesc {
+  const ChanCtl* ctl;
+  const float* const* in;
+  float* const* out;
+  __device__ __forceinline__ ChanCtl get_ctl(int c) const { return ctl[c]; }
+  __device__ __forceinline__ const float* get_in(int c) const { return in[c]; }
+  __device__ __forceinline__ float* get_out(int c) const { return out[c]; }
+};
+struct ParDesc {
+  ParamDesc p;
+  __device__ __forceinline__ ChanCtl get_ctl(int c) const { return p.ctl[c]; }
+  __device__ __forceinline__ const float* get_in(int c) const { return p.in[c]; }
+  __device__ __forceinline__ float* get_out(int c) const { return p.out[c]; }
+};
+
 
 template <int LOG2M>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T)
@@ -52,21 +68,20 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   }
 }
 
-template <int LOG2M>
+template <int LOG2M, class D>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T)
-    head_kernel(DevState s, const ChanCtl* __restrict__ ctl, const float* const* __restrict__ inp,
-                float* const* __restrict__ outp, int cur) {
+    head_kernel(DevState s, const __grid_constant__ D desc, int cur) {
   using S = FftShape<LOG2M>;
   constexpr int M = S::M, T = S::T, KP = S::KP;
   extern __shared__ float2 sm[];
   float2* z = sm;       // old / only IR
   float2* z2 = sm + M;  // new IR on a swap block
   const int c = blockIdx.x;
-  const ChanCtl cc = ctl[c];
+  const ChanCtl cc = desc.get_ctl(c);
   if (!cc.run) return;
   const bool swap = cc.swap != 0;
-  const float* x = inp[c];
-  float* y = outp[c];
+  const float* x = desc.get_in(c);
+  float* y = desc.get_out(c);
   float* prev = s.prev + (size_t)c * M;
   const float2* h0 = s.H + h_index(s, c, cc.slot_cur, 0);
   const float2* h1 = s.H + h_index(s, c, cc.slot_new, 0);
@@ -167,11 +182,11 @@ __device__ __forceinline__ float4 mac4(float4 acc, float4 f, float4 h, bool dc) 
   return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
 
-template <int UX, int SY, int D>
+template <int UX, int SY, int D, class DS>
 __global__ void __launch_bounds__(UX* SY)
-    tail_kernel(DevState s, const ChanCtl* __restrict__ ctl, int which, int cur) {
+    tail_kernel(DevState s, const __grid_constant__ DS desc, int which, int cur) {
   const int c = blockIdx.y;
-  const ChanCtl cc = ctl[c];
+  const ChanCtl cc = desc.get_ctl(c);
   if (which == 0 ? !cc.run : !cc.swap) return;
   const int slot = (which == 0) ? (cc.swap ? cc.slot_new : cc.slot_cur) : cc.slot_new;
   const int U = s.B >> 1;  // float4 units per partition
@@ -268,9 +283,9 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                : "memory");
 }
 
-template <int BR, int RS, int NS>
+template <int BR, int RS, int NS, class DS>
 __global__ void __launch_bounds__(BR / 2)
-    tail_bulk_kernel(DevState s, const ChanCtl* __restrict__ ctl, int which, int cur) {
+    tail_bulk_kernel(DevState s, const __grid_constant__ DS desc, int which, int cur) {
   constexpr int U = BR / 2;                     // threads = float4 units of the slice
   constexpr uint32_t kRowBytes = BR * sizeof(float2);
   extern __shared__ __align__(128) unsigned char bulk_smem[];
@@ -278,7 +293,7 @@ __global__ void __launch_bounds__(BR / 2)
   float4* fbuf = hbuf + NS * RS * U;                                // [NS][RS][U]
   uint64_t* bars = reinterpret_cast<uint64_t*>(fbuf + NS * RS * U);  // [NS]
   const int c = blockIdx.y;
-  const ChanCtl cc = ctl[c];
+  const ChanCtl cc = desc.get_ctl(c);
   if (which == 0 ? !cc.run : !cc.swap) return;
   const int slot = (which == 0) ? (cc.swap ? cc.slot_new : cc.slot_cur) : cc.slot_new;
   const int P = s.P;
@@ -352,7 +367,10 @@ constexpr int bulk_smem_bytes() {
 template <int LOG2M>
 cudaError_t set_attrs() {
   const int smem = (FftShape<LOG2M>::TW_SMEM ? 4 : 2) * (1 << LOG2M) * (int)sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(head_kernel<LOG2M>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e =
+      cudaFuncSetAttribute(head_kernel<LOG2M, DevDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(head_kernel<LOG2M, ParDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(ir_spectrum_kernel<LOG2M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (1 << LOG2M) * (int)sizeof(float2));
@@ -368,10 +386,13 @@ cudaError_t launch_ir_t(const DevState& s, const float* ir, const int* chans, in
 }
 
 template <int LOG2M>
-cudaError_t launch_head_t(const DevState& s, const ChanCtl* ctl, const float* const* in, float* const* out,
-                          int cur, cudaStream_t st) {
+cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, cudaStream_t st) {
   using S = FftShape<LOG2M>;
-  head_kernel<LOG2M><<<s.C, S::T, (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2), st>>>(s, ctl, in, out, cur);
+  const size_t smem = (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2);
+  if (d.param)
+    head_kernel<LOG2M, ParDesc><<<s.C, S::T, smem, st>>>(s, ParDesc{*d.param}, cur);
+  else
+    head_kernel<LOG2M, DevDesc><<<s.C, S::T, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, cur);
   return cudaGetLastError();
 }
 
@@ -390,27 +411,38 @@ cudaError_t launch_head_t(const DevState& s, const ChanCtl* ctl, const float* co
   }
 
 template <int UX, int SY, int D>
-cudaError_t launch_tail_t(const DevState& s, const ChanCtl* ctl, int which, int cur, cudaStream_t st) {
+cudaError_t launch_tail_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st) {
   const int U = s.B >> 1;
   dim3 grid((U + UX - 1) / UX, s.C);
   dim3 block(UX, SY);
-  tail_kernel<UX, SY, D><<<grid, block, 0, st>>>(s, ctl, which, cur);
+  if (d.param)
+    tail_kernel<UX, SY, D, ParDesc><<<grid, block, 0, st>>>(s, ParDesc{*d.param}, which, cur);
+  else
+    tail_kernel<UX, SY, D, DevDesc><<<grid, block, 0, st>>>(s, DevDesc{d.ctl, d.in, d.out}, which, cur);
   return cudaGetLastError();
 }
 
 template <int BR, int RS, int NS>
-cudaError_t launch_bulk_t(const DevState& s, const ChanCtl* ctl, int which, int cur, cudaStream_t st) {
+cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st) {
   if (s.B % BR != 0) return cudaErrorInvalidValue;
-  static cudaError_t attr = cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 bulk_smem_bytes<BR, RS, NS>());
+  constexpr int smem = bulk_smem_bytes<BR, RS, NS>();
+  static cudaError_t attr = [] {
+    cudaError_t e = cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS, DevDesc>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS, ParDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem);
+  }();
   if (attr != cudaSuccess) return attr;
   dim3 grid(s.B / BR, s.C);
-  tail_bulk_kernel<BR, RS, NS><<<grid, BR / 2, bulk_smem_bytes<BR, RS, NS>(), st>>>(s, ctl, which, cur);
+  if (d.param)
+    tail_bulk_kernel<BR, RS, NS, ParDesc><<<grid, BR / 2, smem, st>>>(s, ParDesc{*d.param}, which, cur);
+  else
+    tail_bulk_kernel<BR, RS, NS, DevDesc><<<grid, BR / 2, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, which, cur);
   return cudaGetLastError();
 }
 
-using TailLauncher = cudaError_t (*)(const DevState&, const ChanCtl*, int, int, cudaStream_t);
+using TailLauncher = cudaError_t (*)(const DevState&, const BlockRef&, int, int, cudaStream_t);
 struct TailEntry {
   MacTiling t;
   TailLauncher fn;
@@ -454,18 +486,17 @@ cudaError_t launch_ir_spectrum(const DevState& s, const float* ir, const int* ch
   TANB_DISPATCH_LOG2(s.log2B, launch_ir_t, s, ir, chans, nch, ctl, st);
 }
 
-cudaError_t launch_head_ptrs(const DevState& s, const ChanCtl* ctl, const float* const* in,
-                             float* const* out, int cur, cudaStream_t st) {
-  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, ctl, in, out, cur, st);
+cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st) {
+  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, d, cur, st);
 }
 
-cudaError_t launch_tail(const DevState& s, const ChanCtl* ctl, int which, int cur, MacTiling t,
+cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, MacTiling t,
                         cudaStream_t st) {
   if (s.P <= 1) return cudaSuccess;
   for (int i = 0; i < kTailCount; ++i)
     if (kTail[i].t.ux == t.ux && kTail[i].t.sy == t.sy && kTail[i].t.depth == t.depth &&
         kTail[i].t.kind == t.kind)
-      return kTail[i].fn(s, ctl, which, cur, st);
+      return kTail[i].fn(s, d, which, cur, st);
   return cudaErrorInvalidValue;
 }
 

@@ -174,8 +174,12 @@ extern "C" int32_t tanb_convolve_no_alloc(const float* in, const float* ir, floa
                                                                    samples, b * B, 1);
       if ((e = cudaGetLastError()) != cudaSuccess) break;
       cur = (cur - 1 + (int)P) % (int)P;
-      if ((e = tanb::launch_head_ptrs(s, ctl, in_rows, out_rows, cur, st)) != cudaSuccess) break;
-      e = tanb::launch_tail(s, ctl, 0, cur, tanb::MacTiling{32, 8}, st);
+      tanb::BlockRef ref;
+      ref.ctl = ctl;
+      ref.in = in_rows;
+      ref.out = out_rows;
+      if ((e = tanb::launch_head(s, ref, cur, st)) != cudaSuccess) break;
+      e = tanb::launch_tail(s, ref, 0, cur, tanb::MacTiling{32, 8}, st);
     }
   } while (0);
   if (e != cudaSuccess) {

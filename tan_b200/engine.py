@@ -32,6 +32,12 @@ class Session:
         rows = (ctypes.c_void_p * self.channels)(*[ir[c].ctypes.data for c in range(self.channels)])
         return lib().tanb_engine_update_response_td(self.engine._h, self.id, rows, ir.shape[1])
 
+    def update_response_td_device(self, ir) -> int:
+        """IR rows resident on the device: a (channels, n) CUDA tensor."""
+        base, stride = ir.data_ptr(), ir.stride(0) * ir.element_size()
+        rows = (ctypes.c_void_p * self.channels)(*[base + c * stride for c in range(self.channels)])
+        return lib().tanb_engine_update_response_td_device(self.engine._h, self.id, rows, ir.shape[1])
+
     def close(self) -> int:
         return lib().tanb_engine_close_session(self.engine._h, self.id)
 

@@ -1,0 +1,102 @@
+"""Multi-GPU control plane on CPU: session placement and the per-rank loop,
+run as world_size-2 gloo process groups (no GPU). Also checks that a rank
+failing mid-run ends the others with an error instead of a hang."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from tan_b200 import sharding as sh
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _sessions(n=60, seed=5):
+    g = np.random.Generator(np.random.PCG64(seed))
+    return [sh.SessionSpec(i, int(g.integers(1, 9)), int(np.exp(g.uniform(np.log(8192), np.log(524288)))))
+            for i in range(n)]
+
+
+def test_placement_is_complete_and_balanced():
+    ss = _sessions()
+    pl = sh.assign(ss, 4, 256)
+    assert sorted(pl) == [s.sid for s in ss]
+    assert all(0 <= r < 4 for r in pl.values())
+    per = sh.loads(ss, pl, 4, 256)
+    assert max(per) / min(per) < 1.15
+
+
+def test_placement_respects_memory_budget():
+    ss = _sessions(40)
+    total = sum(sh.device_bytes(s, 256) for s in ss)
+    budget = total // 3  # two ranks cannot hold everything
+    pl = sh.assign(ss, 2, 256, budget)
+    used = [0, 0]
+    for s in ss:
+        if pl[s.sid] >= 0:
+            used[pl[s.sid]] += sh.device_bytes(s, 256)
+    assert max(used) <= budget
+    assert any(r == -1 for r in pl.values())
+
+
+def _worker(rank, world, port, mode, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    try:
+        ss = _sessions(30, seed=9)
+        pl = sh.broadcast_placement(dist, ss, 256)
+        mine = [s for s in ss if pl[s.sid] == rank]
+        # per-rank work of one block (stand-in for the engine): bytes of its shard
+        t = torch.tensor([float(sum(sh.tail_bytes(s, 256) for s in mine))], dtype=torch.float64)
+        if mode == "fail" and rank == 1:
+            raise RuntimeError("injected failure on rank 1 before the reduction")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        q.put((rank, sorted(s.sid for s in mine), float(t.item()), None))
+    except Exception as e:  # noqa: BLE001
+        q.put((rank, None, None, type(e).__name__))
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:
+            pass
+
+
+def _run(mode):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_worker, args=(r, 2, port, mode, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = [q.get(timeout=120) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    return sorted(out)
+
+
+def test_two_rank_placement_covers_every_session_once():
+    out = _run("ok")
+    (r0, s0, m0, e0), (r1, s1, m1, e1) = out
+    assert e0 is None and e1 is None
+    assert sorted(s0 + s1) == list(range(30)) and not set(s0) & set(s1)
+    assert m0 == m1 > 0
+
+
+def test_failed_rank_ends_peers_with_an_error():
+    out = _run("fail")
+    errs = {r: e for r, _, _, e in out}
+    assert errs[1] == "RuntimeError"
+    assert errs[0] is not None  # the peer's collective failed or timed out, it did not hang
