@@ -251,12 +251,18 @@ int32_t tanb_engine_open_session(tanb_engine* engine, uint32_t channels, uint32_
                                  uint32_t* first_slot);
 int32_t tanb_engine_close_session(tanb_engine* engine, int32_t session);
 
-/* UpdateResponseTD for one session (host IR rows, n <= ir_length): the new IR
- * takes effect with a one-block crossfade on the next processed block. */
-int32_t tanb_engine_update_response_td(tanb_engine* engine, int32_t session, const float* const* ir, size_t n);
+/* UpdateResponseTD for one session (host IR rows, n <= ir_length). The IR is
+ * copied before this returns and transformed on the engine's update stream,
+ * off the audio path; it takes effect, with a one-block crossfade, on the
+ * first tanb_engine_process* call after the transform has finished. With
+ * TANB_OPERATION_FLAG_BLOCK_UNTIL_READY the call waits for the transform, so
+ * the swap lands on the next block (the reference flag's meaning,
+ * TrueAudioNext.h:112-120). May be called from another thread than Process. */
+int32_t tanb_engine_update_response_td(tanb_engine* engine, int32_t session, const float* const* ir, size_t n,
+                                       uint32_t operationFlags);
 /* Same with device-resident IR rows. */
 int32_t tanb_engine_update_response_td_device(tanb_engine* engine, int32_t session, const float* const* ir,
-                                              size_t n);
+                                              size_t n, uint32_t operationFlags);
 
 /* Pinned host I/O buffers [max_channels][block]: write slot s's input block at
  * in[s * block], read its output at out[s * block] after tanb_engine_process. */
@@ -277,6 +283,11 @@ void* tanb_engine_stream(tanb_engine* engine);
  * items high-water mark, out[4] arena bytes in use, out[5] budget, out[6]
  * algorithmic tail bytes per block, out[7] tail grid size. */
 int32_t tanb_engine_info(tanb_engine* engine, int64_t out[8]);
+
+/* out[0] blocks the session has processed, out[1] its block index at which the
+ * last IR update took effect (-1: none yet), out[2] 1 while an update is
+ * uploaded but not yet in effect. */
+int32_t tanb_engine_session_state(tanb_engine* engine, int32_t session, int64_t out[3]);
 
 /* Device-time accounting of tanb_engine_process_device: counts[0] heads,
  * counts[1] tails, counts[2] IR updates, counts[3] timed blocks; ms[0] head,

@@ -92,8 +92,8 @@ SIGNATURES = {
     "tanb_engine_release": (_i32, [_vp]),
     "tanb_engine_open_session": (_i32, [_vp, _u32, _u32, ctypes.POINTER(ctypes.c_int32), _u32p]),
     "tanb_engine_close_session": (_i32, [_vp, _i32]),
-    "tanb_engine_update_response_td": (_i32, [_vp, _i32, _pp, _sz]),
-    "tanb_engine_update_response_td_device": (_i32, [_vp, _i32, _pp, _sz]),
+    "tanb_engine_update_response_td": (_i32, [_vp, _i32, _pp, _sz, _u32]),
+    "tanb_engine_update_response_td_device": (_i32, [_vp, _i32, _pp, _sz, _u32]),
     "tanb_engine_io": (_i32, [_vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
                               ctypes.POINTER(ctypes.POINTER(ctypes.c_float))]),
     "tanb_engine_process": (_i32, [_vp]),
@@ -101,6 +101,7 @@ SIGNATURES = {
     "tanb_engine_synchronize": (_i32, [_vp]),
     "tanb_engine_stream": (_vp, [_vp]),
     "tanb_engine_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
+    "tanb_engine_session_state": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_engine_profile": (_i32, [_vp, _i32]),
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_convolve_no_alloc": (_i32, [_vp, _vp, _vp, _u32, _sz, _sz, _u32, _vp]),

@@ -107,6 +107,11 @@ struct Session {
   int C = 0, L = 0, P = 0, nitem = 0;
   size_t slot0 = 0, item0 = 0;
   size_t arena_off = 0, arena_bytes = 0;
+  // IR update staged on the update stream, waiting for its event before commit
+  bool staged = false;
+  cudaEvent_t staged_ev = nullptr;
+  int64_t blocks = 0;            // blocks processed since the session opened
+  int64_t last_swap_block = -1;  // session block at which the last IR update took effect
 };
 
 }  // namespace
@@ -116,7 +121,9 @@ struct tanb_engine {
   std::mutex mu;
   int B = 0, log2B = 0, spec = 0, Q = 32;
   size_t budget = 0, max_channels = 0, max_items = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // audio path: head, tail, I/O copies
+  cudaStream_t upd_stream = nullptr;  // IR uploads and transforms
+  std::mutex upd_mu;                  // serialises IR updates (taken before mu)
   char* arena = nullptr;
   RangeAlloc arena_alloc, slot_alloc, item_alloc;
   EngChan* d_chans = nullptr;
@@ -171,7 +178,11 @@ void destroy_graph(tanb_engine* e) {
 }
 
 void free_engine(tanb_engine* e) {
+  if (e->upd_stream) cudaStreamSynchronize(e->upd_stream);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  for (auto& kv : e->sessions)
+    if (kv.second.staged_ev) cudaEventDestroy(kv.second.staged_ev);
+  e->sessions.clear();
   destroy_graph(e);
   cudaFree(e->arena);
   cudaFree(e->d_chans);
@@ -191,8 +202,10 @@ void free_engine(tanb_engine* e) {
   if (e->pa) cudaEventDestroy(e->pa);
   if (e->pb) cudaEventDestroy(e->pb);
   if (e->pc) cudaEventDestroy(e->pc);
+  if (e->upd_stream) cudaStreamDestroy(e->upd_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
 }
+
 
 cudaError_t upload_chans(tanb_engine* e, size_t first, size_t n) {
   if (!n) return cudaSuccess;
@@ -209,6 +222,31 @@ cudaError_t upload_items(tanb_engine* e, size_t first, size_t n) {
 void update_hwm(tanb_engine* e) {
   e->nslots_hwm = e->slot_alloc.high_water();
   e->nitems_hwm = e->item_alloc.high_water();
+}
+
+// Commits every staged IR update whose transform has finished: the channels'
+// pending flags go to the device table and the new IR's tail for the coming
+// block is computed from the current delay line, both on the audio stream
+// before this block's head (which then crossfades to the new IR). Caller holds mu.
+cudaError_t commit_updates(tanb_engine* e) {
+  for (auto& kv : e->sessions) {
+    Session& s = kv.second;
+    if (!s.staged) continue;
+    cudaError_t q = cudaEventQuery(s.staged_ev);
+    if (q == cudaErrorNotReady) continue;
+    if (q != cudaSuccess) return q;
+    s.staged = false;
+    s.last_swap_block = s.blocks;  // the head of this block crossfades to the new IR
+    for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j].pending = 1;
+    cudaError_t r = upload_chans(e, s.slot0, s.C);
+    if (r != cudaSuccess) return r;
+    if (s.nitem) {
+      r = tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, s.C * s.nitem, 1,
+                                std::min(e->tail_grid, s.C * s.nitem), e->stream);
+      if (r != cudaSuccess) return r;
+    }
+  }
+  return cudaSuccess;
 }
 
 // Enqueues one block: head over all slots, output copy (host mode), tail.
@@ -252,7 +290,8 @@ cudaError_t ensure_graph(tanb_engine* e) {
 // Host mirror of what the head kernel does to the channel table.
 void advance_mirror(tanb_engine* e) {
   for (auto& kv : e->sessions) {
-    const Session& s = kv.second;
+    Session& s = kv.second;
+    s.blocks += 1;
     for (int j = 0; j < s.C; ++j) {
       EngChan& ch = e->h_chans[s.slot0 + j];
       ch.cur = (ch.cur - 1 + ch.P) % ch.P;
@@ -289,6 +328,7 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   cudaError_t r = cudaSetDevice(ctx->device);
   if (r == cudaSuccess) r = tanb::eng_prepare();
   if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->upd_stream, cudaStreamNonBlocking);
   const size_t io = e->max_channels * e->B;
   if (r == cudaSuccess) r = cudaMalloc(&e->arena, std::max<size_t>(budget_bytes, kAlign));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_chans, e->max_channels * sizeof(EngChan));
@@ -407,6 +447,7 @@ int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_
   }
   ENG_CUDA(upload_chans(e, s.slot0, s.C));
   ENG_CUDA(upload_items(e, s.item0, nit_total));
+  ENG_CUDA(cudaEventCreateWithFlags(&s.staged_ev, cudaEventDisableTiming));
   s.id = e->next_id++;
   e->sessions[s.id] = s;
   update_hwm(e);
@@ -417,12 +458,15 @@ int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_
 
 int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  std::lock_guard<std::mutex> ulock(e->upd_mu);  // no IR upload may still write this session's memory
   std::lock_guard<std::mutex> lock(e->mu);
   auto it = e->sessions.find(session);
   if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
   ENG_CUDA(cudaSetDevice(e->ctx->device));
+  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
   ENG_CUDA(cudaStreamSynchronize(e->stream));
   const Session s = it->second;
+  if (s.staged_ev) cudaEventDestroy(s.staged_ev);
   for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j] = EngChan{};
   const size_t nit_total = (size_t)s.C * s.nitem;
   for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0};
@@ -436,16 +480,29 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   return TANB_OK;
 }
 
-static int32_t engine_update(tanb_engine* e, int32_t session, const float* const* ir, size_t n, bool device) {
+static int32_t engine_update(tanb_engine* e, int32_t session, const float* const* ir, size_t n, bool device,
+                             uint32_t op) {
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
-  std::lock_guard<std::mutex> lock(e->mu);
-  auto it = e->sessions.find(session);
-  if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
-  const Session& s = it->second;
   if (!ir) return efail(TANB_INVALID_ARG, "ppBuffer == NULL");
-  if (n > (size_t)s.L) return efail(TANB_INVALID_ARG, "IR length %zu exceeds the session's %d", n, s.L);
+  std::lock_guard<std::mutex> ulock(e->upd_mu);
+  Session s;
+  {
+    // read the session and choose the idle IR slots under the main lock: the
+    // audio path flips slots only under this lock, so the choice is consistent
+    std::lock_guard<std::mutex> lock(e->mu);
+    auto it = e->sessions.find(session);
+    if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
+    s = it->second;
+    if (n > (size_t)s.L) return efail(TANB_INVALID_ARG, "IR length %zu exceeds the session's %d", n, s.L);
+    for (int j = 0; j < s.C; ++j) {
+      if (!ir[j] && n) return efail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", j);
+      e->h_upd[j] = EngUpd{(int)(s.slot0 + j), 1 - e->h_chans[s.slot0 + j].active, (int64_t)s.P * e->B};
+    }
+    it->second.staged = false;  // a newer upload supersedes one not yet committed
+  }
   ENG_CUDA(cudaSetDevice(e->ctx->device));
-  ENG_CUDA(cudaStreamSynchronize(e->stream));  // staging reuse
+  // IR staging of the previous upload must have been consumed
+  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
   const size_t PB = (size_t)s.P * e->B;
   const size_t need = PB * s.C;
   if (need > e->ir_cap) {
@@ -458,41 +515,42 @@ static int32_t engine_update(tanb_engine* e, int32_t session, const float* const
     ENG_CUDA(cudaMallocHost(&e->h_ir, need * sizeof(float)));
     e->ir_cap = need;
   }
-  for (int j = 0; j < s.C; ++j)
-    if (!ir[j] && n) return efail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", j);
   for (int j = 0; j < s.C; ++j) {
     if (device) {
       float* row = e->d_ir + (size_t)j * PB;
-      if (n) ENG_CUDA(cudaMemcpyAsync(row, ir[j], n * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
-      ENG_CUDA(cudaMemsetAsync(row + n, 0, (PB - n) * sizeof(float), e->stream));
+      if (n) ENG_CUDA(cudaMemcpyAsync(row, ir[j], n * sizeof(float), cudaMemcpyDeviceToDevice, e->upd_stream));
+      ENG_CUDA(cudaMemsetAsync(row + n, 0, (PB - n) * sizeof(float), e->upd_stream));
     } else {
       float* row = e->h_ir + (size_t)j * PB;
       if (n) std::memcpy(row, ir[j], n * sizeof(float));
       std::memset(row + n, 0, (PB - n) * sizeof(float));
     }
-    EngChan& ch = e->h_chans[s.slot0 + j];
-    e->h_upd[j] = EngUpd{(int)(s.slot0 + j), 1 - ch.active, (int64_t)PB};
-    ch.pending = 1;
   }
   if (!device)
-    ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, need * sizeof(float), cudaMemcpyHostToDevice, e->stream));
-  ENG_CUDA(cudaMemcpyAsync(e->d_upd, e->h_upd, s.C * sizeof(EngUpd), cudaMemcpyHostToDevice, e->stream));
-  ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_ir, e->d_upd, s.C, s.P, e->d_tw, e->stream));
-  e->n_ir += 1;
-  // tail of the new IR for the coming block, from the current delay line
-  if (s.nitem)
-    ENG_CUDA(tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, s.C * s.nitem, 1,
-                                   std::min(e->tail_grid, s.C * s.nitem), e->stream));
+    ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, need * sizeof(float), cudaMemcpyHostToDevice, e->upd_stream));
+  ENG_CUDA(cudaMemcpyAsync(e->d_upd, e->h_upd, s.C * sizeof(EngUpd), cudaMemcpyHostToDevice, e->upd_stream));
+  ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_ir, e->d_upd, s.C, s.P, e->d_tw,
+                               e->upd_stream));
+  ENG_CUDA(cudaEventRecord(s.staged_ev, e->upd_stream));
+  // BLOCK_UNTIL_READY: the new IR is ready for the next block when this returns
+  if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) ENG_CUDA(cudaEventSynchronize(s.staged_ev));
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    auto it = e->sessions.find(session);
+    if (it != e->sessions.end()) it->second.staged = true;
+    e->n_ir += 1;
+  }
   return TANB_OK;
 }
 
-int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const float* const* ir, size_t n) {
-  return engine_update(e, session, ir, n, false);
+int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const float* const* ir, size_t n,
+                                       uint32_t operationFlags) {
+  return engine_update(e, session, ir, n, false, operationFlags);
 }
 
 int32_t tanb_engine_update_response_td_device(tanb_engine* e, int32_t session, const float* const* ir,
-                                              size_t n) {
-  return engine_update(e, session, ir, n, true);
+                                              size_t n, uint32_t operationFlags) {
+  return engine_update(e, session, ir, n, true, operationFlags);
 }
 
 int32_t tanb_engine_io(tanb_engine* e, float** in, float** out) {
@@ -507,6 +565,7 @@ int32_t tanb_engine_process(tanb_engine* e) {
   std::lock_guard<std::mutex> lock(e->mu);
   ENG_CUDA(cudaSetDevice(e->ctx->device));
   if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
+  ENG_CUDA(commit_updates(e));
   ENG_CUDA(ensure_graph(e));
   ENG_CUDA(cudaGraphLaunch(e->graph_exec, e->stream));
   ENG_CUDA(cudaEventSynchronize(e->ev_out));
@@ -523,6 +582,7 @@ int32_t tanb_engine_process_device(tanb_engine* e, const float* in, float* out, 
   ENG_CUDA(cudaSetDevice(e->ctx->device));
   if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
   if (ld == 0) ld = e->B;
+  ENG_CUDA(commit_updates(e));
   if (e->profiling) ENG_CUDA(cudaEventRecord(e->pa, e->stream));
   ENG_CUDA(tanb::eng_launch_head(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, in, out, (int)ld, e->d_tw,
                                  e->stream));
@@ -549,6 +609,7 @@ int32_t tanb_engine_synchronize(tanb_engine* e) {
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   std::lock_guard<std::mutex> lock(e->mu);
   ENG_CUDA(cudaSetDevice(e->ctx->device));
+  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
   ENG_CUDA(cudaStreamSynchronize(e->stream));
   return TANB_OK;
 }
@@ -575,6 +636,17 @@ int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
   out[5] = (int64_t)e->budget;
   out[6] = tail_bytes;
   out[7] = e->tail_grid;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_session_state(tanb_engine* e, int32_t session, int64_t out[3]) {
+  if (!e || !out) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->sessions.find(session);
+  if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
+  out[0] = it->second.blocks;
+  out[1] = it->second.last_swap_block;
+  out[2] = it->second.staged ? 1 : 0;
   return TANB_OK;
 }
 

@@ -3,8 +3,8 @@
 //
 //   eng_ir_kernel    one CTA per (IR partition, updated channel): R2C of the
 //                    partition, optional FP16/BF16 quantisation with a
-//                    power-of-two per-partition scale, stored in the idle slot;
-//                    marks the channel's new IR pending
+//                    power-of-two per-partition scale, stored in the idle slot
+//                    (runs on the engine's update stream)
 //   eng_head_kernel  one CTA per channel slot: as the single-object head, but
 //                    the tail comes from the channel's work-item partial sums
 //                    (added in a fixed order) and the delay-line position and
@@ -119,7 +119,6 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   const float inv = 1.0f / scale;  // exact: power of two
   for (int k = threadIdx.x; k < M; k += T)
     SpecT<SPEC>::put(ch.H, spec_index(ch, u.slot, part, M) + k, make_float2(sm[k].x * inv, sm[k].y * inv));
-  if (part == 0 && threadIdx.x == 0) chans[u.chan].pending = 1;
 }
 
 // ---------------------------------------------------------------------------

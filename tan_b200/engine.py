@@ -27,16 +27,26 @@ class Session:
     def slots(self) -> slice:
         return slice(self.first_slot, self.first_slot + self.channels)
 
-    def update_response_td(self, ir: np.ndarray) -> int:
+    def update_response_td(self, ir: np.ndarray, block_until_ready: bool = False) -> int:
+        """New IR for every channel of the session; with block_until_ready the
+        swap lands on the next block, otherwise on the first block after the
+        transform (done on the engine's update stream) has finished."""
         ir = np.ascontiguousarray(ir, dtype=np.float32)
         rows = (ctypes.c_void_p * self.channels)(*[ir[c].ctypes.data for c in range(self.channels)])
-        return lib().tanb_engine_update_response_td(self.engine._h, self.id, rows, ir.shape[1])
+        return lib().tanb_engine_update_response_td(self.engine._h, self.id, rows, ir.shape[1],
+                                                    1 if block_until_ready else 0)
 
-    def update_response_td_device(self, ir) -> int:
+    def update_response_td_device(self, ir, block_until_ready: bool = False) -> int:
         """IR rows resident on the device: a (channels, n) CUDA tensor."""
         base, stride = ir.data_ptr(), ir.stride(0) * ir.element_size()
         rows = (ctypes.c_void_p * self.channels)(*[base + c * stride for c in range(self.channels)])
-        return lib().tanb_engine_update_response_td_device(self.engine._h, self.id, rows, ir.shape[1])
+        return lib().tanb_engine_update_response_td_device(self.engine._h, self.id, rows, ir.shape[1],
+                                                           1 if block_until_ready else 0)
+
+    def state(self) -> dict:
+        out = (ctypes.c_int64 * 3)()
+        lib().tanb_engine_session_state(self.engine._h, self.id, out)
+        return {"blocks": out[0], "last_swap_block": out[1], "staged": bool(out[2])}
 
     def close(self) -> int:
         return lib().tanb_engine_close_session(self.engine._h, self.id)

@@ -58,16 +58,49 @@ def percentiles(lat_ms):
 def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256, spectrum=eng.SPECTRUM_FP32,
           budget=150 << 30, max_channels=1 << 16, ch_range=(1, 8), len_range=(8192, 524288), seed=20261203 + 4,
           prefill=True):
-    """Runs the serving loop; returns a dict of latency and occupancy statistics."""
+    """Runs the serving loop; returns a dict of latency and occupancy statistics.
+
+    The audio thread admits and retires sessions and runs one engine block per
+    block period; a control-plane thread produces IRs and uploads them with
+    UpdateResponseTD (asynchronous: a swap lands on the first block after its
+    transform finished) and closes retired sessions, as the reference's update
+    thread does for TANConvolution. The audio input buffer is filled once (the
+    caller's audio I/O would write it in place); the block latency is the host
+    wall time of admission + engine block."""
+    import queue
+    import threading
+
     g = np.random.Generator(np.random.PCG64(seed))
+    gw = np.random.Generator(np.random.PCG64(seed + 1))  # the control thread's own stream
     pool = IRPool(g, length=len_range[1])
     e = eng.Engine(ctx, block, spectrum, budget_bytes=budget, max_channels=max_channels)
+    e.inp[:] = g.uniform(-1.0, 1.0, e.inp.shape).astype(np.float32)
     deadline_ms = 1000.0 * block / FS
     nblocks = int(seconds * FS / block)
     dt = block / FS
-    live = {}  # id -> (session, end_time, next_swap_time)
-    refused = 0
-    admitted = 0
+    work = queue.Queue()
+    errors = []
+
+    def control():
+        while True:
+            item = work.get()
+            if item is None:
+                return
+            kind, sess = item
+            try:
+                if kind == "ir":
+                    rc = sess.update_response_td(pool.get(gw, sess.channels, sess.ir_length))
+                else:
+                    rc = sess.close()
+                if rc != cv.AMF_OK:
+                    errors.append((kind, rc, cv.last_error()))
+            except Exception as ex:  # noqa: BLE001
+                errors.append((kind, -1, repr(ex)))
+
+    ctl = threading.Thread(target=control, daemon=True)
+    ctl.start()
+    live = {}  # id -> [session, end_time, next_swap_time]
+    refused = admitted = 0
     lat, chans = [], []
     t = 0.0
     next_arrival = g.exponential(1.0 / rate)
@@ -81,41 +114,41 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
             refused += 1
             return
         admitted += 1
-        s.update_response_td(pool.get(g, C, L))
+        work.put(("ir", s))
         live[s.id] = [s, now + g.exponential(lifetime), now + g.exponential(1.0 / swap_rate)]
 
     if prefill:  # start in steady state: rate x lifetime sessions already running
         for _ in range(int(rate * lifetime)):
             new_session(0.0)
-    x = g.uniform(-1.0, 1.0, (max_channels, block)).astype(np.float32)
+        while not work.empty():
+            time.sleep(0.01)
+    nch = sum(v[0].channels for v in live.values())
     for k in range(nblocks):
         t0 = time.perf_counter()
         while next_arrival <= t:
             new_session(t)
             next_arrival += g.exponential(1.0 / rate)
         for sid in [sid for sid, v in live.items() if v[1] <= t]:
-            live.pop(sid)[0].close()
+            work.put(("close", live.pop(sid)[0]))
         for v in live.values():
             if v[2] <= t:
-                s = v[0]
-                s.update_response_td(pool.get(g, s.channels, s.ir_length))
+                work.put(("ir", v[0]))
                 v[2] = t + g.exponential(1.0 / swap_rate)
-        info_ch = 0
-        for v in live.values():
-            s = v[0]
-            e.inp[s.slots] = x[s.slots]
-            info_ch += s.channels
-        rc = e.process() if live else cv.AMF_OK
+        rc = e.process()
         assert rc == cv.AMF_OK, cv.last_error()
         lat.append(1000.0 * (time.perf_counter() - t0))
-        chans.append(info_ch)
+        chans.append(e.info()["channels"])
         t += dt
+    work.put(None)
+    ctl.join()
     e.synchronize()
+    info = e.info()
     e.release()
     lat = np.asarray(lat)
     return {"blocks": nblocks, "deadline_ms": deadline_ms, "latency_ms": percentiles(lat),
             "deadline_misses": int((lat > deadline_ms).sum()), "concurrent_channels_mean": float(np.mean(chans)),
             "concurrent_channels_max": int(np.max(chans)), "admitted": admitted, "refused": refused,
+            "control_errors": errors[:5], "arena_bytes_end": info["arena_bytes"],
             "spectrum": ["fp32", "fp16", "bf16"][spectrum]}
 
 

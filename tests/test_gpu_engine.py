@@ -46,7 +46,7 @@ def run_engine(engine, sessions, nb, close_at=None, open_late=None):
             s = sessions[i]
             kk = k - s["start"]
             if kk in s["events"]:
-                assert sess.update_response_td(s["events"][kk]) == 0
+                assert sess.update_response_td(s["events"][kk], block_until_ready=True) == 0
             engine.inp[sess.slots] = s["x"][:, kk * B:(kk + 1) * B]
         assert engine.process() == 0, cv.last_error()
         for i, sess in live.items():
@@ -134,4 +134,43 @@ def test_engine_admission_by_budget(tan_ctx):
     rc, s = engine.open_session(2, 65536)
     assert rc == 0
     assert engine.process() == 0
+    engine.release()
+
+
+def test_engine_async_update_from_another_thread(tan_ctx):
+    """IR updates issued from a second thread while blocks run: the swap lands
+    on the first block after the upload finished (reported by the engine), and
+    the output equals the plain path with the swap at that block."""
+    import threading
+
+    g = H.rng(34)
+    B, nb, C, L = 256, 60, 2, 30000
+    x = H.noise(g, C, nb * B)
+    h0, h1 = H.irs(g, C, L), H.irs(g, C, L)
+    engine = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=256 << 20, max_channels=8)
+    rc, sess = engine.open_session(C, L)
+    assert rc == 0
+    assert sess.update_response_td(h0, block_until_ready=True) == 0
+    y = np.zeros((C, nb * B), np.float32)
+    started = threading.Event()
+
+    def worker():
+        started.wait()
+        assert sess.update_response_td(h1) == 0
+
+    t = threading.Thread(target=worker)
+    t.start()
+    for k in range(nb):
+        if k == 10:
+            started.set()
+        engine.inp[sess.slots] = x[:, k * B:(k + 1) * B]
+        assert engine.process() == 0, cv.last_error()
+        y[:, k * B:(k + 1) * B] = engine.out[sess.slots]
+    t.join()
+    st = sess.state()
+    k_swap = st["last_swap_block"]
+    assert st["blocks"] == nb and 10 <= k_swap < nb and not st["staged"]
+    ya = alone(tan_ctx, x, B, {0: h0, k_swap: h1})
+    rms = np.sqrt(np.mean(ya.astype(np.float64) ** 2))
+    assert np.max(np.abs(y - ya)) <= TOL * rms
     engine.release()
