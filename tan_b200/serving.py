@@ -122,7 +122,6 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
             new_session(0.0)
         while not work.empty():
             time.sleep(0.01)
-    nch = sum(v[0].channels for v in live.values())
     for k in range(nblocks):
         t0 = time.perf_counter()
         while next_arrival <= t:
@@ -160,7 +159,7 @@ def _block_latencies_batched(ctx, nsess, C, L, block, spectrum, blocks, g, pool)
         if rc != cv.AMF_OK:
             e.release()
             return None
-        s.update_response_td(pool.get(g, C, L))
+        s.update_response_td(pool.get(g, C, L), block_until_ready=True)
         sess.append(s)
     x = g.uniform(-1, 1, (nsess * C + 8, block)).astype(np.float32)
     lat = []
