@@ -295,6 +295,46 @@ int32_t tanb_engine_session_state(tanb_engine* engine, int32_t session, int64_t 
 int32_t tanb_engine_profile(tanb_engine* engine, int32_t enable);
 int32_t tanb_engine_profile_read(tanb_engine* engine, int64_t counts[4], double ms[2]);
 
+/* ---------------------------------------------------------------------------
+ * Non-uniformly partitioned convolution: the TAN_CONVOLUTION_METHOD_*_NONUNIFORM
+ * family (CPU variant ConvolutionImpl.cpp:224-246, 2416-2428; GPU two-stream
+ * engine tan/tanlibrary/src/Graal2/Reverberate.cpp), with a level schedule of
+ * block sizes that grow along the IR. Zero added latency: level l (block N_l,
+ * K_l partitions) starts at tap o_l >= N_l, so only the first level is on a
+ * block's critical path.
+ * ------------------------------------------------------------------------- */
+typedef struct tanb_nu tanb_nu;
+
+/* Default schedule: two partitions per size from base_block doubling up to
+ * max_block, the largest size covering the rest of the IR. Arrays hold >= 16. */
+int32_t tanb_nu_schedule(uint32_t ir_length, uint32_t base_block, uint32_t max_block, uint32_t* nlevels,
+                         uint32_t* level_block, uint32_t* level_parts);
+
+/* C channels, IR length, levels (block sizes nondecreasing powers of two in
+ * [32, 8192], level 0's block = the base block; each level's first tap >= its
+ * block), spectrum TANB_SPECTRUM_*. */
+int32_t tanb_nu_create(tanb_context* ctx, uint32_t channels, uint32_t ir_length, uint32_t nlevels,
+                       const uint32_t* level_block, const uint32_t* level_parts, uint32_t spectrum, tanb_nu** nu);
+int32_t tanb_nu_release(tanb_nu* nu);
+
+/* Host IR rows (n <= ir_length), transformed synchronously; takes effect at the
+ * next block without a crossfade (the levels' queued contributions of the old
+ * IR still play out). */
+int32_t tanb_nu_set_response(tanb_nu* nu, const float* const* ir, size_t n);
+
+/* Pinned host I/O [channels][base_block] and one base block through them. */
+int32_t tanb_nu_io(tanb_nu* nu, float** in, float** out);
+int32_t tanb_nu_process(tanb_nu* nu);
+
+/* One base block with device I/O, rows of `ld` floats; asynchronous. */
+int32_t tanb_nu_process_device(tanb_nu* nu, const float* in, float* out, uint32_t ld);
+int32_t tanb_nu_synchronize(tanb_nu* nu);
+void* tanb_nu_stream(tanb_nu* nu);
+
+/* out[0] channels, out[1] base block, out[2] levels, out[3] device bytes,
+ * out[4] average algorithmic tail bytes per base block, out[5] blocks done. */
+int32_t tanb_nu_info(tanb_nu* nu, int64_t out[6]);
+
 /* No reference counterpart. One-shot convolution that allocates no device
  * memory, for callers that cannot call cudaMalloc on this path -- e.g. a
  * plugin inside a host application's real-time audio callback, where an

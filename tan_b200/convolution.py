@@ -104,6 +104,17 @@ SIGNATURES = {
     "tanb_engine_session_state": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_engine_profile": (_i32, [_vp, _i32]),
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
+    "tanb_nu_schedule": (_i32, [_u32, _u32, _u32, _u32p, _u32p, _u32p]),
+    "tanb_nu_create": (_i32, [_vp, _u32, _u32, _u32, _u32p, _u32p, _u32, ctypes.POINTER(_vp)]),
+    "tanb_nu_release": (_i32, [_vp]),
+    "tanb_nu_set_response": (_i32, [_vp, _pp, _sz]),
+    "tanb_nu_io": (_i32, [_vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
+                          ctypes.POINTER(ctypes.POINTER(ctypes.c_float))]),
+    "tanb_nu_process": (_i32, [_vp]),
+    "tanb_nu_process_device": (_i32, [_vp, _vp, _vp, _u32]),
+    "tanb_nu_synchronize": (_i32, [_vp]),
+    "tanb_nu_stream": (_vp, [_vp]),
+    "tanb_nu_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_convolve_no_alloc": (_i32, [_vp, _vp, _vp, _u32, _sz, _sz, _u32, _vp]),
     "tanb_last_error": (ctypes.c_char_p, []),
 }
