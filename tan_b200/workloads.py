@@ -1,0 +1,220 @@
+"""Measurements of the path on each benchmark configuration (seeded synthetic
+inputs with the configurations' shapes; no public dataset is involved).
+
+    python -m tan_b200.workloads cfg1|cfg3|cfg4|nu-tune [--quick]
+
+cfg1  drop-in TANConvolution, 2 ch, B=1024, IR 8192, 200 blocks, FP32
+cfg3  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096..262144,
+      input at -6 dBFS, FP32 / FP16 / BF16 spectra; error vs FP64 per channel
+cfg4  non-uniform partitions, 256 ch, IR 2^20, base block 128, schedule from the
+      autotuner, FP32 / FP16; error vs FP64 on sampled channels
+Each prints one JSON object: throughput (GSamples/s), per-block latency
+percentiles, and error in dB (20 log10 rms(err) / rms(ref)).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import convolution as cv
+from . import engine as eng
+from . import nupols
+
+FS = 48000
+
+
+def _rng(i):
+    return np.random.Generator(np.random.PCG64(20261203 + i))
+
+
+def _ir(g, n, rt60):
+    t = np.arange(n, dtype=np.float64)
+    h = g.standard_normal(n) * np.exp(-np.log(1000.0) * t / (rt60 * FS))
+    return (h / np.linalg.norm(h)).astype(np.float32)
+
+
+def _conv64(x, h):
+    n = 1
+    while n < x.size + h.size - 1:
+        n <<= 1
+    return np.fft.irfft(np.fft.rfft(x.astype(np.float64), n) * np.fft.rfft(h.astype(np.float64), n), n)[: x.size]
+
+
+def _db(y, ref):
+    e = np.sqrt(np.mean((y.astype(np.float64) - ref) ** 2))
+    r = np.sqrt(np.mean(ref ** 2))
+    return float(20 * np.log10(e / r)) if e > 0 else -999.0
+
+
+def _pct(a):
+    a = np.asarray(a)
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "max": float(a.max())}
+
+
+def cfg1(ctx, quick=False):
+    g = _rng(0)
+    C, B, L, nb = 2, 1024, 8192, 200
+    x = g.uniform(-1, 1, (C, nb * B)).astype(np.float32)
+    h = np.stack([_ir(g, L, 0.3) for _ in range(C)])
+    conv = cv.TANConvolution(ctx)
+    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_PARTITIONED_UNIFORM, L, B, C) == 0
+    assert conv.UpdateResponseTD(h, L) == 0
+    y = np.zeros_like(x)
+    lat = []
+    for k in range(nb):
+        xs = np.ascontiguousarray(x[:, k * B:(k + 1) * B])
+        ys = np.zeros_like(xs)
+        t0 = time.perf_counter()
+        rc, _ = conv.Process(xs, ys, B)
+        lat.append(1e3 * (time.perf_counter() - t0))
+        y[:, k * B:(k + 1) * B] = ys
+    conv.Release()
+    # block 0 crossfades from the initial zero IR
+    err = []
+    for c in range(C):
+        ref = _conv64(x[c], h[c])
+        ref[:B] *= np.arange(B) / B
+        err.append(_db(y[c], ref))
+    return {"config": "cfg1", "channels": C, "block": B, "ir": L, "blocks": nb,
+            "gsamples_per_s_host": C * B * nb / (sum(lat) / 1e3) / 1e9, "latency_ms": _pct(lat),
+            "error_db_vs_fp64": err}
+
+
+def cfg3(ctx, quick=False):
+    g = _rng(2)
+    C, B = (256 if quick else 1024), 256
+    nb = 48
+    lens = np.exp(g.uniform(np.log(4096), np.log(262144), C)).astype(int)
+    x = (g.uniform(-1, 1, (C, nb * B)) * 10 ** (-6 / 20)).astype(np.float32)
+    irs = [_ir(g, int(L), float(g.uniform(0.2, 3.0))) for L in lens]
+    sample = g.choice(C, 32, replace=False)
+    refs = {int(c): _conv64(x[c], irs[c]) for c in sample}
+    out = {"config": "cfg3", "channels": C, "block": B, "ir_lengths": [int(lens.min()), int(np.median(lens)),
+                                                                       int(lens.max())], "blocks": nb}
+    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp16", eng.SPECTRUM_FP16), ("bf16", eng.SPECTRUM_BF16)):
+        e = eng.Engine(ctx, B, spec, budget_bytes=60 << 30, max_channels=C)
+        sess = []
+        for c in range(C):
+            rc, s = e.open_session(1, int(lens[c]))
+            assert rc == 0, cv.last_error()
+            sess.append(s)
+        for c in range(C):
+            assert sess[c].update_response_td(irs[c][None, :], block_until_ready=True) == 0
+        y = np.zeros_like(x)
+        lat = []
+        for k in range(nb):
+            for c in range(C):
+                e.inp[sess[c].first_slot] = x[c, k * B:(k + 1) * B]
+            t0 = time.perf_counter()
+            assert e.process() == 0
+            lat.append(1e3 * (time.perf_counter() - t0))
+            for c in range(C):
+                y[c, k * B:(k + 1) * B] = e.out[sess[c].first_slot]
+        info = e.info()
+        e.release()
+        errs = []
+        for c in sample:
+            ref = refs[int(c)].copy()
+            ref[:B] *= np.arange(B) / B
+            errs.append(_db(y[c], ref))
+        out[name] = {"error_db_vs_fp64": {"min": min(errs), "median": float(np.median(errs)), "max": max(errs),
+                                          "channels_sampled": len(errs)},
+                     "latency_ms": _pct(lat[4:]), "tail_bytes_per_block": info["tail_bytes_per_block"],
+                     "device_bytes": info["arena_bytes"]}
+    return out
+
+
+def tune_nu(ctx, C, L, B0, max_blocks=(1024, 2048, 4096, 8192), mids=(1, 2), spectrum=0, periods=2):
+    """Times candidate schedules over whole periods of the largest level and
+    returns them sorted by mean block time (device-resident input)."""
+    import torch
+
+    res = []
+    g = _rng(40)
+    for mb in max_blocks:
+        for mid in mids:
+            lv = nupols.schedule(L, B0, mb)
+            if mid == 1 and len(lv) > 2:
+                # single partitions in the middle levels, the first level keeps two
+                lv = [lv[0]] + [(b, 1) for b, _ in lv[1:-1]] + [lv[-1]]
+                off = sum(b * k for b, k in lv[:-1])
+                lv[-1] = (lv[-1][0], -(-(L - off) // lv[-1][0]))
+            try:
+                nu = nupols.NonUniform(ctx, C, L, lv, spectrum)
+            except cv.TANError:
+                continue
+            period = lv[-1][0] // B0
+            n = period * periods
+            x = torch.from_numpy(g.uniform(-1, 1, (C, B0 * n)).astype(np.float32)).cuda()
+            y = torch.zeros_like(x)
+            st = torch.cuda.ExternalStream(nu.stream())
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+            for k in range(n):
+                ev[k][0].record(st)
+                nu.process_device(x.data_ptr() + k * B0 * 4, y.data_ptr() + k * B0 * 4, B0 * n)
+                ev[k][1].record(st)
+            nu.synchronize()
+            ms = [a.elapsed_time(b) for a, b in ev]
+            res.append({"levels": lv, "mean_ms": float(np.mean(ms[period:])), "max_ms": float(np.max(ms[period:])),
+                        "tail_bytes_per_block": nu.info()["tail_bytes_per_block"]})
+            nu.release()
+            del x, y
+    res.sort(key=lambda r: r["mean_ms"])
+    return res
+
+
+def cfg4(ctx, quick=False):
+    g = _rng(3)
+    C, L, B0 = (64 if quick else 256), 1 << 20, 128
+    deadline = 1000.0 * B0 / FS
+    cands = tune_nu(ctx, C, L, B0)
+    ok = [r for r in cands if r["max_ms"] < deadline] or cands
+    best = ok[0]
+    nb = 600 if quick else 2000
+    x = g.uniform(-1, 1, (C, nb * B0)).astype(np.float32)
+    irs = np.stack([_ir(g, L, 8.0) for _ in range(C)])
+    sample = [0, C // 2, C - 1]
+    refs = {c: _conv64(x[c], irs[c]) for c in sample}
+    out = {"config": "cfg4", "channels": C, "ir": L, "base_block": B0, "blocks": nb, "deadline_ms": deadline,
+           "autotuner": [{"levels": r["levels"], "mean_ms": r["mean_ms"], "max_ms": r["max_ms"]} for r in cands],
+           "schedule": best["levels"]}
+    for name, spec in (("fp32", 0), ("fp16", 1)):
+        nu = nupols.NonUniform(ctx, C, L, best["levels"], spec)
+        assert nu.set_response(irs) == 0
+        y = np.zeros_like(x)
+        lat = []
+        for k in range(nb):
+            nu.inp[:] = x[:, k * B0:(k + 1) * B0]
+            t0 = time.perf_counter()
+            assert nu.process() == 0
+            lat.append(1e3 * (time.perf_counter() - t0))
+            y[:, k * B0:(k + 1) * B0] = nu.out
+        info = nu.info()
+        nu.release()
+        out[name] = {"error_db_vs_fp64": [_db(y[c], refs[c]) for c in sample], "latency_ms": _pct(lat),
+                     "gsamples_per_s_host": C * B0 * nb / (sum(lat) / 1e3) / 1e9,
+                     "deadline_misses": int((np.asarray(lat) > deadline).sum()),
+                     "device_bytes": info["device_bytes"], "avg_tail_bytes_per_block": info["tail_bytes_per_block"]}
+    # the same IR as uniform partitions (block 128) would stream this many bytes per block
+    out["uniform_tail_bytes_per_block"] = C * ((L // B0) - 1) * B0 * 16
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("which", choices=["cfg1", "cfg3", "cfg4", "nu-tune"])
+    ap.add_argument("--quick", action="store_true")
+    a = ap.parse_args()
+    ctx = cv.TANContext(0)
+    if a.which == "nu-tune":
+        r = tune_nu(ctx, 64 if a.quick else 256, 1 << 20, 128)
+    else:
+        r = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4}[a.which](ctx, a.quick)
+    print(json.dumps(r))
+
+
+if __name__ == "__main__":
+    main()
