@@ -473,6 +473,23 @@ cudaError_t enqueue_nu_block(tanb_nu* v, const float* in, float* out, int ld, bo
   return cudaGetLastError();
 }
 
+// The host-buffer block as one CUDA graph, captured once. Creation calls this
+// so that module loading, instantiation and the upload of the graph to the
+// device are not paid by the first audio block.
+cudaError_t ensure_graph(tanb_nu* v) {
+  if (v->graph) return cudaSuccess;
+  cudaGraph_t g = nullptr;
+  cudaError_t r = cudaStreamBeginCapture(v->stream, cudaStreamCaptureModeThreadLocal);
+  if (r != cudaSuccess) return r;
+  r = enqueue_nu_block(v, v->d_in, v->d_out, v->d.B0, true);
+  cudaError_t r2 = cudaStreamEndCapture(v->stream, &g);
+  if (r == cudaSuccess) r = r2;
+  if (r == cudaSuccess) r = cudaGraphInstantiate(&v->graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (r == cudaSuccess) r = cudaGraphUpload(v->graph, v->stream);
+  return r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -570,11 +587,17 @@ int32_t tanb_nu_create(tanb_context* ctx, uint32_t channels, uint32_t ir_length,
     if ((e = nu_alloc(v, &p, 2 * N * sizeof(float2))) != cudaSuccess) break;
     std::vector<float2> tw(2 * N);
     tanb::make_twiddles((int)(2 * N), tw.data());
-    if ((e = cudaMemcpy(p, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    // Ordered after this buffer's zero fill, which is queued on the same
+    // (non-blocking) stream; a copy on another stream could land first and
+    // then be zeroed. A pageable source is staged before the call returns.
+    if ((e = cudaMemcpyAsync(p, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, v->stream)) !=
+        cudaSuccess)
+      break;
     d.tw[l] = (const float2*)p;
   }
   if (e == cudaSuccess) e = cudaMallocHost(&v->h_in, C * d.B0 * sizeof(float));
   if (e == cudaSuccess) e = cudaMallocHost(&v->h_out, C * d.B0 * sizeof(float));
+  if (e == cudaSuccess) e = ensure_graph(v);
   if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
   if (e != cudaSuccess) {
     nu_free(v);
@@ -628,17 +651,7 @@ int32_t tanb_nu_process(tanb_nu* v) {
   if (!v) return nfail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(v->mu);
   NU_CUDA(cudaSetDevice(v->ctx->device));
-  if (!v->graph) {
-    cudaGraph_t g = nullptr;
-    NU_CUDA(cudaStreamBeginCapture(v->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t r = enqueue_nu_block(v, v->d_in, v->d_out, v->d.B0, true);
-    cudaError_t r2 = cudaStreamEndCapture(v->stream, &g);
-    if (r != cudaSuccess) return nfail(TANB_FAIL, "capture: %s", cudaGetErrorString(r));
-    if (r2 != cudaSuccess) return nfail(TANB_FAIL, "capture: %s", cudaGetErrorString(r2));
-    r = cudaGraphInstantiate(&v->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (r != cudaSuccess) return nfail(TANB_FAIL, "instantiate: %s", cudaGetErrorString(r));
-  }
+  NU_CUDA(ensure_graph(v));
   NU_CUDA(cudaGraphLaunch(v->graph, v->stream));
   NU_CUDA(cudaEventSynchronize(v->ev_out));
   v->k += 1;

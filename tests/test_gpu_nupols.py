@@ -82,3 +82,29 @@ def test_nu_rejects_schedules_that_add_latency(tan_ctx):
         nupols.NonUniform(tan_ctx, 1, 10000, [(128, 1), (256, 40)])  # level 1 starts at 128 < 256
     with pytest.raises(cv.TANError):
         nupols.NonUniform(tan_ctx, 1, 10000, [(128, 2), (256, 2)])  # does not cover the IR
+
+
+@pytest.mark.parametrize("C,levels,nb", [
+    (2, [(128, 2), (256, 1), (512, 1), (1024, 1), (2048, 1), (4096, 8)], 260),   # cfg4's shape, every level reached
+    (2, [(128, 2), (256, 2), (512, 2), (1024, 2), (2048, 6)], 200),
+    (64, [(128, 2), (256, 1), (512, 1), (1024, 5)], 64),
+    (2, [(128, 2), (256, 1), (512, 1), (1024, 1), (2048, 1), (4096, 1), (8192, 4)], 400),
+    # enough channels that the creation-time zero fills are still running when
+    # the twiddle tables are uploaded
+    (128, [(128, 2), (256, 1), (512, 1), (1024, 1), (2048, 1), (4096, 20)], 400),
+])
+def test_nu_signal_longer_than_every_level_offset(tan_ctx, C, levels, nb):
+    """The output window reaches every level's contributions, with several
+    blocks of each level (its tail included)."""
+    g = H.rng(sum(b * k for b, k in levels) + C)
+    L = nupols.coverage(levels)
+    B = levels[0][0]
+    assert nb * B > L // 2
+    x = H.noise(g, C, nb * B)
+    h = H.irs(g, C, L, (2.0, 4.0))
+    nu = nupols.NonUniform(tan_ctx, C, L, levels)
+    assert nu.set_response(h) == 0
+    y = nu.run(x)
+    for c in (range(C) if C <= 8 else (0, C // 2, C - 1)):
+        assert fp64.error_db(y[c], fp64.conv_fp64(x[c], h[c])) < -120, c
+    nu.release()
