@@ -279,6 +279,11 @@ int32_t td_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem 
 int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_t>& run,
                   std::vector<uint8_t>& flush);
 
+// Per-update descriptors, one upload: [ChanCtl x C][int channel list x C]
+// [8-byte aligned: IR row pointers x C].
+size_t uctl_ptr_offset(size_t C) { return ((sizeof(ChanCtl) + sizeof(int)) * C + 7) & ~size_t(7); }
+size_t uctl_bytes(size_t C) { return uctl_ptr_offset(C) + C * sizeof(void*); }
+
 int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags,
                       uint32_t op) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
@@ -290,7 +295,7 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   if (v->td) return td_update(v, mem, ir, n, flags, op);
   if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
 
-  const int C = v->C, PB = v->P * v->B;
+  const int C = v->C;
   std::vector<int> chans;
   for (int c = 0; c < C; ++c) {
     if (flags && (flags[c] & kFlush)) TANB_CUDA(flush_channel(v, c));
@@ -302,21 +307,22 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
 
   TANB_CUDA(cudaEventSynchronize(v->ev_ir));
   const int nch = (int)chans.size();
+  tanb::IrRows rows;
+  rows.n = (long long)n;
   if (mem == Mem::Host) {
-    for (int j = 0; j < nch; ++j) {
-      float* row = v->h_ir + (size_t)j * PB;
-      if (n) std::memcpy(row, ir[chans[j]], n * sizeof(float));
-      std::memset(row + n, 0, (PB - n) * sizeof(float));
-    }
-    TANB_CUDA(cudaMemcpyAsync(v->d_ir, v->h_ir, (size_t)nch * PB * sizeof(float), cudaMemcpyHostToDevice,
-                              v->stream));
+    // compact staging (row stride n); the kernel reads zeros past n
+    for (int j = 0; j < nch; ++j)
+      if (n) std::memcpy(v->h_ir + (size_t)j * n, ir[chans[j]], n * sizeof(float));
+    if (n)
+      TANB_CUDA(cudaMemcpyAsync(v->d_ir, v->h_ir, (size_t)nch * n * sizeof(float), cudaMemcpyHostToDevice,
+                                v->stream));
+    rows.base = v->d_ir;
+    rows.stride = (long long)n;
   } else {
-    for (int j = 0; j < nch; ++j) {
-      float* row = v->d_ir + (size_t)j * PB;
-      if (n)
-        TANB_CUDA(cudaMemcpyAsync(row, ir[chans[j]], n * sizeof(float), cudaMemcpyDeviceToDevice, v->stream));
-      TANB_CUDA(cudaMemsetAsync(row + n, 0, (PB - n) * sizeof(float), v->stream));
-    }
+    // the kernel reads the caller's rows in place
+    const float** up = reinterpret_cast<const float**>(v->h_uctl + uctl_ptr_offset(C));
+    for (int j = 0; j < nch; ++j) up[j] = ir[chans[j]];
+    rows.ptrs = reinterpret_cast<const float* const*>(v->d_uctl + uctl_ptr_offset(C));
   }
   for (int c : chans) {
     if (!v->pending[c]) {
@@ -328,13 +334,12 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   int* uch = reinterpret_cast<int*>(v->h_uctl + sizeof(ChanCtl) * C);
   for (int c = 0; c < C; ++c) uctl[c] = ChanCtl{v->pending[c], v->pending[c], v->active[c], v->slot_new[c]};
   for (int j = 0; j < nch; ++j) uch[j] = chans[j];
-  TANB_CUDA(cudaMemcpyAsync(v->d_uctl, v->h_uctl, (sizeof(ChanCtl) + sizeof(int)) * C, cudaMemcpyHostToDevice,
-                            v->stream));
+  TANB_CUDA(cudaMemcpyAsync(v->d_uctl, v->h_uctl, uctl_bytes(C), cudaMemcpyHostToDevice, v->stream));
   TANB_CUDA(cudaEventRecord(v->ev_ir, v->stream));
   const ChanCtl* d_uctl = reinterpret_cast<const ChanCtl*>(v->d_uctl);
   const int* d_uch = reinterpret_cast<const int*>(v->d_uctl + sizeof(ChanCtl) * C);
   TANB_CUDA(counted(v, tanb_convolution::kIr,
-                    [&] { return tanb::launch_ir_spectrum(v->ds, v->d_ir, d_uch, nch, d_uctl, v->stream); }));
+                    [&] { return tanb::launch_ir_spectrum(v->ds, rows, d_uch, nch, d_uctl, v->stream); }));
   // tail of the pending IR for the next block, from the current delay line
   if (v->P > 1)
     TANB_CUDA(counted(v, tanb_convolution::kTail,
@@ -477,25 +482,27 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       TANB_CUDA(counted(v, tanb_convolution::kHead, [&] { return tanb::launch_head(v->ds, ref, cur_b[b], v->stream); }));
       const bool last = (b == nb - 1);
       if (last) {
-        if (out_mem == Mem::Host)
-          TANB_CUDA(cudaMemcpyAsync(v->h_out, v->d_out, (size_t)nb * C * B * sizeof(float),
-                                    cudaMemcpyDeviceToHost, v->stream));
-        TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
         v->last_desc = dctl;
         v->last_is_param = param;
         if (param) v->last_pdesc = v->pdesc[b];
         v->last_cur = cur_b[b];
-        if (v->finalize_mode) {
-          v->finalize_due = true;
-        } else if (P > 1) {
-          TANB_CUDA(counted(v, tanb_convolution::kTail,
-                            [&] { return tanb::launch_tail(v->ds, ref, 0, cur_b[b], v->tiling, v->stream); }));
-        }
+      }
+      if (last && v->finalize_mode) {
+        v->finalize_due = true;
       } else if (P > 1) {
-        TANB_CUDA(counted(v, tanb_convolution::kTail,
-                          [&] { return tanb::launch_tail(v->ds, ref, 0, cur_b[b], v->tiling, v->stream); }));
+        // Directly behind the head (programmatic serialization): the tail
+        // streams partitions 2..P-1 while the head runs.
+        TANB_CUDA(counted(v, tanb_convolution::kTail, [&] {
+          return tanb::launch_tail(v->ds, ref, 0, cur_b[b], v->tiling, v->stream, true);
+        }));
       }
     }
+    // Outputs are final after the heads; in the default mode the last tail,
+    // which overlaps its head, completes before the copy as well.
+    if (out_mem == Mem::Host)
+      TANB_CUDA(cudaMemcpyAsync(v->h_out, v->d_out, (size_t)nb * C * B * sizeof(float), cudaMemcpyDeviceToHost,
+                                v->stream));
+    TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
     if (out_mem == Mem::Host) {
       TANB_CUDA(cudaEventSynchronize(v->ev_out));
       if (*v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
@@ -799,7 +806,7 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
   v->desc_bytes = (sizeof(ChanCtl) + 2 * sizeof(void*)) * Cs;
   const size_t stage_bytes = kMaxBlocksPerChunk * (v->desc_bytes + Cs * Bs * sizeof(float));
   const size_t out_floats = kMaxBlocksPerChunk * Cs * Bs;
-  const size_t uctl_bytes = (sizeof(ChanCtl) + sizeof(int)) * Cs;
+
   do {
     if ((e = dev_alloc(v, &v->ds.H, Cs * 2 * Ps * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->ds.fdl, Cs * Ps * Bs)) != cudaSuccess) break;
@@ -809,11 +816,11 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
     if ((e = dev_alloc(v, &v->d_stage, stage_bytes)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_out, out_floats)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_ir, Cs * Ps * Bs)) != cudaSuccess) break;
-    if ((e = dev_alloc(v, &v->d_uctl, uctl_bytes)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_uctl, uctl_bytes(C))) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_stage, stage_bytes)) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_out, out_floats * sizeof(float))) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_ir, Cs * Ps * Bs * sizeof(float))) != cudaSuccess) break;
-    if ((e = cudaMallocHost(&v->h_uctl, uctl_bytes)) != cudaSuccess) break;
+    if ((e = cudaMallocHost(&v->h_uctl, uctl_bytes(C))) != cudaSuccess) break;
     if ((e = cudaHostAlloc(&v->h_err, sizeof(int), cudaHostAllocMapped)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_stage, cudaEventDisableTiming)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_ir, cudaEventDisableTiming)) != cudaSuccess) break;

@@ -84,10 +84,19 @@ struct BlockRef {
   float* const* out = nullptr;
 };
 
+// Where the IR-spectrum kernel reads row j (the IR of channel chans[j]):
+// ptrs[j] when ptrs (a device array) is set, else base + j * stride. Samples
+// at and after n read as zero, so rows need no padding to P*B.
+struct IrRows {
+  const float* base = nullptr;
+  long long stride = 0;
+  const float* const* ptrs = nullptr;
+  long long n = 0;
+};
+
 // R2C of each IR partition into slot `slot_new` of the channels listed in
-// `chans` (device array of nch channel indices). `ir` is [nch][P*B] floats,
-// row j holding the zero-padded IR of channel chans[j].
-cudaError_t launch_ir_spectrum(const DevState& s, const float* ir, const int* chans, int nch,
+// `chans` (device array of nch channel indices).
+cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* chans, int nch,
                                const ChanCtl* ctl, cudaStream_t st);
 
 // Head of one block for every running channel: FFT of [prev, x], insert into
@@ -101,8 +110,13 @@ cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStrea
 //   tail[c][which] = sum_{i=1}^{P-1} FDL[c][(cur + i - 1) mod P] * H[c][slot][i]
 // which = 0: running channels, slot = swap ? slot_new : slot_cur
 // which = 1: channels with swap set (pending IR), slot = slot_new
+// pdl: launch with programmatic stream serialization. Only for a launch that
+// directly follows launch_head of the same block in the stream: the kernel
+// then streams partitions 2..P-1 while the head runs and waits for it before
+// partition 1 and before writing the tail buffer. Any other predecessor may
+// write what partitions >= 2 read, so every other launch passes false.
 cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, MacTiling t,
-                        cudaStream_t st);
+                        cudaStream_t st, bool pdl = false);
 
 // Per-channel descriptor of one TIME_DOMAIN call.
 struct TdChan {

@@ -15,12 +15,40 @@
 // overlap-save needs no overlap buffer and gives the exact new-IR output on a
 // swap block from the same delay line.
 #include <cmath>
+#include <utility>
 
 #include "tanb_fft.cuh"
 #include "tanb_internal.h"
 
 namespace tanb {
 namespace {
+
+// Programmatic dependent launch (sm_90+): a kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may begin once every CTA
+// of the kernel before it in the stream has executed launch_dependents (or
+// exited); griddepcontrol.wait then blocks until that kernel has completed and
+// its memory operations are visible. Without the attribute both are no-ops.
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Launch of `kernel`, with programmatic stream serialization when `pdl` is set.
+template <class... KArgs, class... Args>
+cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                     Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Descriptor sources for the head and tail kernels.
 struct DevDesc {
@@ -41,8 +69,7 @@ struct ParDesc {
 
 template <int LOG2M>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T)
-    ir_spectrum_kernel(DevState s, const float* __restrict__ ir, const int* __restrict__ chans,
-                       const ChanCtl* __restrict__ ctl) {
+    ir_spectrum_kernel(DevState s, IrRows ir, const int* __restrict__ chans, const ChanCtl* __restrict__ ctl) {
   using S = FftShape<LOG2M>;
   constexpr int M = S::M, T = S::T;
   extern __shared__ float2 sm[];
@@ -50,9 +77,17 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   const int row = blockIdx.y;
   const int c = chans[row];
   const int slot = ctl[c].slot_new;
-  const float* h = ir + (size_t)row * s.P * M + (size_t)part * M;
-  for (int n = threadIdx.x; n < M; n += T)
-    sm[n] = (n < M / 2) ? make_float2(h[2 * n], h[2 * n + 1]) : make_float2(0.f, 0.f);
+  const float* h = ir.ptrs ? ir.ptrs[row] : ir.base + (size_t)row * ir.stride;
+  const long long t0 = (long long)part * M;  // first sample of this partition
+  for (int n = threadIdx.x; n < M; n += T) {
+    const long long t = t0 + 2 * n;
+    float2 v = make_float2(0.f, 0.f);
+    if (n < M / 2) {
+      if (t < ir.n) v.x = h[t];
+      if (t + 1 < ir.n) v.y = h[t + 1];
+    }
+    sm[n] = v;
+  }
   __syncthreads();
   fft_inplace<LOG2M, false>(sm, s.tw);
   float2* H = s.H + h_index(s, c, slot, part);
@@ -76,6 +111,9 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   extern __shared__ float2 sm[];
   float2* z = sm;       // old / only IR
   float2* z2 = sm + M;  // new IR on a swap block
+  // The tail launched behind this kernel may start now: it reads nothing this
+  // kernel writes until its grid-dependency wait.
+  griddep_launch_dependents();
   const int c = blockIdx.x;
   const ChanCtl cc = desc.get_ctl(c);
   if (!cc.run) return;
@@ -194,16 +232,19 @@ __global__ void __launch_bounds__(UX* SY)
   const int u = blockIdx.x * UX + tx;
   const int P = s.P;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (u < U && P > 1) {
-    const float4* Hc = reinterpret_cast<const float4*>(s.H + h_index(s, c, slot, 0)) + u;
-    const float4* Fc = reinterpret_cast<const float4*>(s.fdl + (size_t)c * P * s.B) + u;
+  const bool act = u < U && P > 1;
+  const float4* Hc = reinterpret_cast<const float4*>(s.H + h_index(s, c, slot, 0)) + u;
+  const float4* Fc = reinterpret_cast<const float4*>(s.fdl + (size_t)c * P * s.B) + u;
+  const bool dc = (u == 0);
+  if (act) {
     const int nparts = P - 1;
     const int chunk = (nparts + SY - 1) / SY;
     const int i0 = 1 + ty * chunk;
     const int i1 = min(P, i0 + chunk);
-    int fs = (cur + i0 - 1) % P;
-    const bool dc = (u == 0);
-    int i = i0;
+    // Partition 1 multiplies the spectrum the preceding head kernel inserts
+    // into slot `cur`; row ty == 0 adds it after the grid-dependency wait.
+    int i = (i0 == 1) ? 2 : i0;
+    int fs = (cur + i - 1) % P;
     for (; i + D <= i1; i += D) {
       float4 h[D], f[D];
 #pragma unroll
@@ -222,6 +263,11 @@ __global__ void __launch_bounds__(UX* SY)
       acc = mac4(acc, f, h, dc);
     }
   }
+  // Waits for the head kernel of this block when launched behind it with
+  // programmatic serialization (returns at once otherwise): after this, its
+  // delay-line write is visible and its read of the tail buffer is done.
+  griddep_wait();
+  if (act && ty == 0) acc = mac4(acc, Fc[(size_t)cur * U], __ldg(Hc + (size_t)U), dc);
   if constexpr (SY > 1) {
     __shared__ float4 red[SY][UX];
     red[ty][tx] = acc;
@@ -295,6 +341,7 @@ __global__ void __launch_bounds__(BR / 2)
   const int c = blockIdx.y;
   const ChanCtl cc = desc.get_ctl(c);
   if (which == 0 ? !cc.run : !cc.swap) return;
+  griddep_wait();  // its first chunk holds partition 1 (see tail_kernel)
   const int slot = (which == 0) ? (cc.swap ? cc.slot_new : cc.slot_cur) : cc.slot_new;
   const int P = s.P;
   const int bin0 = blockIdx.x * BR;
@@ -377,7 +424,7 @@ cudaError_t set_attrs() {
 }
 
 template <int LOG2M>
-cudaError_t launch_ir_t(const DevState& s, const float* ir, const int* chans, int nch, const ChanCtl* ctl,
+cudaError_t launch_ir_t(const DevState& s, const IrRows& ir, const int* chans, int nch, const ChanCtl* ctl,
                         cudaStream_t st) {
   using S = FftShape<LOG2M>;
   dim3 grid(s.P, nch);
@@ -411,19 +458,18 @@ cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, cudaStr
   }
 
 template <int UX, int SY, int D>
-cudaError_t launch_tail_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st) {
+cudaError_t launch_tail_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st, bool pdl) {
   const int U = s.B >> 1;
   dim3 grid((U + UX - 1) / UX, s.C);
   dim3 block(UX, SY);
   if (d.param)
-    tail_kernel<UX, SY, D, ParDesc><<<grid, block, 0, st>>>(s, ParDesc{*d.param}, which, cur);
-  else
-    tail_kernel<UX, SY, D, DevDesc><<<grid, block, 0, st>>>(s, DevDesc{d.ctl, d.in, d.out}, which, cur);
-  return cudaGetLastError();
+    return launch_k(tail_kernel<UX, SY, D, ParDesc>, grid, block, 0, st, pdl, s, ParDesc{*d.param}, which, cur);
+  return launch_k(tail_kernel<UX, SY, D, DevDesc>, grid, block, 0, st, pdl, s, DevDesc{d.ctl, d.in, d.out}, which,
+                  cur);
 }
 
 template <int BR, int RS, int NS>
-cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st) {
+cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st, bool pdl) {
   if (s.B % BR != 0) return cudaErrorInvalidValue;
   constexpr int smem = bulk_smem_bytes<BR, RS, NS>();
   static cudaError_t attr = [] {
@@ -436,13 +482,13 @@ cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int c
   if (attr != cudaSuccess) return attr;
   dim3 grid(s.B / BR, s.C);
   if (d.param)
-    tail_bulk_kernel<BR, RS, NS, ParDesc><<<grid, BR / 2, smem, st>>>(s, ParDesc{*d.param}, which, cur);
-  else
-    tail_bulk_kernel<BR, RS, NS, DevDesc><<<grid, BR / 2, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, which, cur);
-  return cudaGetLastError();
+    return launch_k(tail_bulk_kernel<BR, RS, NS, ParDesc>, grid, dim3(BR / 2), smem, st, pdl, s,
+                    ParDesc{*d.param}, which, cur);
+  return launch_k(tail_bulk_kernel<BR, RS, NS, DevDesc>, grid, dim3(BR / 2), smem, st, pdl, s,
+                  DevDesc{d.ctl, d.in, d.out}, which, cur);
 }
 
-using TailLauncher = cudaError_t (*)(const DevState&, const BlockRef&, int, int, cudaStream_t);
+using TailLauncher = cudaError_t (*)(const DevState&, const BlockRef&, int, int, cudaStream_t, bool);
 struct TailEntry {
   MacTiling t;
   TailLauncher fn;
@@ -480,7 +526,7 @@ cudaError_t prepare_kernels() {
   return result;
 }
 
-cudaError_t launch_ir_spectrum(const DevState& s, const float* ir, const int* chans, int nch,
+cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* chans, int nch,
                                const ChanCtl* ctl, cudaStream_t st) {
   if (nch <= 0) return cudaSuccess;
   TANB_DISPATCH_LOG2(s.log2B, launch_ir_t, s, ir, chans, nch, ctl, st);
@@ -491,12 +537,12 @@ cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStrea
 }
 
 cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, MacTiling t,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool pdl) {
   if (s.P <= 1) return cudaSuccess;
   for (int i = 0; i < kTailCount; ++i)
     if (kTail[i].t.ux == t.ux && kTail[i].t.sy == t.sy && kTail[i].t.depth == t.depth &&
         kTail[i].t.kind == t.kind)
-      return kTail[i].fn(s, d, which, cur, st);
+      return kTail[i].fn(s, d, which, cur, st, pdl);
   return cudaErrorInvalidValue;
 }
 

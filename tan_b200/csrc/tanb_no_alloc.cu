@@ -166,7 +166,11 @@ extern "C" int32_t tanb_convolve_no_alloc(const float* in, const float* ir, floa
     describe_kernel<<<(unsigned)((C + 127) / 128), 128, 0, st>>>(ctl, in_rows, out_rows, chans, nullptr, nullptr,
                                                                  (int)C, samples, 0, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) break;
-    if ((e = tanb::launch_ir_spectrum(s, irp, chans, (int)C, ctl, st)) != cudaSuccess) break;
+    tanb::IrRows rows;
+    rows.base = irp;
+    rows.stride = (long long)(P * B);
+    rows.n = (long long)(P * B);
+    if ((e = tanb::launch_ir_spectrum(s, rows, chans, (int)C, ctl, st)) != cudaSuccess) break;
     int cur = 0;
     const size_t nb = samples / B;
     for (size_t b = 0; b < nb && e == cudaSuccess; ++b) {
@@ -179,7 +183,7 @@ extern "C" int32_t tanb_convolve_no_alloc(const float* in, const float* ir, floa
       ref.in = in_rows;
       ref.out = out_rows;
       if ((e = tanb::launch_head(s, ref, cur, st)) != cudaSuccess) break;
-      e = tanb::launch_tail(s, ref, 0, cur, tanb::MacTiling{32, 8}, st);
+      e = tanb::launch_tail(s, ref, 0, cur, tanb::MacTiling{32, 8}, st, true);
     }
   } while (0);
   if (e != cudaSuccess) {

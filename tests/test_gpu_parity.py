@@ -298,3 +298,40 @@ def test_every_tail_tiling_matches_restatement(tan_ctx, B, L):
         conv.Release()
         idx += 1
     assert tested >= 10
+
+
+@pytest.mark.parametrize("n_ir", [1, 777, 2999, 3000])
+def test_device_rows_update_equals_host_rows_update(tan_ctx, n_ir):
+    """UpdateResponseTD from device rows (read in place at any 4-byte offset,
+    zero past n) gives bit-identical outputs to the host-row update, for odd
+    and short lengths, with a swap mid-stream that skips a stopped channel."""
+    import torch
+
+    g = H.rng(60 + n_ir)
+    C, B, L, nb = 3, 256, 3000, 14
+    x = H.noise(g, C, nb * B)
+    h0 = np.ascontiguousarray(H.irs(g, C, L)[:, :n_ir])
+    h1 = np.ascontiguousarray(H.irs(g, C, L)[:, :n_ir])
+    stop1 = np.array([0, cv.TAN_CONVOLUTION_CHANNEL_FLAG_STOP_INPUT, 0], np.uint32)
+    host = make(tan_ctx, L, B, C)
+    y_host, _ = H.run_stream(host, x, B, {0: (h0, None), 7: (h1, stop1)})
+    dev = make(tan_ctx, L, B, C)
+    # rows one float past the start of a wider buffer: no alignment beyond 4 bytes
+    wide = torch.zeros((2, C, n_ir + 3), dtype=torch.float32, device="cuda")
+    wide[0, :, 1:n_ir + 1] = torch.from_numpy(h0)
+    wide[1, :, 1:n_ir + 1] = torch.from_numpy(h1)
+    rows = [[wide[s, c].data_ptr() + 4 for c in range(C)] for s in range(2)]
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros_like(xd)
+    for k in range(nb):
+        if k == 0:
+            assert dev.UpdateResponseTDDevice(rows[0], n_ir) == 0
+        if k == 7:
+            assert dev.UpdateResponseTDDevice(rows[1], n_ir, stop1) == 0
+        rc, done = dev.ProcessDevice([xd[c, k * B:(k + 1) * B] for c in range(C)],
+                                     [yd[c, k * B:(k + 1) * B] for c in range(C)], B)
+        assert rc == 0 and done == B
+    assert dev.Synchronize() == 0
+    assert np.array_equal(yd.cpu().numpy(), y_host)
+    host.Release()
+    dev.Release()
