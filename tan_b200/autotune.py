@@ -1,9 +1,9 @@
 """Autotuner for the partition multiply-accumulate (the tail kernel).
 
 For one shape (block B, IR length L, channels C) it runs the convolution on the
-device with every compiled tail tiling, timing the tail kernel with CUDA events
-on the object's stream (L2 flushed before every timed block), and keeps the
-fastest. Results are cached in tuning.json next to this file, keyed by shape;
+device with every compiled tail tiling, timing whole blocks (head plus the tail
+that overlaps it) with CUDA events on the object's stream, L2 flushed before
+every timed block, and keeps the tiling with the shortest block time. Results are cached in tuning.json next to this file, keyed by shape;
 TANConvolution objects created through `tuned()` apply the cached choice.
 
     python -m tan_b200.autotune --block 512 --length 65536 --channels 64
@@ -38,57 +38,77 @@ def save_cache(d: dict) -> None:
         json.dump(d, f, indent=1, sort_keys=True)
 
 
-def measure(ctx, B: int, L: int, C: int, steps: int = 40, warmup: int = 5, seed: int = 7):
-    """Returns [(index, (ux, sy, depth), mean tail us)] for every compiled tiling."""
+def measure(ctx, B: int, L: int, C: int, steps: int = 120, warmup: int = 8, seed: int = 7):
+    """Returns [(index, (ux, sy, depth), mean block us, mean tail us)] for every
+    compiled tiling. The block time is one Process call on device buffers (the
+    head, then the tail launched behind it so that the two overlap), timed with
+    CUDA events around the call; the tail time comes from a second pass with
+    events around each kernel launch (the tail then runs after its head)."""
     import torch
 
     g = np.random.Generator(np.random.PCG64(seed))
-    conv = cv.TANConvolution(ctx)
-    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == cv.AMF_OK, cv.last_error()
     dev = ctx.device
     h = torch.from_numpy((g.standard_normal((C, L)) * 0.01).astype(np.float32)).to(f"cuda:{dev}")
-    assert conv.UpdateResponseTDDevice(h, L) == 0
     x = torch.from_numpy(g.uniform(-1, 1, (C, B)).astype(np.float32)).to(f"cuda:{dev}")
     y = torch.zeros_like(x)
     flush_w = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
     flush_r = torch.ones(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
-    stream = torch.cuda.ExternalStream(conv.stream(), device=dev)
     results = []
     idx = 0
     while True:
+        conv = cv.TANConvolution(ctx)
+        assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == cv.AMF_OK, cv.last_error()
         rc, tiling = conv.tiling(idx)
         if rc != cv.AMF_OK:
+            conv.Release()
             break
         if tiling[0] > B // 2:  # more units per CTA row than the block has bin pairs
+            conv.Release()
             idx += 1
             continue
-        for k in range(warmup + steps):
-            if k == warmup:
-                conv.Synchronize()
-                conv.profile_read()
-                conv.profile(True)
+        assert conv.UpdateResponseTDDevice(h, L) == 0
+        stream = torch.cuda.ExternalStream(conv.stream(), device=dev)
+
+        def flush():
             with torch.cuda.stream(stream):
                 flush_w.zero_()
                 flush_r.sum()
-            rc, _ = conv.ProcessDevice(x, y, B)
-            assert rc == 0
+
+        for _ in range(warmup):
+            flush()
+            assert conv.ProcessDevice(x, y, B)[0] == 0
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            flush()
+            a.record(stream)
+            assert conv.ProcessDevice(x, y, B)[0] == 0
+            b.record(stream)
+        conv.Synchronize()
+        torch.cuda.synchronize()
+        block_us = 1000.0 * sum(a.elapsed_time(b) for a, b in ev) / steps
+        conv.profile_read()
+        conv.profile(True)
+        for _ in range(steps):
+            flush()
+            assert conv.ProcessDevice(x, y, B)[0] == 0
         conv.Synchronize()
         conv.profile(False)
         p = conv.profile_read()["tail"]
-        results.append((idx, tiling, 1000.0 * p["ms"] / max(1, p["timed"])))
+        results.append((idx, tiling, block_us, 1000.0 * p["ms"] / max(1, p["timed"])))
+        conv.Release()
         idx += 1
-    conv.Release()
     return results
 
 
 def tune(ctx, B: int, L: int, C: int, write: bool = True) -> dict:
+    """Chooses the tiling with the shortest block time (head + overlapped tail)."""
     res = measure(ctx, B, L, C)
     best = min(res, key=lambda r: r[2])
     P = max(1, -(-L // B))
     bytes_per_launch = C * ((P - 1) * B * 16 + B * 8)
-    entry = {"index": best[0], "tiling": list(best[1]), "tail_us": best[2],
-             "gbs": bytes_per_launch / (best[2] * 1e-6) / 1e9,
-             "all": [{"index": i, "tiling": list(t), "tail_us": us} for i, t, us in res]}
+    entry = {"index": best[0], "tiling": list(best[1]), "block_us": best[2], "tail_us": best[3],
+             "gbs": bytes_per_launch / (best[3] * 1e-6) / 1e9,
+             "all": [{"index": i, "tiling": list(t), "block_us": b, "tail_us": us} for i, t, b, us in res]}
     if write:
         d = load_cache()
         d[key(B, L, C)] = entry

@@ -174,10 +174,13 @@ def _block_latencies_batched(ctx, nsess, C, L, block, spectrum, blocks, g, pool)
 
 
 def _block_latencies_plain(ctx, nsess, C, L, block, blocks, g, pool):
+    from . import autotune
+
     convs = []
     for _ in range(nsess):
-        conv = cv.TANConvolution(ctx)
-        if conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, block, C) != cv.AMF_OK:
+        try:  # the drop-in with its autotuned tail tiling for this shape
+            conv = autotune.tuned(ctx, cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, block, C)
+        except cv.TANError:
             for c in convs:
                 c.Release()
             return None
