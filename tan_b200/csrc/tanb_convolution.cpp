@@ -5,14 +5,18 @@
 // Per Process call the host
 //   1. runs the channel-flag bookkeeping per block (ConvolutionImpl.cpp:2867-2907),
 //   2. writes one descriptor per block (per-channel run / swap / IR slots and
-//      the input and output row pointers) and the input samples into pinned
-//      staging, copied to the device in one transfer,
-//   3. enqueues head + tail kernels per block, the output copy before the last
-//      tail, and waits only for the output copy.
+//      the input and output row pointers): a kernel parameter for up to 128
+//      channels, else pinned staging copied to the device in one transfer,
+//   3. for host rows, copies the inputs into pinned staging that the head
+//      kernel reads in place and points the outputs at pinned staging that it
+//      writes in place (no separate host<->device copies),
+//   4. enqueues per block the head and, behind it, the tail (programmatic
+//      dependent launch, so the two overlap), and waits for the last of them.
 // UpdateResponseTD transforms the new IR into the idle slot and precomputes
 // that IR's tail, so the swap block costs the same device time as any other.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -21,6 +25,7 @@
 #include <vector>
 
 #include "../../include/tanb.h"
+#include "tanb_host_pool.h"
 #include "tanb_internal.h"
 
 using tanb::ChanCtl;
@@ -56,6 +61,10 @@ int32_t fail(int32_t code, const char* fmt, ...) {
   } while (0)
 
 constexpr int kMaxBlocksPerChunk = 8;
+// Host-row IR updates of at least this many bytes are staged on the host pool
+// in kStageGroups channel groups.
+constexpr size_t kParallelStageBytes = 1u << 20;
+constexpr int kStageGroups = 4;
 constexpr uint32_t kStopInput = TANB_CHANNEL_FLAG_STOP_INPUT;
 constexpr uint32_t kFlush = TANB_CHANNEL_FLAG_FLUSH_STREAM;
 
@@ -83,12 +92,12 @@ struct tanb_convolution {
   std::vector<uint8_t> available, flushed;
   int cur = 0;  // delay-line slot of the newest spectrum
 
-  // Process staging: [kMaxBlocksPerChunk] descriptors, then inputs
+  // Process staging: pinned [kMaxBlocksPerChunk] descriptors, then inputs;
+  // pinned outputs; the device copy of the descriptors (more than 128 channels)
   size_t desc_bytes = 0;
   uint8_t* h_stage = nullptr;
   uint8_t* d_stage = nullptr;
   float* h_out = nullptr;
-  float* d_out = nullptr;
   const ChanCtl* last_desc = nullptr;  // device descriptor of the last head (for ProcessFinalize)
   int last_cur = 0;
   // per-block descriptors passed as kernel parameters (C <= kParamChannels)
@@ -195,7 +204,6 @@ void free_all(tanb_convolution* v) {
   cudaFree(v->ds.tail);
   cudaFree(v->d_tw);
   cudaFree(v->d_stage);
-  cudaFree(v->d_out);
   cudaFree(v->d_ir);
   cudaFree(v->d_uctl);
   cudaFreeHost(v->h_stage);
@@ -220,7 +228,7 @@ void free_all(tanb_convolution* v) {
   v->ds = DevState{};
   v->d_tw = nullptr;
   v->d_stage = v->h_stage = nullptr;
-  v->d_out = v->h_out = nullptr;
+  v->h_out = nullptr;
   v->d_ir = v->h_ir = nullptr;
   v->d_uctl = v->h_uctl = nullptr;
   v->ev_stage = v->ev_ir = v->ev_out = nullptr;
@@ -310,12 +318,23 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   tanb::IrRows rows;
   rows.n = (long long)n;
   if (mem == Mem::Host) {
-    // compact staging (row stride n); the kernel reads zeros past n
-    for (int j = 0; j < nch; ++j)
-      if (n) std::memcpy(v->h_ir + (size_t)j * n, ir[chans[j]], n * sizeof(float));
-    if (n)
-      TANB_CUDA(cudaMemcpyAsync(v->d_ir, v->h_ir, (size_t)nch * n * sizeof(float), cudaMemcpyHostToDevice,
-                                v->stream));
+    // Compact staging (row stride n; the kernel reads zeros past n). Large
+    // updates copy rows on the host pool in channel groups and send each group
+    // as soon as it is staged, so its transfer overlaps the next group's copy.
+    const size_t row_bytes = n * sizeof(float);
+    const int groups = (row_bytes * nch >= kParallelStageBytes) ? std::min(nch, kStageGroups) : 1;
+    for (int q = 0; q < groups && n; ++q) {
+      const int j0 = (int)((long long)nch * q / groups), j1 = (int)((long long)nch * (q + 1) / groups);
+      if (groups > 1) {
+        tanb::host_parallel_for(j1 - j0, [&](int r) {
+          std::memcpy(v->h_ir + (size_t)(j0 + r) * n, ir[chans[j0 + r]], row_bytes);
+        });
+      } else {
+        for (int j = j0; j < j1; ++j) std::memcpy(v->h_ir + (size_t)j * n, ir[chans[j]], row_bytes);
+      }
+      TANB_CUDA(cudaMemcpyAsync(v->d_ir + (size_t)j0 * n, v->h_ir + (size_t)j0 * n, (size_t)(j1 - j0) * row_bytes,
+                                cudaMemcpyHostToDevice, v->stream));
+    }
     rows.base = v->d_ir;
     rows.stride = (long long)n;
   } else {
@@ -442,15 +461,18 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
           v->active[c] = v->slot_new[c];
           v->pending[c] = 0;
         }
-        // A null row reads as silence and its output is discarded.
+        // A null row reads as silence and its output is discarded. Host rows
+        // go through pinned staging that the head kernel reads and writes in
+        // place (mapped host memory under unified addressing): no separate
+        // host<->device copies per block.
         if (in_mem == Mem::Host) {
-          din[c] = in[c] ? v->stage_in(v->d_stage, b, c) : nullptr;
+          din[c] = in[c] ? v->stage_in(v->h_stage, b, c) : nullptr;
           if (run[c] && in[c]) std::memcpy(v->stage_in(v->h_stage, b, c), in[c] + blk * B, B * sizeof(float));
         } else {
           din[c] = in[c] ? in[c] + blk * B : nullptr;
         }
         if (out_mem == Mem::Host) {
-          dout[c] = v->d_out + ((size_t)b * C + c) * B;
+          dout[c] = v->h_out + ((size_t)b * C + c) * B;
         } else {
           dout[c] = out[c] ? out[c] + blk * B : nullptr;
         }
@@ -464,9 +486,6 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     if (nb == 0) break;
     if (!param)
       TANB_CUDA(cudaMemcpyAsync(v->d_stage, v->h_stage, nb * v->desc_bytes, cudaMemcpyHostToDevice, v->stream));
-    if (in_mem == Mem::Host)
-      TANB_CUDA(cudaMemcpyAsync(v->stage_in(v->d_stage, 0, 0), v->stage_in(v->h_stage, 0, 0),
-                                (size_t)nb * C * B * sizeof(float), cudaMemcpyHostToDevice, v->stream));
     TANB_CUDA(cudaEventRecord(v->ev_stage, v->stream));
     for (int b = 0; b < nb; ++b) {
       for (int c : flush_b[b]) TANB_CUDA(flush_channel(v, c));
@@ -498,10 +517,8 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       }
     }
     // Outputs are final after the heads; in the default mode the last tail,
-    // which overlaps its head, completes before the copy as well.
-    if (out_mem == Mem::Host)
-      TANB_CUDA(cudaMemcpyAsync(v->h_out, v->d_out, (size_t)nb * C * B * sizeof(float), cudaMemcpyDeviceToHost,
-                                v->stream));
+    // which overlaps its head, completes before this event as well. The
+    // staged inputs and outputs are free again once it has completed.
     TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
     if (out_mem == Mem::Host) {
       TANB_CUDA(cudaEventSynchronize(v->ev_out));
@@ -813,8 +830,7 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
     if ((e = dev_alloc(v, &v->ds.prev, Cs * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->ds.tail, Cs * 2 * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_tw, 2 * Bs)) != cudaSuccess) break;
-    if ((e = dev_alloc(v, &v->d_stage, stage_bytes)) != cudaSuccess) break;
-    if ((e = dev_alloc(v, &v->d_out, out_floats)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_stage, kMaxBlocksPerChunk * v->desc_bytes)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_ir, Cs * Ps * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_uctl, uctl_bytes(C))) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_stage, stage_bytes)) != cudaSuccess) break;

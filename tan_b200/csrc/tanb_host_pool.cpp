@@ -1,0 +1,105 @@
+// Host worker pool (tanb_host_pool.h). A job is an index range handed out one
+// index at a time through an atomic counter; workers sleep on a condition
+// variable between jobs. Jobs are serialised by a mutex, so concurrent API
+// calls from several threads take turns. In a process forked after the pool
+// started, jobs run serially on the caller.
+#include "tanb_host_pool.h"
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include <unistd.h>
+
+namespace tanb {
+namespace {
+
+class Pool {
+ public:
+  explicit Pool(int nthreads) : pid_(getpid()) {
+    for (int t = 0; t < nthreads; ++t) workers_.emplace_back([this] { loop(); });
+  }
+
+  // A process forked after the pool started has none of its threads.
+  bool usable() const { return getpid() == pid_; }
+
+  int threads() const { return (int)workers_.size(); }
+
+  void run(int n, const std::function<void(int)>& fn) {
+    std::lock_guard<std::mutex> job_lock(job_mu_);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fn_ = &fn;
+      n_ = n;
+      next_.store(0);
+      busy_ = (int)workers_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [this] { return busy_ == 0; });
+    fn_ = nullptr;
+  }
+
+ private:
+  void work() {
+    for (int i = next_.fetch_add(1); i < n_; i = next_.fetch_add(1)) (*fn_)(i);
+  }
+
+  void loop() {
+    unsigned long long seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+      }
+      work();
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        --busy_;
+      }
+      done_cv_.notify_one();
+    }
+  }
+
+  const pid_t pid_;
+  std::vector<std::thread> workers_;
+  std::mutex job_mu_;  // one job at a time
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(int)>* fn_ = nullptr;
+  int n_ = 0;
+  std::atomic<int> next_{0};
+  int busy_ = 0;
+  unsigned long long gen_ = 0;
+};
+
+Pool& pool() {
+  // half of the host's hardware threads, at most 8: enough to saturate the
+  // memory bandwidth of a copy without taking the whole host
+  // Never destroyed: its idle workers end with the process (a destructor
+  // would have to join them, also in a forked child that does not have them).
+  static Pool* p = new Pool(std::max(1, std::min(8, (int)std::thread::hardware_concurrency() / 2) - 1));
+  return *p;
+}
+
+}  // namespace
+
+void host_parallel_for(int n, const std::function<void(int)>& fn) {
+  if (n <= 0) return;
+  Pool& p = pool();
+  if (n == 1 || !p.usable()) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  p.run(n, fn);
+}
+
+int host_pool_threads() { return pool().threads(); }
+
+}  // namespace tanb

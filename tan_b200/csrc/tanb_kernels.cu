@@ -15,6 +15,7 @@
 // overlap-save needs no overlap buffer and gives the exact new-IR output on a
 // swap block from the same delay line.
 #include <cmath>
+#include <cstdint>
 #include <utility>
 
 #include "tanb_fft.cuh"
@@ -148,10 +149,20 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
       ph[q][1] = h0[km];
     }
   }
-  // frame [x_{k-1}, x_k] packed as complex pairs
+  // frame [x_{k-1}, x_k] packed as complex pairs; 8-byte loads where the
+  // caller's row allows (rows in pinned host staging are read over the bus)
+  const bool x_vec = x && (reinterpret_cast<uintptr_t>(x) & 7) == 0;
   for (int n = threadIdx.x; n < M; n += T) {
-    const float* src = (n < M / 2) ? prev + 2 * n : (x ? x + 2 * (n - M / 2) : nullptr);
-    z[n] = src ? make_float2(src[0], src[1]) : make_float2(0.f, 0.f);
+    if (n < M / 2) {
+      z[n] = reinterpret_cast<const float2*>(prev)[n];
+    } else if (!x) {
+      z[n] = make_float2(0.f, 0.f);
+    } else if (x_vec) {
+      z[n] = reinterpret_cast<const float2*>(x)[n - M / 2];
+    } else {
+      const float* src = x + 2 * (n - M / 2);
+      z[n] = make_float2(src[0], src[1]);
+    }
   }
   __syncthreads();
   for (int n = threadIdx.x; n < M / 2; n += T) reinterpret_cast<float2*>(prev)[n] = z[n + M / 2];
@@ -196,18 +207,21 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   // overlap-save: samples [B, 2B) of the circular result are the output
   if (!y) return;
   const float step = 1.0f / (float)M;
+  const bool y_vec = (reinterpret_cast<uintptr_t>(y) & 7) == 0;
   for (int m = M / 2 + threadIdx.x; m < M; m += T) {
     const int i = 2 * (m - M / 2);
-    const float2 yo = z[m];
-    if (!swap) {
-      y[i] = yo.x;
-      y[i + 1] = yo.y;
-    } else {
+    float2 o = z[m];
+    if (swap) {
       const float2 yn = z2[m];
       const float a0 = step * (float)i, b0 = step * (float)(M - i);
       const float a1 = step * (float)(i + 1), b1 = step * (float)(M - i - 1);
-      y[i] = yn.x * a0 + yo.x * b0;
-      y[i + 1] = yn.y * a1 + yo.y * b1;
+      o = make_float2(yn.x * a0 + o.x * b0, yn.y * a1 + o.y * b1);
+    }
+    if (y_vec) {
+      reinterpret_cast<float2*>(y)[i / 2] = o;
+    } else {
+      y[i] = o.x;
+      y[i + 1] = o.y;
     }
   }
 }
