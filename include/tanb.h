@@ -225,9 +225,10 @@ int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6],
 /* ---------------------------------------------------------------------------
  * Batched engine. No single reference counterpart: it is the serving form of
  * the same path -- many TANConvolution-equivalent sessions (C channels, IR
- * length L each) processed together, one head and one tail launch per block
- * for all of them, the role the reference's GPU engine plays with its channel
- * maps (tan/tanlibrary/src/Graal/GraalConv.cpp:644-704, 1883-2145).
+ * length L each) processed together in ONE kernel launch per audio block (heads
+ * of every channel side by side with the partition multiply-accumulate work
+ * items for the next block), the role the reference's GPU engine plays with
+ * its channel maps (tan/tanlibrary/src/Graal/GraalConv.cpp:644-704, 1883-2145).
  * ------------------------------------------------------------------------- */
 typedef struct tanb_engine tanb_engine;
 
@@ -265,11 +266,20 @@ int32_t tanb_engine_update_response_td_device(tanb_engine* engine, int32_t sessi
                                               size_t n, uint32_t operationFlags);
 
 /* Pinned host I/O buffers [max_channels][block]: write slot s's input block at
- * in[s * block], read its output at out[s * block] after tanb_engine_process. */
+ * in[s * block], read its output at out[s * block] after tanb_engine_process.
+ * The block launch reads and writes them in place (mapped host memory). */
 int32_t tanb_engine_io(tanb_engine* engine, float** in, float** out);
 
-/* One block for every open session through the host buffers; returns when the
- * output is in the pinned output buffer (the tail for the next block runs on). */
+/* Copies `count` input rows of `block` samples, row j from src + j * ld, into
+ * the pinned input buffer at slots [first_slot, first_slot + count), spread
+ * over host threads for large copies. Call between tanb_engine_process calls
+ * (the block launch reads the buffer in place). */
+int32_t tanb_engine_write_input(tanb_engine* engine, uint32_t first_slot, const float* src, uint32_t count,
+                                size_t ld);
+
+/* One block for every open session through the host buffers (one CUDA graph
+ * holding the block launch); returns when the output is in the pinned output
+ * buffer. */
 int32_t tanb_engine_process(tanb_engine* engine);
 
 /* One block with device-resident I/O: slot s reads in[s * ld] (null: silence)
@@ -281,7 +291,8 @@ void* tanb_engine_stream(tanb_engine* engine);
 
 /* out[0] sessions, out[1] channels, out[2] slot high-water mark, out[3] work
  * items high-water mark, out[4] arena bytes in use, out[5] budget, out[6]
- * algorithmic tail bytes per block, out[7] tail grid size. */
+ * algorithmic bytes of one block launch (heads and work items), out[7] tail
+ * CTAs of the block launch at most. */
 int32_t tanb_engine_info(tanb_engine* engine, int64_t out[8]);
 
 /* out[0] blocks the session has processed, out[1] its block index at which the
@@ -289,9 +300,10 @@ int32_t tanb_engine_info(tanb_engine* engine, int64_t out[8]);
  * uploaded but not yet in effect. */
 int32_t tanb_engine_session_state(tanb_engine* engine, int32_t session, int64_t out[3]);
 
-/* Device-time accounting of tanb_engine_process_device: counts[0] heads,
- * counts[1] tails, counts[2] IR updates, counts[3] timed blocks; ms[0] head,
- * ms[1] tail device milliseconds. Reading resets. */
+/* Accounting: counts[0] block launches, counts[1] commit launches (partial
+ * sums of a newly committed IR), counts[2] IR updates, counts[3] blocks timed;
+ * ms[0] device milliseconds of the timed block launches (tanb_engine_process_device
+ * with profiling enabled), ms[1] 0. Reading resets. */
 int32_t tanb_engine_profile(tanb_engine* engine, int32_t enable);
 int32_t tanb_engine_profile_read(tanb_engine* engine, int64_t counts[4], double ms[2]);
 

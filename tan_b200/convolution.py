@@ -96,6 +96,7 @@ SIGNATURES = {
     "tanb_engine_update_response_td_device": (_i32, [_vp, _i32, _pp, _sz, _u32]),
     "tanb_engine_io": (_i32, [_vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
                               ctypes.POINTER(ctypes.POINTER(ctypes.c_float))]),
+    "tanb_engine_write_input": (_i32, [_vp, _u32, _vp, _u32, _sz]),
     "tanb_engine_process": (_i32, [_vp]),
     "tanb_engine_process_device": (_i32, [_vp, _vp, _vp, _u32]),
     "tanb_engine_synchronize": (_i32, [_vp]),

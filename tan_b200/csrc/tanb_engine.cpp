@@ -6,10 +6,11 @@
 // device-memory arena sized by the caller's budget; opening a session that does
 // not fit is refused with AMF_OUT_OF_MEMORY (admission by memory budget).
 //
-// Per audio block one CUDA graph runs: input copy (pinned -> device), the head
-// kernel over every channel slot, output copy, then the persistent tail kernel
-// over every work item for the next block. The graph is re-instantiated only
-// when the high-water marks of channel slots or work items change.
+// Per audio block one CUDA graph runs a single kernel launch: the heads of every
+// channel slot (reading the pinned input buffer and writing the pinned output
+// buffer in place) side by side with persistent CTAs over the tail work items,
+// which compute the next block's partial sums. The graph is re-instantiated
+// only when the high-water marks of channel slots or work items change.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +24,7 @@
 
 #include "../../include/tanb.h"
 #include "tanb_engine.h"
+#include "tanb_host_pool.h"
 #include "tanb_internal.h"
 
 using tanb::EngChan;
@@ -130,10 +132,10 @@ struct tanb_engine {
   EngChan* h_chans = nullptr;
   EngItem* d_items = nullptr;
   EngItem* h_items = nullptr;
-  float* h_in = nullptr;
-  float* h_out = nullptr;
-  float* d_in = nullptr;
-  float* d_out = nullptr;
+  float* h_in = nullptr;   // pinned; read in place by the heads
+  float* h_out = nullptr;  // pinned; written in place by the heads
+  long long* d_block = nullptr;     // blocks processed (device)
+  unsigned int* d_done = nullptr;   // CTAs finished in the running launch
   float* h_ir = nullptr;
   float* d_ir = nullptr;
   size_t ir_cap = 0;
@@ -146,13 +148,14 @@ struct tanb_engine {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaEvent_t ev_out = nullptr;
+  cudaEvent_t ev_audio = nullptr;  // audio-stream point an IR upload waits for
   std::map<int, Session> sessions;
   int next_id = 1;
   // accounting
   bool profiling = false;
-  cudaEvent_t pa = nullptr, pb = nullptr, pc = nullptr;
-  double ms_head = 0, ms_tail = 0;
-  int64_t n_head = 0, n_tail = 0, n_ir = 0, n_timed = 0;
+  cudaEvent_t pa = nullptr, pb = nullptr;
+  double ms_block = 0;
+  int64_t n_block = 0, n_commit = 0, n_ir = 0, n_timed = 0;
 };
 
 namespace {
@@ -165,7 +168,7 @@ size_t session_bytes(const tanb_engine* e, int C, int P, int nitem) {
   if (e->spec != tanb::kSpecFP32) per += align_up(2 * (size_t)P * 4);     // scales
   per += align_up((size_t)P * B * 8);                                    // fdl
   per += align_up(B * 4);                                                // prev
-  per += align_up(2 * (size_t)nitem * B * 8);                            // partials
+  per += align_up(4 * (size_t)nitem * B * 8);                            // partials
   return per * C;
 }
 
@@ -187,8 +190,7 @@ void free_engine(tanb_engine* e) {
   cudaFree(e->arena);
   cudaFree(e->d_chans);
   cudaFree(e->d_items);
-  cudaFree(e->d_in);
-  cudaFree(e->d_out);
+  cudaFree(e->d_block);
   cudaFree(e->d_ir);
   cudaFree(e->d_upd);
   cudaFree(e->d_tw);
@@ -199,9 +201,9 @@ void free_engine(tanb_engine* e) {
   cudaFreeHost(e->h_ir);
   cudaFreeHost(e->h_upd);
   if (e->ev_out) cudaEventDestroy(e->ev_out);
+  if (e->ev_audio) cudaEventDestroy(e->ev_audio);
   if (e->pa) cudaEventDestroy(e->pa);
   if (e->pb) cudaEventDestroy(e->pb);
-  if (e->pc) cudaEventDestroy(e->pc);
   if (e->upd_stream) cudaStreamDestroy(e->upd_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
 }
@@ -225,9 +227,10 @@ void update_hwm(tanb_engine* e) {
 }
 
 // Commits every staged IR update whose transform has finished: the channels'
-// pending flags go to the device table and the new IR's tail for the coming
-// block is computed from the current delay line, both on the audio stream
-// before this block's head (which then crossfades to the new IR). Caller holds mu.
+// pending flags go to the device table and the new IR's partial sums for the
+// coming block are computed from the current delay line, both on the audio
+// stream before this block's launch (whose heads then crossfade to the new IR).
+// Caller holds mu.
 cudaError_t commit_updates(tanb_engine* e) {
   for (auto& kv : e->sessions) {
     Session& s = kv.second;
@@ -238,37 +241,28 @@ cudaError_t commit_updates(tanb_engine* e) {
     s.staged = false;
     s.last_swap_block = s.blocks;  // the head of this block crossfades to the new IR
     for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j].pending = 1;
-    cudaError_t r = upload_chans(e, s.slot0, s.C);
+    // not a copy of the mirror: process_device returns before the device has
+    // run this, and the mirror advances right away
+    cudaError_t r = tanb::eng_launch_mark_pending(e->d_chans, (int)s.slot0, s.C, e->stream);
     if (r != cudaSuccess) return r;
     if (s.nitem) {
-      r = tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, s.C * s.nitem, 1,
-                                std::min(e->tail_grid, s.C * s.nitem), e->stream);
+      r = tanb::eng_launch_commit(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, s.C * s.nitem,
+                                  std::min(e->tail_grid, s.C * s.nitem), e->d_block, e->stream);
       if (r != cudaSuccess) return r;
+      e->n_commit += 1;
     }
   }
   return cudaSuccess;
 }
 
-// Enqueues one block: head over all slots, output copy (host mode), tail.
-cudaError_t enqueue_block(tanb_engine* e, const float* in, float* out, size_t ld, bool host) {
-  cudaError_t r;
-  if (host && e->nslots_hwm) {
-    r = cudaMemcpyAsync(e->d_in, e->h_in, e->nslots_hwm * e->B * sizeof(float), cudaMemcpyHostToDevice, e->stream);
-    if (r != cudaSuccess) return r;
-  }
-  r = tanb::eng_launch_head(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, in, out, (int)ld, e->d_tw,
-                            e->stream);
-  if (r != cudaSuccess) return r;
-  if (host && e->nslots_hwm) {
-    r = cudaMemcpyAsync(e->h_out, e->d_out, e->nslots_hwm * e->B * sizeof(float), cudaMemcpyDeviceToHost,
-                        e->stream);
-    if (r != cudaSuccess) return r;
-  }
-  // inside stream capture a plain record only marks a capture dependency; the
-  // external flag makes it an event-record node that fires on every launch
-  if ((r = cudaEventRecordWithFlags(e->ev_out, e->stream, cudaEventRecordExternal)) != cudaSuccess) return r;
-  return tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, 0, (int)e->nitems_hwm, 0, e->tail_grid,
-                               e->stream);
+int tail_ctas(const tanb_engine* e) { return (int)std::min<size_t>(e->tail_grid, e->nitems_hwm); }
+
+// Enqueues one block: the single launch over all slots and work items (in and
+// out: device rows or the pinned host buffers).
+cudaError_t enqueue_block(tanb_engine* e, const float* in, float* out, size_t ld) {
+  return tanb::eng_launch_block(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, e->d_items, (int)e->nitems_hwm,
+                                tail_ctas(e), in, out, (int)ld, e->d_tw, tanb::EngSync{e->d_block, e->d_done},
+                                e->stream);
 }
 
 cudaError_t ensure_graph(tanb_engine* e) {
@@ -276,7 +270,10 @@ cudaError_t ensure_graph(tanb_engine* e) {
   destroy_graph(e);
   cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
   if (r != cudaSuccess) return r;
-  cudaError_t r2 = enqueue_block(e, e->d_in, e->d_out, e->B, true);
+  cudaError_t r2 = enqueue_block(e, e->h_in, e->h_out, e->B);
+  // inside stream capture a plain record only marks a capture dependency; the
+  // external flag makes it an event-record node that fires on every launch
+  if (r2 == cudaSuccess) r2 = cudaEventRecordWithFlags(e->ev_out, e->stream, cudaEventRecordExternal);
   r = cudaStreamEndCapture(e->stream, &e->graph);
   if (r2 != cudaSuccess) return r2;
   if (r != cudaSuccess) return r;
@@ -333,8 +330,7 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   if (r == cudaSuccess) r = cudaMalloc(&e->arena, std::max<size_t>(budget_bytes, kAlign));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_chans, e->max_channels * sizeof(EngChan));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_items, e->max_items * sizeof(EngItem));
-  if (r == cudaSuccess) r = cudaMalloc(&e->d_in, io * sizeof(float));
-  if (r == cudaSuccess) r = cudaMalloc(&e->d_out, io * sizeof(float));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_block, 2 * sizeof(long long));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_upd, e->max_channels * sizeof(EngUpd));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_tw, 2 * e->B * sizeof(float2));
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_chans, e->max_channels * sizeof(EngChan));
@@ -343,9 +339,9 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_out, io * sizeof(float));
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_upd, e->max_channels * sizeof(EngUpd));
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_audio, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreate(&e->pa);
   if (r == cudaSuccess) r = cudaEventCreate(&e->pb);
-  if (r == cudaSuccess) r = cudaEventCreate(&e->pc);
   if (r != cudaSuccess) {
     free_engine(e);
     delete e;
@@ -356,6 +352,7 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   std::memset(e->h_chans, 0, e->max_channels * sizeof(EngChan));
   for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0};
   std::memset(e->h_in, 0, io * sizeof(float));
+  std::memset(e->h_out, 0, io * sizeof(float));
   e->arena_alloc.reset(budget_bytes / kAlign);
   e->slot_alloc.reset(e->max_channels);
   e->item_alloc.reset(e->max_items);
@@ -364,11 +361,14 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   r = cudaMemcpyAsync(e->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, e->stream);
   if (r == cudaSuccess) r = cudaMemsetAsync(e->d_chans, 0, e->max_channels * sizeof(EngChan), e->stream);
   if (r == cudaSuccess) r = upload_items(e, 0, e->max_items);
-  if (r == cudaSuccess) r = cudaMemsetAsync(e->d_in, 0, io * sizeof(float), e->stream);
+  if (e->d_block) e->d_done = reinterpret_cast<unsigned int*>(e->d_block + 1);
+  if (r == cudaSuccess) r = cudaMemsetAsync(e->d_block, 0, 2 * sizeof(long long), e->stream);
   if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
-  int sms = 148, per_sm = 1;
+  // tail CTAs of the block launch: as many as fit on the GPU at once (B / 4
+  // threads each at up to 64 registers: 1024 threads per SM)
+  int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  per_sm = std::max(1, 2048 / (e->B / 2));
+  const int per_sm = std::max(1, std::min(32, 1024 / (e->B / 4)));
   e->tail_grid = sms * per_sm;
   if (r != cudaSuccess) {
     free_engine(e);
@@ -400,7 +400,8 @@ int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_
   s.C = (int)channels;
   s.L = (int)ir_length;
   s.P = (int)std::max<uint32_t>(1, (ir_length + e->B - 1) / e->B);
-  s.nitem = s.P > 1 ? (s.P - 1 + e->Q - 1) / e->Q : 0;
+  // work items cover partitions [2, P); the head does partitions 0 and 1
+  s.nitem = s.P > 2 ? (s.P - 2 + e->Q - 1) / e->Q : 0;
   s.arena_bytes = session_bytes(e, s.C, s.P, s.nitem);
   if (!e->arena_alloc.alloc(s.arena_bytes / kAlign, &s.arena_off))
     return efail(TANB_OUT_OF_MEMORY, "session of %u channels x %u taps needs %zu bytes; device budget exhausted",
@@ -432,7 +433,7 @@ int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_
     ch.prev = reinterpret_cast<float*>(base);
     base += align_up(B * 4);
     ch.part = reinterpret_cast<float2*>(base);
-    base += align_up(2 * (size_t)s.nitem * B * 8);
+    base += align_up(4 * (size_t)s.nitem * B * 8);
     ch.P = s.P;
     ch.nitem = s.nitem;
     ch.cur = 0;
@@ -441,12 +442,14 @@ int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_
     ch.run = 1;
     e->h_chans[s.slot0 + j] = ch;
     for (int r = 0; r < s.nitem; ++r) {
-      const int i0 = 1 + r * e->Q;
+      const int i0 = 2 + r * e->Q;
       e->h_items[s.item0 + (size_t)j * s.nitem + r] = EngItem{(int)(s.slot0 + j), i0, std::min(s.P, i0 + e->Q), r};
     }
   }
   ENG_CUDA(upload_chans(e, s.slot0, s.C));
   ENG_CUDA(upload_items(e, s.item0, nit_total));
+  // the copies read the pinned mirrors, which the next block advances
+  ENG_CUDA(cudaStreamSynchronize(e->stream));
   ENG_CUDA(cudaEventCreateWithFlags(&s.staged_ev, cudaEventDisableTiming));
   s.id = e->next_id++;
   e->sessions[s.id] = s;
@@ -472,6 +475,7 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0};
   ENG_CUDA(upload_chans(e, s.slot0, s.C));
   ENG_CUDA(upload_items(e, s.item0, nit_total));
+  ENG_CUDA(cudaStreamSynchronize(e->stream));  // the copies read the pinned mirrors
   e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
   e->slot_alloc.release(s.slot0, s.C);
   e->item_alloc.release(s.item0, nit_total);
@@ -485,6 +489,9 @@ static int32_t engine_update(tanb_engine* e, int32_t session, const float* const
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   if (!ir) return efail(TANB_INVALID_ARG, "ppBuffer == NULL");
   std::lock_guard<std::mutex> ulock(e->upd_mu);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  // the previous upload's copies read the pinned staging rewritten below
+  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
   Session s;
   {
     // read the session and choose the idle IR slots under the main lock: the
@@ -496,13 +503,15 @@ static int32_t engine_update(tanb_engine* e, int32_t session, const float* const
     if (n > (size_t)s.L) return efail(TANB_INVALID_ARG, "IR length %zu exceeds the session's %d", n, s.L);
     for (int j = 0; j < s.C; ++j) {
       if (!ir[j] && n) return efail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", j);
-      e->h_upd[j] = EngUpd{(int)(s.slot0 + j), 1 - e->h_chans[s.slot0 + j].active, (int64_t)s.P * e->B};
+      e->h_upd[j] = EngUpd{(int)(s.slot0 + j), 1 - e->h_chans[s.slot0 + j].active, nullptr, (int64_t)n};
     }
     it->second.staged = false;  // a newer upload supersedes one not yet committed
+    // The mirror (and so the idle-slot choice) already reflects every block
+    // enqueued on the audio stream; blocks still running there may read the
+    // chosen slot (a crossfade from it), so the transform waits for them.
+    ENG_CUDA(cudaEventRecord(e->ev_audio, e->stream));
+    ENG_CUDA(cudaStreamWaitEvent(e->upd_stream, e->ev_audio, 0));
   }
-  ENG_CUDA(cudaSetDevice(e->ctx->device));
-  // IR staging of the previous upload must have been consumed
-  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
   const size_t PB = (size_t)s.P * e->B;
   const size_t need = PB * s.C;
   if (need > e->ir_cap) {
@@ -515,22 +524,22 @@ static int32_t engine_update(tanb_engine* e, int32_t session, const float* const
     ENG_CUDA(cudaMallocHost(&e->h_ir, need * sizeof(float)));
     e->ir_cap = need;
   }
-  for (int j = 0; j < s.C; ++j) {
-    if (device) {
-      float* row = e->d_ir + (size_t)j * PB;
-      if (n) ENG_CUDA(cudaMemcpyAsync(row, ir[j], n * sizeof(float), cudaMemcpyDeviceToDevice, e->upd_stream));
-      ENG_CUDA(cudaMemsetAsync(row + n, 0, (PB - n) * sizeof(float), e->upd_stream));
-    } else {
-      float* row = e->h_ir + (size_t)j * PB;
-      if (n) std::memcpy(row, ir[j], n * sizeof(float));
-      std::memset(row + n, 0, (PB - n) * sizeof(float));
-    }
+  if (device) {
+    // the transform reads the caller's rows in place
+    for (int j = 0; j < s.C; ++j) e->h_upd[j].src = ir[j];
+  } else if (n) {
+    // compact staging (row stride n) copied on the host pool, one transfer
+    auto copy_row = [&](int j) { std::memcpy(e->h_ir + (size_t)j * n, ir[j], n * sizeof(float)); };
+    if ((size_t)s.C * n * sizeof(float) >= (1u << 20))
+      tanb::host_parallel_for(s.C, copy_row);
+    else
+      for (int j = 0; j < s.C; ++j) copy_row(j);
+    ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, (size_t)s.C * n * sizeof(float), cudaMemcpyHostToDevice,
+                             e->upd_stream));
+    for (int j = 0; j < s.C; ++j) e->h_upd[j].src = e->d_ir + (size_t)j * n;
   }
-  if (!device)
-    ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, need * sizeof(float), cudaMemcpyHostToDevice, e->upd_stream));
   ENG_CUDA(cudaMemcpyAsync(e->d_upd, e->h_upd, s.C * sizeof(EngUpd), cudaMemcpyHostToDevice, e->upd_stream));
-  ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_ir, e->d_upd, s.C, s.P, e->d_tw,
-                               e->upd_stream));
+  ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_upd, s.C, s.P, e->d_tw, e->upd_stream));
   ENG_CUDA(cudaEventRecord(s.staged_ev, e->upd_stream));
   // BLOCK_UNTIL_READY: the new IR is ready for the next block when this returns
   if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) ENG_CUDA(cudaEventSynchronize(s.staged_ev));
@@ -560,6 +569,25 @@ int32_t tanb_engine_io(tanb_engine* e, float** in, float** out) {
   return TANB_OK;
 }
 
+int32_t tanb_engine_write_input(tanb_engine* e, uint32_t first_slot, const float* src, uint32_t count, size_t ld) {
+  if (!e || (!src && count)) return efail(TANB_INVALID_POINTER, "null argument");
+  if ((size_t)first_slot + count > e->max_channels) return efail(TANB_INVALID_ARG, "slots out of range");
+  if (count && ld < (size_t)e->B) return efail(TANB_INVALID_ARG, "ld %zu < block %d", ld, e->B);
+  const size_t B = e->B;
+  constexpr uint32_t kRowsPerTask = 64;
+  const uint32_t tasks = (count + kRowsPerTask - 1) / kRowsPerTask;
+  auto copy = [&](int t) {
+    const uint32_t r0 = (uint32_t)t * kRowsPerTask, r1 = std::min(count, r0 + kRowsPerTask);
+    for (uint32_t r = r0; r < r1; ++r)
+      std::memcpy(e->h_in + (size_t)(first_slot + r) * B, src + (size_t)r * ld, B * sizeof(float));
+  };
+  if ((size_t)count * B * sizeof(float) >= (1u << 20))
+    tanb::host_parallel_for((int)tasks, copy);
+  else
+    for (uint32_t t = 0; t < tasks; ++t) copy((int)t);
+  return TANB_OK;
+}
+
 int32_t tanb_engine_process(tanb_engine* e) {
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   std::lock_guard<std::mutex> lock(e->mu);
@@ -569,8 +597,7 @@ int32_t tanb_engine_process(tanb_engine* e) {
   ENG_CUDA(ensure_graph(e));
   ENG_CUDA(cudaGraphLaunch(e->graph_exec, e->stream));
   ENG_CUDA(cudaEventSynchronize(e->ev_out));
-  e->n_head += 1;
-  e->n_tail += e->nitems_hwm ? 1 : 0;
+  e->n_block += 1;
   advance_mirror(e);
   return TANB_OK;
 }
@@ -584,23 +611,16 @@ int32_t tanb_engine_process_device(tanb_engine* e, const float* in, float* out, 
   if (ld == 0) ld = e->B;
   ENG_CUDA(commit_updates(e));
   if (e->profiling) ENG_CUDA(cudaEventRecord(e->pa, e->stream));
-  ENG_CUDA(tanb::eng_launch_head(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, in, out, (int)ld, e->d_tw,
-                                 e->stream));
-  if (e->profiling) ENG_CUDA(cudaEventRecord(e->pb, e->stream));
-  ENG_CUDA(tanb::eng_launch_tail(e->log2B, e->spec, e->d_chans, e->d_items, 0, (int)e->nitems_hwm, 0,
-                                 e->tail_grid, e->stream));
+  ENG_CUDA(enqueue_block(e, in, out, ld));
   if (e->profiling) {
-    ENG_CUDA(cudaEventRecord(e->pc, e->stream));
-    ENG_CUDA(cudaEventSynchronize(e->pc));
-    float a = 0, b = 0;
+    ENG_CUDA(cudaEventRecord(e->pb, e->stream));
+    ENG_CUDA(cudaEventSynchronize(e->pb));
+    float a = 0;
     cudaEventElapsedTime(&a, e->pa, e->pb);
-    cudaEventElapsedTime(&b, e->pb, e->pc);
-    e->ms_head += a;
-    e->ms_tail += b;
+    e->ms_block += a;
     e->n_timed += 1;
   }
-  e->n_head += 1;
-  e->n_tail += e->nitems_hwm ? 1 : 0;
+  e->n_block += 1;
   advance_mirror(e);
   return TANB_OK;
 }
@@ -619,14 +639,19 @@ void* tanb_engine_stream(tanb_engine* e) { return e ? (void*)e->stream : nullptr
 int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
   if (!e || !out) return efail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(e->mu);
-  int64_t chans = 0, bytes = 0, tail_bytes = 0;
+  int64_t chans = 0, bytes = 0, block_bytes = 0;
+  const int64_t B = e->B, sb = (int64_t)spec_bytes(e->spec);
   for (auto& kv : e->sessions) {
     const Session& s = kv.second;
     chans += s.C;
     bytes += (int64_t)s.arena_bytes;
-    // per block: (P-1) partitions x B bins of IR spectrum + delay line, plus partial rows
-    tail_bytes += (int64_t)s.C * ((int64_t)(s.P - 1) * e->B * (int64_t)(spec_bytes(e->spec) + 8) +
-                                  (int64_t)s.nitem * e->B * 8);
+    // algorithmic bytes of one block launch per channel: tail items stream
+    // partitions [2, P) of IR spectrum and delay line and write their partial
+    // rows; the head reads input, history, the partial rows, partitions 0 and
+    // 1 of the spectrum and X_{k-1}, and writes output, history and X_k
+    const int64_t tail = (s.P > 2 ? (int64_t)(s.P - 2) * B * (sb + 8) : 0) + (int64_t)s.nitem * B * 8;
+    const int64_t head = 4 * B * 4 + (int64_t)s.nitem * B * 8 + (s.P > 1 ? 2 * B * sb + B * 8 : B * sb) + B * 8;
+    block_bytes += (int64_t)s.C * (tail + head);
   }
   out[0] = (int64_t)e->sessions.size();
   out[1] = chans;
@@ -634,7 +659,7 @@ int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
   out[3] = (int64_t)e->nitems_hwm;
   out[4] = bytes;
   out[5] = (int64_t)e->budget;
-  out[6] = tail_bytes;
+  out[6] = block_bytes;
   out[7] = e->tail_grid;
   return TANB_OK;
 }
@@ -660,14 +685,14 @@ int32_t tanb_engine_profile(tanb_engine* e, int32_t enable) {
 int32_t tanb_engine_profile_read(tanb_engine* e, int64_t counts[4], double ms[2]) {
   if (!e || !counts || !ms) return efail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(e->mu);
-  counts[0] = e->n_head;
-  counts[1] = e->n_tail;
+  counts[0] = e->n_block;
+  counts[1] = e->n_commit;
   counts[2] = e->n_ir;
   counts[3] = e->n_timed;
-  ms[0] = e->ms_head;
-  ms[1] = e->ms_tail;
-  e->n_head = e->n_tail = e->n_ir = e->n_timed = 0;
-  e->ms_head = e->ms_tail = 0;
+  ms[0] = e->ms_block;
+  ms[1] = 0.0;
+  e->n_block = e->n_commit = e->n_ir = e->n_timed = 0;
+  e->ms_block = 0;
   return TANB_OK;
 }
 

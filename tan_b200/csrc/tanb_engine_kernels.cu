@@ -1,19 +1,24 @@
 // Kernels of the batched engine: every channel of every open session runs in
-// one head launch and one persistent tail launch per audio block.
+// ONE launch per audio block.
 //
-//   eng_ir_kernel    one CTA per (IR partition, updated channel): R2C of the
-//                    partition, optional FP16/BF16 quantisation with a
-//                    power-of-two per-partition scale, stored in the idle slot
-//                    (runs on the engine's update stream)
-//   eng_head_kernel  one CTA per channel slot: as the single-object head, but
-//                    the tail comes from the channel's work-item partial sums
-//                    (added in a fixed order) and the delay-line position and
-//                    IR slot state live in the device channel table
-//   eng_tail_kernel  persistent grid over work items (channel, partition range):
-//                    each item streams its partitions of IR spectrum and delay
-//                    line once (float4 / uint2 loads) and writes one partial
-//                    sum row -- items are of bounded size, so channels with
-//                    uneven partition counts balance across the 148 SMs
+//   eng_ir_kernel      one CTA per (IR partition, updated channel): R2C of the
+//                      partition, optional FP16/BF16 quantisation with a
+//                      power-of-two per-partition scale, stored in the idle slot
+//                      (runs on the engine's update stream)
+//   eng_block_kernel   per block: CTAs [0, nslots) are the heads of the channel
+//                      slots (as the single-object head, with the tail from the
+//                      channel's partial-sum rows plus the partition-1 product
+//                      computed here); the remaining CTAs are a persistent grid
+//                      over work items (channel, partition range within
+//                      [2, P)) writing the partial sums of the NEXT block. Those
+//                      read only delay-line slots X_{k-1} and older, which no
+//                      head writes, and write the other parity's rows, which no
+//                      head reads, so heads and tail items run side by side in
+//                      one grid with no dependency between them. Channel state
+//                      (delay-line position, IR slots) is read by every CTA as
+//                      it was at launch; the last CTA to finish advances it.
+//   eng_commit_kernel  partial sums of a newly committed IR for the coming block
+//                      (before that block's launch), from the current delay line
 //
 // The per-block sums are the reference's head and tail
 // (tan/tanlibrary/src/TrueAudioNext/convolution/ConvolutionImpl.cpp:2380-2643);
@@ -21,6 +26,8 @@
 // GPU engine gives processAccum (tan/tanlibrary/src/Graal/GraalConv.cpp:1883-2145).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+
+#include <cstdint>
 
 #include "tanb_engine.h"
 #include "tanb_fft.cuh"
@@ -64,8 +71,7 @@ __device__ __forceinline__ size_t spec_index(const EngChan& ch, int slot, int pa
 // ---------------------------------------------------------------------------
 template <int LOG2M, int SPEC>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T)
-    eng_ir_kernel(EngChan* __restrict__ chans, const float* __restrict__ ir, const EngUpd* __restrict__ upd,
-                  const float2* __restrict__ tw) {
+    eng_ir_kernel(EngChan* __restrict__ chans, const EngUpd* __restrict__ upd, const float2* __restrict__ tw) {
   using S = FftShape<LOG2M>;
   constexpr int M = S::M, T = S::T;
   extern __shared__ float2 sm[];
@@ -74,9 +80,17 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   const EngUpd u = upd[blockIdx.y];
   const EngChan ch = chans[u.chan];
   if (part >= ch.P) return;
-  const float* h = ir + (size_t)blockIdx.y * u.stride + (size_t)part * M;
-  for (int n = threadIdx.x; n < M; n += T)
-    sm[n] = (n < M / 2) ? make_float2(h[2 * n], h[2 * n + 1]) : make_float2(0.f, 0.f);
+  // samples [part * M, part * M + M) of the row; zero at and after u.n
+  const long long t0 = (long long)part * M;
+  for (int n = threadIdx.x; n < M; n += T) {
+    const long long t = t0 + 2 * n;
+    float2 v = make_float2(0.f, 0.f);
+    if (n < M / 2) {
+      if (t < u.n) v.x = u.src[t];
+      if (t + 1 < u.n) v.y = u.src[t + 1];
+    }
+    sm[n] = v;
+  }
   __syncthreads();
   fft_inplace<LOG2M, false>(sm, tw);
   // split step in place: thread owning pair (k, M-k) writes both
@@ -122,120 +136,8 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
 }
 
 // ---------------------------------------------------------------------------
-template <int LOG2M, int SPEC>
-__global__ void __launch_bounds__(FftShape<LOG2M>::T)
-    eng_head_kernel(EngChan* __restrict__ chans, const float* __restrict__ in_base, float* __restrict__ out_base,
-                    int ld, const float2* __restrict__ tw) {
-  using S = FftShape<LOG2M>;
-  constexpr int M = S::M, T = S::T;
-  extern __shared__ float2 sm[];
-  float2* z = sm;
-  float2* z2 = sm + M;
-  const int c = blockIdx.x;
-  const EngChan ch = chans[c];
-  if (!ch.run) return;
-  const bool swap = ch.pending != 0;
-  const int P = ch.P;
-  const int cur = (ch.cur - 1 + P) % P;
-  const int slot_old = ch.active, slot_new = 1 - ch.active;
-  const float* x = in_base ? in_base + (size_t)c * ld : nullptr;
-  float* y = out_base + (size_t)c * ld;
-
-  for (int n = threadIdx.x; n < M; n += T) {
-    const float* src = (n < M / 2) ? ch.prev + 2 * n : (x ? x + 2 * (n - M / 2) : nullptr);
-    z[n] = src ? make_float2(src[0], src[1]) : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  for (int n = threadIdx.x; n < M / 2; n += T) reinterpret_cast<float2*>(ch.prev)[n] = z[n + M / 2];
-  fft_inplace<LOG2M, false>(z, tw);
-
-  float2* F = ch.fdl + (size_t)cur * M;
-  const size_t h0 = spec_index(ch, slot_old, 0, M);
-  const size_t h1 = spec_index(ch, slot_new, 0, M);
-  float s0 = 1.f, s1 = 1.f;
-  if constexpr (SPEC != kSpecFP32) {
-    s0 = ch.scale[(size_t)slot_old * P];
-    s1 = ch.scale[(size_t)slot_new * P];
-  }
-  const float inv_n = 1.0f / (float)(2 * M);
-  const float2* part0 = ch.part;
-  const float2* part1 = ch.part + (size_t)ch.nitem * M;
-  for (int k = threadIdx.x; k <= M / 2; k += T) {
-    const int km = (k == 0) ? 0 : M - k;
-    // tails: partial sums of the work items, in item order
-    float2 tk = make_float2(0.f, 0.f), tm = tk, uk = tk, um = tk;
-    for (int r = 0; r < ch.nitem; ++r) {
-      const float2 a = part0[(size_t)r * M + k], b = part0[(size_t)r * M + km];
-      tk.x += a.x; tk.y += a.y;
-      tm.x += b.x; tm.y += b.y;
-      if (swap) {
-        const float2 a1 = part1[(size_t)r * M + k], b1 = part1[(size_t)r * M + km];
-        uk.x += a1.x; uk.y += a1.y;
-        um.x += b1.x; um.y += b1.y;
-      }
-    }
-    if (k == 0) {
-      const float2 X = rfft_post_dc(z[0]);
-      F[0] = X;
-      float2 hh = SpecT<SPEC>::get(ch.H, h0);
-      hh.x *= s0; hh.y *= s0;
-      z[0] = irfft_pre_dc(c_mac_dc(tk, X, hh), inv_n);
-      if (swap) {
-        float2 hn = SpecT<SPEC>::get(ch.H, h1);
-        hn.x *= s1; hn.y *= s1;
-        z2[0] = irfft_pre_dc(c_mac_dc(uk, X, hn), inv_n);
-      }
-    } else {
-      const float2 wk = __ldg(tw + k), wm = __ldg(tw + km);
-      const float2 a = z[k], b = z[km];
-      const float2 Xk = rfft_post(a, b, wk);
-      const float2 Xm = rfft_post(b, a, wm);
-      F[k] = Xk;
-      if (km != k) F[km] = Xm;
-      float2 hk = SpecT<SPEC>::get(ch.H, h0 + k), hm = SpecT<SPEC>::get(ch.H, h0 + km);
-      hk.x *= s0; hk.y *= s0; hm.x *= s0; hm.y *= s0;
-      const float2 Ak = c_mac(tk, Xk, hk);
-      const float2 Am = c_mac(tm, Xm, hm);
-      z[k] = irfft_pre(Ak, Am, wk, inv_n);
-      if (km != k) z[km] = irfft_pre(Am, Ak, wm, inv_n);
-      if (swap) {
-        float2 gk = SpecT<SPEC>::get(ch.H, h1 + k), gm = SpecT<SPEC>::get(ch.H, h1 + km);
-        gk.x *= s1; gk.y *= s1; gm.x *= s1; gm.y *= s1;
-        const float2 Bk = c_mac(uk, Xk, gk);
-        const float2 Bm = c_mac(um, Xm, gm);
-        z2[k] = irfft_pre(Bk, Bm, wk, inv_n);
-        if (km != k) z2[km] = irfft_pre(Bm, Bk, wm, inv_n);
-      }
-    }
-  }
-  __syncthreads();
-  fft_inplace<LOG2M, true>(z, tw);
-  if (swap) fft_inplace<LOG2M, true>(z2, tw);
-  const float step = 1.0f / (float)M;
-  for (int m = M / 2 + threadIdx.x; m < M; m += T) {
-    const int i = 2 * (m - M / 2);
-    const float2 yo = z[m];
-    if (!swap) {
-      y[i] = yo.x;
-      y[i + 1] = yo.y;
-    } else {
-      const float2 yn = z2[m];
-      y[i] = yn.x * (step * (float)i) + yo.x * (step * (float)(M - i));
-      y[i + 1] = yn.y * (step * (float)(i + 1)) + yo.y * (step * (float)(M - i - 1));
-    }
-  }
-  if (threadIdx.x == 0) {
-    chans[c].cur = cur;
-    if (swap) {
-      chans[c].active = slot_new;
-      chans[c].pending = 0;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Two packed bins per thread. FDL rows are float4 pairs; spectra are float4
-// (FP32) or uint2 (two half2 / bfloat162) pairs.
+// Two packed bins (one float4 of a delay-line row) per unit; spectra are float4
+// (FP32) or uint2 (two half2 / bfloat162) per unit.
 template <int SPEC>
 __device__ __forceinline__ void load_h2(const void* H, size_t idx2, float2& a, float2& b) {
   if constexpr (SPEC == kSpecFP32) {
@@ -254,71 +156,280 @@ __device__ __forceinline__ void load_h2(const void* H, size_t idx2, float2& a, f
   }
 }
 
+template <int SPEC>
+__device__ __forceinline__ float2 spec_bin(const EngChan& ch, int slot, int part, int M, int k) {
+  float2 h = SpecT<SPEC>::get(ch.H, spec_index(ch, slot, part, M) + k);
+  if constexpr (SPEC != kSpecFP32) {
+    const float s = ch.scale[(size_t)slot * ch.P + part];
+    h.x *= s;
+    h.y *= s;
+  }
+  return h;
+}
+
+// Partial-sum row of a channel: rows [2 parity][2 mode][nitem][M] float2; mode
+// 0 = the IR in use for that block, 1 = a newly committed IR (swap block).
+__device__ __forceinline__ float2* part_row(const EngChan& ch, int parity, int mode, int row, int M) {
+  return ch.part + ((size_t)(parity * 2 + mode) * ch.nitem + row) * M;
+}
+
+// One work item: sum over partitions i in [w.i0, w.i1) of delay-line slot
+// (ch.cur + i + fs_off) mod P times IR-spectrum partition i of `slot`, into
+// part_row(parity, mode, w.row). M / 4 threads, units u and u + M / 4 each.
 template <int LOG2M, int SPEC>
-__global__ void __launch_bounds__(1 << (LOG2M - 1))
-    eng_tail_kernel(const EngChan* __restrict__ chans, const EngItem* __restrict__ items, int item0, int nitems,
-                    int mode) {
-  constexpr int M = 1 << LOG2M;
-  constexpr int U = M / 2;  // threads = pairs of bins
-  const int u = threadIdx.x;
-  for (int it = item0 + blockIdx.x; it < item0 + nitems; it += gridDim.x) {
+__device__ __forceinline__ void eng_item(const EngChan& ch, const EngItem& w, int slot, int fs_off, int parity,
+                                         int mode) {
+  constexpr int M = 1 << LOG2M, U = M / 2, T = M / 4, D = 2;
+  const int P = ch.P;
+  const float4* F = reinterpret_cast<const float4*>(ch.fdl);
+  const size_t hb = ((size_t)slot * P * M) / 2;  // unit index of (slot, partition 0)
+  const float* sc = (SPEC != kSpecFP32) ? ch.scale + (size_t)slot * P : nullptr;
+  const int u0 = threadIdx.x, u1 = threadIdx.x + T;
+  const bool dc = (u0 == 0);
+  float2 a0 = make_float2(0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
+  int fs = (ch.cur + w.i0 + fs_off) % P;
+  int i = w.i0;
+  for (; i + D <= w.i1; i += D) {
+    float4 f0[D], f1[D];
+    float2 p0[D], q0[D], p1[D], q1[D];
+    float s[D];
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      const size_t row = (size_t)fs * U;
+      f0[q] = __ldg(F + row + u0);
+      f1[q] = __ldg(F + row + u1);
+      const size_t hrow = hb + (size_t)(i + q) * U;
+      load_h2<SPEC>(ch.H, hrow + u0, p0[q], q0[q]);
+      load_h2<SPEC>(ch.H, hrow + u1, p1[q], q1[q]);
+      s[q] = (SPEC != kSpecFP32) ? __ldg(sc + i + q) : 1.f;
+      fs = (fs + 1 == P) ? 0 : fs + 1;
+    }
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      if (SPEC != kSpecFP32) {
+        p0[q].x *= s[q]; p0[q].y *= s[q]; q0[q].x *= s[q]; q0[q].y *= s[q];
+        p1[q].x *= s[q]; p1[q].y *= s[q]; q1[q].x *= s[q]; q1[q].y *= s[q];
+      }
+      const float2 fa = make_float2(f0[q].x, f0[q].y), fb = make_float2(f0[q].z, f0[q].w);
+      const float2 ga = make_float2(f1[q].x, f1[q].y), gb = make_float2(f1[q].z, f1[q].w);
+      a0 = dc ? c_mac_dc(a0, fa, p0[q]) : c_mac(a0, fa, p0[q]);
+      a1 = c_mac(a1, fb, q0[q]);
+      b0 = c_mac(b0, ga, p1[q]);
+      b1 = c_mac(b1, gb, q1[q]);
+    }
+  }
+  for (; i < w.i1; ++i) {
+    const size_t row = (size_t)fs * U;
+    const float4 g0 = __ldg(F + row + u0), g1 = __ldg(F + row + u1);
+    float2 pa, qa, pb, qb;
+    const size_t hrow = hb + (size_t)i * U;
+    load_h2<SPEC>(ch.H, hrow + u0, pa, qa);
+    load_h2<SPEC>(ch.H, hrow + u1, pb, qb);
+    if (SPEC != kSpecFP32) {
+      const float s = __ldg(sc + i);
+      pa.x *= s; pa.y *= s; qa.x *= s; qa.y *= s;
+      pb.x *= s; pb.y *= s; qb.x *= s; qb.y *= s;
+    }
+    fs = (fs + 1 == P) ? 0 : fs + 1;
+    const float2 fa = make_float2(g0.x, g0.y), fb = make_float2(g0.z, g0.w);
+    const float2 ga = make_float2(g1.x, g1.y), gb = make_float2(g1.z, g1.w);
+    a0 = dc ? c_mac_dc(a0, fa, pa) : c_mac(a0, fa, pa);
+    a1 = c_mac(a1, fb, qa);
+    b0 = c_mac(b0, ga, pb);
+    b1 = c_mac(b1, gb, qb);
+  }
+  float4* dst = reinterpret_cast<float4*>(part_row(ch, parity, mode, w.row, M));
+  dst[u0] = make_float4(a0.x, a0.y, a1.x, a1.y);
+  dst[u1] = make_float4(b0.x, b0.y, b1.x, b1.y);
+}
+
+// Head of block k for one channel (state `ch` as at launch). Tail of the IR in
+// use: the partial-sum rows of parity k plus X_{k-1} * H_1; on a swap block the
+// same for the new IR (mode-1 rows), and the output crossfades.
+template <int LOG2M, int SPEC>
+__device__ __forceinline__ void eng_head(const EngChan& ch, float2* sm, const float* x, float* y,
+                                         const float2* __restrict__ tw, int parity) {
+  using S = FftShape<LOG2M>;
+  constexpr int M = S::M, T = S::T;
+  float2* z = sm;
+  float2* z2 = sm + M;
+  const bool swap = ch.pending != 0;
+  const int P = ch.P;
+  const int cur = (ch.cur - 1 + P) % P;  // slot of X_k
+  const int slot_old = ch.active, slot_new = 1 - ch.active;
+
+  const bool x_vec = x && (reinterpret_cast<uintptr_t>(x) & 7) == 0;
+  for (int n = threadIdx.x; n < M; n += T) {
+    if (n < M / 2) {
+      z[n] = reinterpret_cast<const float2*>(ch.prev)[n];
+    } else if (!x) {
+      z[n] = make_float2(0.f, 0.f);
+    } else if (x_vec) {
+      z[n] = reinterpret_cast<const float2*>(x)[n - M / 2];
+    } else {
+      const float* src = x + 2 * (n - M / 2);
+      z[n] = make_float2(src[0], src[1]);
+    }
+  }
+  __syncthreads();
+  for (int n = threadIdx.x; n < M / 2; n += T) reinterpret_cast<float2*>(ch.prev)[n] = z[n + M / 2];
+  fft_inplace<LOG2M, false>(z, tw);
+
+  float2* F = ch.fdl + (size_t)cur * M;
+  const float2* Fp = ch.fdl + (size_t)ch.cur * M;  // X_{k-1}: partition 1
+  const float inv_n = 1.0f / (float)(2 * M);
+  const float2* pa = part_row(ch, parity, 0, 0, M);
+  const float2* pb = part_row(ch, parity, 1, 0, M);
+  for (int k = threadIdx.x; k <= M / 2; k += T) {
+    const int km = (k == 0) ? 0 : M - k;
+    // tails: partial sums of the work items in item order, then partition 1
+    float2 tk = make_float2(0.f, 0.f), tm = tk, uk = tk, um = tk;
+    for (int r = 0; r < ch.nitem; ++r) {
+      const float2 a = pa[(size_t)r * M + k], b = pa[(size_t)r * M + km];
+      tk.x += a.x; tk.y += a.y;
+      tm.x += b.x; tm.y += b.y;
+      if (swap) {
+        const float2 a1 = pb[(size_t)r * M + k], b1 = pb[(size_t)r * M + km];
+        uk.x += a1.x; uk.y += a1.y;
+        um.x += b1.x; um.y += b1.y;
+      }
+    }
+    if (P > 1) {
+      const float2 xk = Fp[k], xm = Fp[km];
+      const float2 hk = spec_bin<SPEC>(ch, slot_old, 1, M, k);
+      if (k == 0) {
+        tk = c_mac_dc(tk, xk, hk);
+        if (swap) uk = c_mac_dc(uk, xk, spec_bin<SPEC>(ch, slot_new, 1, M, 0));
+      } else {
+        tk = c_mac(tk, xk, hk);
+        tm = c_mac(tm, xm, spec_bin<SPEC>(ch, slot_old, 1, M, km));
+        if (swap) {
+          uk = c_mac(uk, xk, spec_bin<SPEC>(ch, slot_new, 1, M, k));
+          um = c_mac(um, xm, spec_bin<SPEC>(ch, slot_new, 1, M, km));
+        }
+      }
+    }
+    if (k == 0) {
+      const float2 X = rfft_post_dc(z[0]);
+      F[0] = X;
+      z[0] = irfft_pre_dc(c_mac_dc(tk, X, spec_bin<SPEC>(ch, slot_old, 0, M, 0)), inv_n);
+      if (swap) z2[0] = irfft_pre_dc(c_mac_dc(uk, X, spec_bin<SPEC>(ch, slot_new, 0, M, 0)), inv_n);
+    } else {
+      const float2 wk = __ldg(tw + k), wm = __ldg(tw + km);
+      const float2 a = z[k], b = z[km];
+      const float2 Xk = rfft_post(a, b, wk);
+      const float2 Xm = rfft_post(b, a, wm);
+      F[k] = Xk;
+      if (km != k) F[km] = Xm;
+      const float2 Ak = c_mac(tk, Xk, spec_bin<SPEC>(ch, slot_old, 0, M, k));
+      const float2 Am = c_mac(tm, Xm, spec_bin<SPEC>(ch, slot_old, 0, M, km));
+      z[k] = irfft_pre(Ak, Am, wk, inv_n);
+      if (km != k) z[km] = irfft_pre(Am, Ak, wm, inv_n);
+      if (swap) {
+        const float2 Bk = c_mac(uk, Xk, spec_bin<SPEC>(ch, slot_new, 0, M, k));
+        const float2 Bm = c_mac(um, Xm, spec_bin<SPEC>(ch, slot_new, 0, M, km));
+        z2[k] = irfft_pre(Bk, Bm, wk, inv_n);
+        if (km != k) z2[km] = irfft_pre(Bm, Bk, wm, inv_n);
+      }
+    }
+  }
+  __syncthreads();
+  fft_inplace<LOG2M, true>(z, tw);
+  if (swap) fft_inplace<LOG2M, true>(z2, tw);
+  const float step = 1.0f / (float)M;
+  const bool y_vec = (reinterpret_cast<uintptr_t>(y) & 7) == 0;
+  for (int m = M / 2 + threadIdx.x; m < M; m += T) {
+    const int i = 2 * (m - M / 2);
+    float2 o = z[m];
+    if (swap) {
+      const float2 yn = z2[m];
+      o = make_float2(yn.x * (step * (float)i) + o.x * (step * (float)(M - i)),
+                      yn.y * (step * (float)(i + 1)) + o.y * (step * (float)(M - i - 1)));
+    }
+    if (y_vec) {
+      reinterpret_cast<float2*>(y)[i / 2] = o;
+    } else {
+      y[i] = o.x;
+      y[i + 1] = o.y;
+    }
+  }
+}
+
+template <int LOG2M, int SPEC>
+__global__ void __launch_bounds__(FftShape<LOG2M>::T)
+    eng_block_kernel(EngChan* __restrict__ chans, int nslots, const EngItem* __restrict__ items, int nitems,
+                     const float* __restrict__ in_base, float* __restrict__ out_base, int ld,
+                     const float2* __restrict__ tw, EngSync sync) {
+  extern __shared__ float2 sm[];
+  __shared__ int last;
+  const long long k = *sync.block;  // blocks processed before this one
+  const int parity = (int)(k & 1);
+  if ((int)blockIdx.x < nslots) {
+    const int c = blockIdx.x;
+    const EngChan ch = chans[c];
+    if (ch.run)
+      eng_head<LOG2M, SPEC>(ch, sm, in_base ? in_base + (size_t)c * ld : nullptr, out_base + (size_t)c * ld, tw,
+                            parity);
+  } else {
+    const int stride = (int)gridDim.x - nslots;
+    for (int it = (int)blockIdx.x - nslots; it < nitems; it += stride) {
+      const EngItem w = items[it];
+      if (w.chan < 0) continue;
+      const EngChan ch = chans[w.chan];
+      if (!ch.run) continue;
+      // the next block's IR: the new one when this block swaps
+      eng_item<LOG2M, SPEC>(ch, w, ch.pending ? 1 - ch.active : ch.active, -2, parity ^ 1, 0);
+    }
+  }
+  // The last CTA to finish advances every channel and the block counter; every
+  // CTA has read the state above before it counts itself done.
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = (atomicAdd(sync.done, 1u) == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int c = threadIdx.x; c < nslots; c += blockDim.x) {
+    EngChan* ch = chans + c;
+    if (!ch->run) continue;
+    ch->cur = (ch->cur - 1 + ch->P) % ch->P;
+    if (ch->pending) {
+      ch->active = 1 - ch->active;
+      ch->pending = 0;
+    }
+  }
+  if (threadIdx.x == 0) {
+    *sync.block = k + 1;
+    *sync.done = 0u;
+  }
+}
+
+template <int LOG2M, int SPEC>
+__global__ void __launch_bounds__(FftShape<LOG2M>::T)
+    eng_commit_kernel(const EngChan* __restrict__ chans, const EngItem* __restrict__ items, int item0, int nitems,
+                      const long long* __restrict__ block) {
+  const int parity = (int)(*block & 1);  // the coming block
+  for (int it = item0 + (int)blockIdx.x; it < item0 + nitems; it += gridDim.x) {
     const EngItem w = items[it];
     if (w.chan < 0) continue;
     const EngChan ch = chans[w.chan];
-    if (mode == 0 ? !ch.run : !ch.pending) continue;
-    const int P = ch.P;
-    const int slot = (mode == 0) ? ch.active : 1 - ch.active;
-    // delay-line slot of partition i for the next block: (cur + i - 1) mod P
-    int fs = (ch.cur + w.i0 - 1) % P;
-    const float4* Fc = reinterpret_cast<const float4*>(ch.fdl) + u;
-    const size_t hbase2 = (((size_t)slot * P) * M) / 2 + u;  // in bin pairs
-    const float* sc = (SPEC != kSpecFP32) ? ch.scale + (size_t)slot * P : nullptr;
-    const bool dc = (u == 0);
-    float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0;
-    int i = w.i0;
-    for (; i + 4 <= w.i1; i += 4) {
-      float4 f[4];
-      float2 ha[4], hb[4];
-      float s[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        f[q] = __ldg(Fc + (size_t)fs * U);
-        load_h2<SPEC>(ch.H, hbase2 + (size_t)(i + q) * U, ha[q], hb[q]);
-        s[q] = (SPEC != kSpecFP32) ? __ldg(sc + i + q) : 1.f;
-        fs = (fs + 1 == P) ? 0 : fs + 1;
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (SPEC != kSpecFP32) {
-          ha[q].x *= s[q]; ha[q].y *= s[q]; hb[q].x *= s[q]; hb[q].y *= s[q];
-        }
-        const float2 fa = make_float2(f[q].x, f[q].y), fb = make_float2(f[q].z, f[q].w);
-        acc0 = dc ? c_mac_dc(acc0, fa, ha[q]) : c_mac(acc0, fa, ha[q]);
-        acc1 = c_mac(acc1, fb, hb[q]);
-      }
-    }
-    for (; i < w.i1; ++i) {
-      const float4 f = __ldg(Fc + (size_t)fs * U);
-      float2 ha, hb;
-      load_h2<SPEC>(ch.H, hbase2 + (size_t)i * U, ha, hb);
-      if (SPEC != kSpecFP32) {
-        const float s = __ldg(sc + i);
-        ha.x *= s; ha.y *= s; hb.x *= s; hb.y *= s;
-      }
-      fs = (fs + 1 == P) ? 0 : fs + 1;
-      const float2 fa = make_float2(f.x, f.y), fb = make_float2(f.z, f.w);
-      acc0 = dc ? c_mac_dc(acc0, fa, ha) : c_mac(acc0, fa, ha);
-      acc1 = c_mac(acc1, fb, hb);
-    }
-    float4* dst = reinterpret_cast<float4*>(ch.part + ((size_t)mode * ch.nitem + w.row) * M);
-    dst[u] = make_float4(acc0.x, acc0.y, acc1.x, acc1.y);
+    if (!ch.pending) continue;
+    eng_item<LOG2M, SPEC>(ch, w, 1 - ch.active, -1, parity, 1);
   }
+}
+
+// Marks channel slots [first, first + n) as holding a newly committed IR.
+__global__ void eng_mark_pending_kernel(EngChan* __restrict__ chans, int first, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) chans[first + i].pending = 1;
 }
 
 template <int LOG2M, int SPEC>
 cudaError_t attrs_t() {
   const int smem = 2 * (1 << LOG2M) * (int)sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(eng_head_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e =
+      cudaFuncSetAttribute(eng_block_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(eng_ir_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem / 2);
 }
@@ -332,26 +443,27 @@ cudaError_t attrs_all() {
 }
 
 template <int LOG2M, int SPEC>
-cudaError_t ir_t(EngChan* chans, const float* ir, const EngUpd* upd, int nupd, int maxP, const float2* tw,
-                 cudaStream_t st) {
+cudaError_t ir_t(EngChan* chans, const EngUpd* upd, int nupd, int maxP, const float2* tw, cudaStream_t st) {
   using S = FftShape<LOG2M>;
   dim3 grid(maxP, nupd);
-  eng_ir_kernel<LOG2M, SPEC><<<grid, S::T, S::M * sizeof(float2), st>>>(chans, ir, upd, tw);
+  eng_ir_kernel<LOG2M, SPEC><<<grid, S::T, S::M * sizeof(float2), st>>>(chans, upd, tw);
   return cudaGetLastError();
 }
 
 template <int LOG2M, int SPEC>
-cudaError_t head_t(EngChan* chans, int nslots, const float* in, float* out, int ld, const float2* tw,
-                   cudaStream_t st) {
+cudaError_t block_t(EngChan* chans, int nslots, const EngItem* items, int nitems, int tail_ctas, const float* in,
+                    float* out, int ld, const float2* tw, EngSync sync, cudaStream_t st) {
   using S = FftShape<LOG2M>;
-  eng_head_kernel<LOG2M, SPEC><<<nslots, S::T, 2 * S::M * sizeof(float2), st>>>(chans, in, out, ld, tw);
+  eng_block_kernel<LOG2M, SPEC><<<nslots + tail_ctas, S::T, 2 * S::M * sizeof(float2), st>>>(
+      chans, nslots, items, nitems, in, out, ld, tw, sync);
   return cudaGetLastError();
 }
 
 template <int LOG2M, int SPEC>
-cudaError_t tail_t(const EngChan* chans, const EngItem* items, int item0, int nitems, int mode, int grid,
-                   cudaStream_t st) {
-  eng_tail_kernel<LOG2M, SPEC><<<grid, 1 << (LOG2M - 1), 0, st>>>(chans, items, item0, nitems, mode);
+cudaError_t commit_t(const EngChan* chans, const EngItem* items, int item0, int nitems, int grid,
+                     const long long* block, cudaStream_t st) {
+  using S = FftShape<LOG2M>;
+  eng_commit_kernel<LOG2M, SPEC><<<grid, S::T, 0, st>>>(chans, items, item0, nitems, block);
   return cudaGetLastError();
 }
 
@@ -389,22 +501,29 @@ cudaError_t eng_prepare() {
   return r;
 }
 
-cudaError_t eng_launch_ir(int log2B, int spec, EngChan* chans, const float* ir, const EngUpd* upd, int nupd,
-                          int maxP, const float2* tw, cudaStream_t st) {
+cudaError_t eng_launch_ir(int log2B, int spec, EngChan* chans, const EngUpd* upd, int nupd, int maxP,
+                          const float2* tw, cudaStream_t st) {
   if (nupd <= 0) return cudaSuccess;
-  ENG_DISPATCH(log2B, spec, ir_t, chans, ir, upd, nupd, maxP, tw, st);
+  ENG_DISPATCH(log2B, spec, ir_t, chans, upd, nupd, maxP, tw, st);
 }
 
-cudaError_t eng_launch_head(int log2B, int spec, EngChan* chans, int nslots, const float* in, float* out, int ld,
-                            const float2* tw, cudaStream_t st) {
+cudaError_t eng_launch_block(int log2B, int spec, EngChan* chans, int nslots, const EngItem* items, int nitems,
+                             int tail_ctas, const float* in, float* out, int ld, const float2* tw, EngSync sync,
+                             cudaStream_t st) {
   if (nslots <= 0) return cudaSuccess;
-  ENG_DISPATCH(log2B, spec, head_t, chans, nslots, in, out, ld, tw, st);
+  ENG_DISPATCH(log2B, spec, block_t, chans, nslots, items, nitems, tail_ctas, in, out, ld, tw, sync, st);
 }
 
-cudaError_t eng_launch_tail(int log2B, int spec, const EngChan* chans, const EngItem* items, int item0,
-                            int nitems, int mode, int grid, cudaStream_t st) {
+cudaError_t eng_launch_mark_pending(EngChan* chans, int first, int n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  eng_mark_pending_kernel<<<(n + 255) / 256, 256, 0, st>>>(chans, first, n);
+  return cudaGetLastError();
+}
+
+cudaError_t eng_launch_commit(int log2B, int spec, const EngChan* chans, const EngItem* items, int item0,
+                              int nitems, int grid, const long long* block, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  ENG_DISPATCH(log2B, spec, tail_t, chans, items, item0, nitems, mode, grid, st);
+  ENG_DISPATCH(log2B, spec, commit_t, chans, items, item0, nitems, grid, block, st);
 }
 
 }  // namespace tanb

@@ -91,6 +91,13 @@ class Engine:
             return rc, None
         return rc, Session(self, sid.value, first.value, channels, ir_length)
 
+    def write_input(self, first_slot: int, x: np.ndarray) -> int:
+        """Copies the first `block` samples of each row of x (float32, C-contiguous
+        rows) into the input buffer at slots first_slot, first_slot + 1, ..."""
+        if x.dtype != np.float32 or not x.flags.c_contiguous or x.ndim != 2:
+            raise TypeError("x must be a C-contiguous float32 (rows, samples) array")
+        return lib().tanb_engine_write_input(self._h, first_slot, x.ctypes.data, x.shape[0], x.shape[1])
+
     def process(self) -> int:
         return lib().tanb_engine_process(self._h)
 
@@ -106,7 +113,7 @@ class Engine:
     def info(self) -> dict:
         out = (ctypes.c_int64 * 8)()
         lib().tanb_engine_info(self._h, out)
-        keys = ("sessions", "channels", "slot_hwm", "item_hwm", "arena_bytes", "budget", "tail_bytes_per_block",
+        keys = ("sessions", "channels", "slot_hwm", "item_hwm", "arena_bytes", "budget", "block_bytes",
                 "tail_grid")
         return dict(zip(keys, list(out)))
 
@@ -117,5 +124,5 @@ class Engine:
         counts = (ctypes.c_int64 * 4)()
         ms = (ctypes.c_double * 2)()
         lib().tanb_engine_profile_read(self._h, counts, ms)
-        return {"heads": counts[0], "tails": counts[1], "ir_updates": counts[2], "timed": counts[3],
-                "head_ms": ms[0], "tail_ms": ms[1]}
+        return {"blocks": counts[0], "commits": counts[1], "ir_updates": counts[2], "timed": counts[3],
+                "block_ms": ms[0]}

@@ -161,11 +161,11 @@ def _block_latencies_batched(ctx, nsess, C, L, block, spectrum, blocks, g, pool)
             return None
         s.update_response_td(pool.get(g, C, L), block_until_ready=True)
         sess.append(s)
-    x = g.uniform(-1, 1, (nsess * C + 8, block)).astype(np.float32)
+    x = g.uniform(-1, 1, (nsess * C, block)).astype(np.float32)
     lat = []
     for k in range(blocks + 5):
         t0 = time.perf_counter()
-        e.inp[: nsess * C] = x[: nsess * C]
+        assert e.write_input(0, x) == cv.AMF_OK  # the block's input, every channel
         assert e.process() == cv.AMF_OK
         if k >= 5:
             lat.append(1000.0 * (time.perf_counter() - t0))

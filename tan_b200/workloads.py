@@ -122,7 +122,7 @@ def cfg3(ctx, quick=False):
             errs.append(_db(y[c], ref))
         out[name] = {"error_db_vs_fp64": {"min": min(errs), "median": float(np.median(errs)), "max": max(errs),
                                           "channels_sampled": len(errs)},
-                     "latency_ms": _pct(lat[4:]), "tail_bytes_per_block": info["tail_bytes_per_block"],
+                     "latency_ms": _pct(lat[4:]), "block_bytes": info["block_bytes"],
                      "device_bytes": info["arena_bytes"]}
     return out
 

@@ -174,3 +174,62 @@ def test_engine_async_update_from_another_thread(tan_ctx):
     rms = np.sqrt(np.mean(ya.astype(np.float64) ** 2))
     assert np.max(np.abs(y - ya)) <= TOL * rms
     engine.release()
+
+
+def test_engine_device_io_equals_host_io(tan_ctx):
+    """process_device (device rows, stride ld) and process (pinned host
+    buffers) run the same block launch: outputs are bit-identical, also on a
+    swap block and for sessions with P <= 2 (no work items)."""
+    import torch
+
+    g = H.rng(35)
+    B, nb = 256, 20
+    specs = [(2, 9000), (1, 700), (3, 40000), (1, 256)]
+    irs0 = [H.irs(g, C, L) for C, L in specs]
+    irs1 = [H.irs(g, C, L) for C, L in specs]
+    engines, sess = [], []
+    for _ in range(2):
+        e = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=256 << 20, max_channels=16, partitions_per_item=8)
+        ss = []
+        for C, L in specs:
+            rc, s = e.open_session(C, L)
+            assert rc == 0
+            ss.append(s)
+        engines.append(e)
+        sess.append(ss)
+    nslots = engines[0].info()["slot_hwm"]
+    x = H.noise(g, nslots, nb * B)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros_like(xd)
+    yh = np.zeros_like(x)
+    for k in range(nb):
+        for j in range(len(specs)):
+            for e, ss in zip(engines, sess):
+                if k in (0, 9):
+                    ir = irs0[j] if k == 0 else irs1[j]
+                    assert ss[j].update_response_td(ir, block_until_ready=True) == 0
+        engines[0].inp[:nslots] = x[:, k * B:(k + 1) * B]
+        assert engines[0].process() == 0
+        yh[:, k * B:(k + 1) * B] = engines[0].out[:nslots]
+        assert engines[1].process_device(xd.data_ptr() + k * B * 4, yd.data_ptr() + k * B * 4, nb * B) == 0, \
+            cv.last_error()
+    assert engines[1].synchronize() == 0
+    assert np.array_equal(yd.cpu().numpy(), yh)
+    for e in engines:
+        e.release()
+
+
+def test_engine_write_input_rows(tan_ctx):
+    """write_input copies block samples of strided rows into the input buffer
+    at consecutive slots (threaded above 1 MB) and refuses slots out of range."""
+    B = 256
+    e = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=64 << 20, max_channels=2048)
+    g = H.rng(36)
+    x = H.noise(g, 1500, 3 * B)  # rows longer than a block: ld = 3B
+    assert e.write_input(5, x) == 0
+    assert np.array_equal(e.inp[5:1505], x[:, :B])
+    small = H.noise(g, 3, B)
+    assert e.write_input(0, small) == 0
+    assert np.array_equal(e.inp[0:3], small)
+    assert e.write_input(2047, small) == cv.AMF_INVALID_ARG
+    e.release()
