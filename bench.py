@@ -253,6 +253,30 @@ def read_traffic(name="tail_kernel_cfg2.txt"):
     return None
 
 
+def size_floor(torch, stream, flush_l2, nbytes, dev, reps=50):
+    """What one bandwidth-bound launch over `nbytes` reaches when timed like the
+    tail kernel: a library reduction (torch sum) reading nbytes from HBM, L2
+    flushed before each launch, CUDA events around it; median of `reps`."""
+    buf = torch.ones(nbytes // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    out = torch.empty((), dtype=torch.float32, device=f"cuda:{dev}")
+    ms = []
+    with torch.cuda.stream(stream):
+        for r in range(reps + 3):
+            flush_l2()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            torch.sum(buf, dtype=torch.float32, out=out)
+            b.record(stream)
+            b.synchronize()
+            if r >= 3:
+                ms.append(a.elapsed_time(b))
+    us = 1e3 * statistics.median(ms)
+    del buf
+    return {"bytes": nbytes, "us": us, "gbs": nbytes / (us * 1e-6) / 1e9,
+            "what": "torch sum over the same bytes, one launch, L2 flushed, CUDA events (median)"}
+
+
 def hbm_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -361,6 +385,7 @@ def run_ours(args):
     bytes_per_tail = C * ((P - 1) * B * 16 + B * 8)
     peak, peak_kind = hbm_peak()
     achieved = bytes_per_tail / (tail_ms_avg / 1e3) / 1e9
+    floor = size_floor(torch, stream, flush_l2, bytes_per_tail, dev)
     conv.Release()
     plain = {"value": value, "ms_per_step": dev_ms / args.steps, "gpu_launches": launches,
              "roofline_frac": achieved / peak, "tail_gbs": achieved}
@@ -424,6 +449,7 @@ def run_ours(args):
     eng_block_us = 1000.0 * eprof["block_ms"] / max(1, eprof["timed"])
     eng_block_bytes = einfo["block_bytes"]
     eng_achieved = eng_block_bytes / (eng_block_us * 1e-6) / 1e9
+    eng_floor = size_floor(torch, estream, eflush, eng_block_bytes, dev)
     engine_path = {"value": eng_value, "ms_per_step": eng_ms / args.steps,
                    "gpu_launches": ecounts["blocks"] + ecounts["commits"] + ecounts["ir_updates"],
                    "roofline_frac": eng_achieved / peak, "block_gbs": eng_achieved,
@@ -493,7 +519,7 @@ def run_ours(args):
         best_name = "engine" if best is engine_path else "drop-in"
         if best is engine_path:
             achieved, bytes_per_tail, tail_ms_avg = eng_achieved, eng_block_bytes, eng_block_us / 1e3
-            launches, clk = engine_path["gpu_launches"], eclk
+            launches, clk, floor = engine_path["gpu_launches"], eclk, eng_floor
         line = {
             "metric": METRIC, "value": best["value"], "unit": "GSamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": best["ms_per_step"], "higher_is_better": True,
@@ -513,7 +539,9 @@ def run_ours(args):
                          if best is engine_path else "tail_kernel (partition MAC)",
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "bytes_per_launch": bytes_per_tail, "avg_launch_us": tail_ms_avg * 1e3,
-                         "launches_timed": tail["timed"], "tiling": list(tiling)},
+                         "launches_timed": tail["timed"], "tiling": list(tiling),
+                         "size_floor": dict(floor, frac_of_peak=floor["gbs"] / peak,
+                                            tail_vs_floor=achieved / floor["gbs"])},
             "kernel_ms": {k: v["ms"] for k, v in prof.items()},
             "e2e": {"value": e2e_value, "unit": "GSamples/s", "h2d_bytes_per_step": C * B * 4 + 32 * C,
                     "d2h_bytes_per_step": C * B * 4,
