@@ -39,6 +39,7 @@ enum {
   TANB_NOT_INITIALIZED = 13,
   TANB_WRONG_STATE = 15,
   TANB_NO_DEVICE = 17,
+  TANB_TAN_CLIPPING_WAS_REQUIRED = 42,
   TANB_TAN_UNSUPPORTED_VERSION = 43
 };
 
@@ -167,6 +168,24 @@ int32_t tanb_convolution_process_device(tanb_convolution* conv,
                                         size_t numOfSamples,
                                         const uint32_t* flagMasks,
                                         size_t* pNumOfSamplesProcessed);
+
+/* Fused PCM pipeline (no single reference counterpart): the per-block chain
+ * of samples/src/common/SimpleVRaudio.cpp:1059-1117 -- TANConverter
+ * short->float of each channel's input, TANConvolution::Process, TANMixer::Mix
+ * of the channels of each output group, TANConverter float->short of each mix
+ * -- in one call, the conversions and the mix done inside the head kernel.
+ * Channel c reads in[c][i * in_step] (int16, converted as
+ * tanb_converter_short_to_float with in_gain) and is mixed into output group
+ * group[c] < ngroups <= channels (every group needs a channel); a group sums
+ * its channels from 0 in ascending channel order (Mixer.cl:26-41) and its
+ * sample i goes to out[g][i * out_step], converted with out_gain by the device
+ * float->short rule (Converter.cl:97-120); *clipped reports any clamped
+ * sample. Whole blocks of n as tanb_convolution_process; no channel flags;
+ * not for TIME_DOMAIN. */
+int32_t tanb_convolution_process_mix_pcm16(tanb_convolution* conv, const int16_t* const* in, size_t in_step,
+                                           float in_gain, const uint32_t* group, uint32_t ngroups,
+                                           int16_t* const* out, size_t out_step, float out_gain, size_t n,
+                                           int32_t* clipped, size_t* done);
 
 /* TANConvolution::ProcessDirect(float* ir[], float* in[], float* out[], ...) --
  * TrueAudioNext.h:223-230, ConvolutionImpl.cpp:721-762. TIME_DOMAIN method only
@@ -306,6 +325,59 @@ int32_t tanb_engine_session_state(tanb_engine* engine, int32_t session, int64_t 
  * with profiling enabled), ms[1] 0. Reading resets. */
 int32_t tanb_engine_profile(tanb_engine* engine, int32_t enable);
 int32_t tanb_engine_profile_read(tanb_engine* engine, int64_t counts[4], double ms[2]);
+
+/* ---------------------------------------------------------------------------
+ * TANConverter (TrueAudioNext.h:344-398; TANCreateConverter :653-656) and
+ * TANMixer (TrueAudioNext.h:611-634; TANCreateMixer :657-660), the conversion
+ * and mixing steps either side of the convolution. Host-pointer overloads give
+ * the reference's CPU results bit for bit (ConverterImpl.cpp:217-408,
+ * MixerImpl.cpp:226-250); device-pointer overloads those of its OpenCL kernels
+ * (Converter.cl:27-120, Mixer.cl:26-41). All computation runs on the GPU.
+ * ------------------------------------------------------------------------- */
+enum { TANB_SAMPLE_TYPE_FLOAT = 0, TANB_SAMPLE_TYPE_SHORT = 1 }; /* TrueAudioNext.h:73-77 */
+
+typedef struct tanb_converter tanb_converter;
+/* TANCreateConverter + Init / Terminate. */
+int32_t tanb_converter_create(tanb_context* ctx, tanb_converter** converter);
+int32_t tanb_converter_release(tanb_converter* converter);
+/* Convert(short*, inputStep, n, float*, outputStep, gain) (TrueAudioNext.h:353-356):
+ * out[i * out_step] = in[i * in_step] * (gain / 32767). */
+int32_t tanb_converter_short_to_float(tanb_converter* converter, const int16_t* in, size_t in_step, size_t n,
+                                      float* out, size_t out_step, float gain);
+/* Convert(float*, inputStep, n, short*, outputStep, gain, bool* clipped)
+ * (TrueAudioNext.h:357-360); *clipped (if not null) as the reference reports it. */
+int32_t tanb_converter_float_to_short(tanb_converter* converter, const float* in, size_t in_step, size_t n,
+                                      int16_t* out, size_t out_step, float gain, int32_t* clipped);
+/* Batch forms over `count` buffers (TrueAudioNext.h:363-373). */
+int32_t tanb_converter_short_to_float_batch(tanb_converter* converter, const int16_t* const* in, size_t in_step,
+                                            size_t n, float* const* out, size_t out_step, float gain,
+                                            int32_t count);
+int32_t tanb_converter_float_to_short_batch(tanb_converter* converter, const float* const* in, size_t in_step,
+                                            size_t n, int16_t* const* out, size_t out_step, float gain,
+                                            int32_t count, int32_t* clipped);
+/* Device buffers (the cl_mem overloads, TrueAudioNext.h:375-397): buffer i's
+ * sample j at in[i] + (in_offsets[i] + j * in_step) elements of in_type, the
+ * same for out; offsets may be null (0). Asynchronous on the converter's
+ * stream unless `clipped` is requested (then it waits, as the reference). */
+int32_t tanb_converter_convert_device(tanb_converter* converter, const void* const* in, size_t in_step,
+                                      const size_t* in_offsets, int32_t in_type, void* const* out, size_t out_step,
+                                      const size_t* out_offsets, int32_t out_type, size_t n, float gain,
+                                      int32_t count, int32_t* clipped);
+int32_t tanb_converter_synchronize(tanb_converter* converter);
+void* tanb_converter_stream(tanb_converter* converter);
+
+typedef struct tanb_mixer tanb_mixer;
+/* TANCreateMixer + Init(buffer_size, num_channels) (TrueAudioNext.h:616). */
+int32_t tanb_mixer_create(tanb_context* ctx, size_t buffer_size, int32_t channels, tanb_mixer** mixer);
+int32_t tanb_mixer_release(tanb_mixer* mixer);
+/* Mix(float* in[], float* out) (TrueAudioNext.h:620-622): host buffers. */
+int32_t tanb_mixer_mix(tanb_mixer* mixer, const float* const* in, float* out);
+/* Mix(cl_mem in[], cl_mem out) (:625-627) and Mix(cl_mem in, cl_mem out, stride)
+ * (:630-633): device buffers, asynchronous on the mixer's stream. */
+int32_t tanb_mixer_mix_device(tanb_mixer* mixer, const float* const* in, float* out);
+int32_t tanb_mixer_mix_device_strided(tanb_mixer* mixer, const float* in, float* out, size_t input_stride);
+int32_t tanb_mixer_synchronize(tanb_mixer* mixer);
+void* tanb_mixer_stream(tanb_mixer* mixer);
 
 /* ---------------------------------------------------------------------------
  * Non-uniformly partitioned convolution: the TAN_CONVOLUTION_METHOD_*_NONUNIFORM

@@ -51,6 +51,17 @@ def lib() -> ctypes.CDLL:
                                                ctypes.POINTER(ctypes.c_int32)]
         fp = ctypes.c_void_p
         L.tanref_rfft.argtypes = [i32, fp, fp, fp]
+        s16p = ctypes.POINTER(ctypes.c_int16)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        L.tanref_convert_s16_f32.argtypes = [s16p, sz, sz, fp, sz, ctypes.c_float]
+        L.tanref_convert_s16_f32.restype = None
+        for name in ("tanref_convert_f32_s16", "tanref_convert_f32_s16_dev"):
+            getattr(L, name).argtypes = [fp, sz, sz, s16p, sz, ctypes.c_float, i32p]
+            getattr(L, name).restype = None
+        L.tanref_mix.argtypes = [fpp, i32, sz, fp]
+        L.tanref_mix.restype = None
+        L.tanref_mix_dev.argtypes = [fp, sz, i32, sz, fp]
+        L.tanref_mix_dev.restype = None
         L.tanref_irfft.argtypes = [i32, fp, fp, fp]
         _lib = L
     return _lib
@@ -161,4 +172,47 @@ def irfft(re: np.ndarray, im: np.ndarray):
     N = 2 * (re.size - 1)
     y = np.zeros(N, np.float32)
     lib().tanref_irfft(N, re.ctypes.data, im.ctypes.data, y.ctypes.data)
+    return y
+
+
+# --- TANConverter / TANMixer restatements --------------------------------------
+
+
+def _span(a: np.ndarray, dtype):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a, a.ctypes.data_as(ctypes.POINTER(np.ctypeslib.as_ctypes_type(dtype)))
+
+
+def convert_s16_f32(x: np.ndarray, gain: float, in_step: int = 1, n: int | None = None) -> np.ndarray:
+    """short -> float (ConverterImpl.cpp:217-246) of samples x[0], x[in_step], ..."""
+    x, px = _span(x, np.int16)
+    n = (x.size + in_step - 1) // in_step if n is None else n
+    y = np.zeros(n, np.float32)
+    lib().tanref_convert_s16_f32(px, in_step, n, y.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 1, gain)
+    return y
+
+
+def convert_f32_s16(x: np.ndarray, gain: float, in_step: int = 1, n: int | None = None, device: bool = False):
+    """float -> short; (output, clipped). device=False: the CPU overload
+    (ConverterImpl.cpp:287-408); device=True: the OpenCL kernel (Converter.cl:97-120)."""
+    x, px = _span(x, np.float32)
+    n = (x.size + in_step - 1) // in_step if n is None else n
+    y = np.zeros(n, np.int16)
+    clip = ctypes.c_int32(0)
+    fn = lib().tanref_convert_f32_s16_dev if device else lib().tanref_convert_f32_s16
+    fn(px, in_step, n, y.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)), 1, gain, ctypes.byref(clip))
+    return y, bool(clip.value)
+
+
+def mix(x: np.ndarray, device: bool = False) -> np.ndarray:
+    """Sum over channels of x (channels, n) in channel order: MixerImpl.cpp:226-250
+    (device=False) or Mixer.cl:26-41 (device=True)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    C, n = x.shape
+    y = np.zeros(n, np.float32)
+    py = y.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    if device:
+        lib().tanref_mix_dev(x.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, C, n, py)
+    else:
+        lib().tanref_mix(_ptrs([x[c] for c in range(C)]), C, n, py)
     return y

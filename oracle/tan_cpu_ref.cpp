@@ -492,4 +492,90 @@ int tanref_irfft(int N, const float* re, const float* im, float* y) {
   return kOk;
 }
 
+// ---------------------------------------------------------------------------
+// TANConverter and TANMixer (test infrastructure, as everything in this file).
+// ---------------------------------------------------------------------------
+
+// short -> float, TANConverterImpl::Convert(short*, ...) ConverterImpl.cpp:217-246:
+// out = (float)in * (gain / SHRT_MAX), scale rounded once to float.
+void tanref_convert_s16_f32(const int16_t* in, size_t in_step, size_t n, float* out, size_t out_step, float gain) {
+  const float scale = gain / 32767;
+  for (size_t i = 0; i < n; ++i) out[i * out_step] = in[i * in_step] * scale;
+}
+
+// float -> short, TANConverterImpl::Convert(float*, ...) ConverterImpl.cpp:287-408
+// with its SSE2 path taken (ConverterImpl.cpp:69): while at least 8 samples
+// remain, 8 products are rounded to nearest even by cvtps2dq (out-of-range and
+// NaN give INT_MIN) and packed to 16 bits with saturation, without setting
+// the clip flag; the last n mod 8 samples are truncated toward zero (cvttss2si,
+// INT_MIN out of range), clamped, and set the flag when clamped.
+void tanref_convert_f32_s16(const float* in, size_t in_step, size_t n, int16_t* out, size_t out_step, float gain,
+                            int32_t* clipped) {
+  const float scale = 32767 * gain;
+  bool clip = false;
+  size_t i = 0;
+  for (; n - i >= 8; i += 8) {
+    alignas(16) float f[8];
+    for (int j = 0; j < 8; ++j) f[j] = in[(i + j) * in_step] * scale;
+    const __m128i a = _mm_cvtps_epi32(_mm_load_ps(f));
+    const __m128i b = _mm_cvtps_epi32(_mm_load_ps(f + 4));
+    alignas(16) int16_t s8[8];
+    _mm_store_si128(reinterpret_cast<__m128i*>(s8), _mm_packs_epi32(a, b));
+    for (int j = 0; j < 8; ++j) out[(i + j) * out_step] = s8[j];
+  }
+  for (; i < n; ++i) {
+    const float f = in[i * in_step] * scale;
+    long v = _mm_cvttss_si32(_mm_set_ss(f));
+    if (v > 32767) {
+      v = 32767;
+      clip = true;
+    }
+    if (v < -32768) {
+      v = -32768;
+      clip = true;
+    }
+    out[i * out_step] = (int16_t)v;
+  }
+  if (clipped) *clipped = clip ? 1 : 0;
+}
+
+// float -> short as the reference's OpenCL kernel floatToShort
+// (Converter.cl:97-120): clamp to [SHRT_MIN, SHRT_MAX] setting the flag, then
+// convert_short (round toward zero). NaN converts to 0 here (the kernel leaves
+// it to the device).
+void tanref_convert_f32_s16_dev(const float* in, size_t in_step, size_t n, int16_t* out, size_t out_step, float gain,
+                                int32_t* clipped) {
+  const float scale = 32767 * gain;
+  bool clip = false;
+  for (size_t i = 0; i < n; ++i) {
+    float f = in[i * in_step] * scale;
+    if (f > 32767) {
+      f = 32767;
+      clip = true;
+    }
+    if (f < -32768) {
+      f = -32768;
+      clip = true;
+    }
+    out[i * out_step] = (f != f) ? 0 : (int16_t)f;
+  }
+  if (clipped) *clipped = clip ? 1 : 0;
+}
+
+// TANMixerImpl::Mix(float**, float*) MixerImpl.cpp:226-250: out = in[0], then
+// out += in[c] for c = 1.. in channel order.
+void tanref_mix(const float* const* in, int channels, size_t n, float* out) {
+  for (int c = 0; c < channels; ++c)
+    for (size_t i = 0; i < n; ++i) out[i] = (c == 0) ? in[0][i] : out[i] + in[c][i];
+}
+
+// Mixer.cl:26-41 (device buffers): sum = 0, then sum += in[c] in channel order.
+void tanref_mix_dev(const float* in, size_t stride, int channels, size_t n, float* out) {
+  for (size_t i = 0; i < n; ++i) {
+    float sum = 0.f;
+    for (int c = 0; c < channels; ++c) sum += in[(size_t)c * stride + i];
+    out[i] = sum;
+  }
+}
+
 }  // extern "C"

@@ -105,6 +105,27 @@ SIGNATURES = {
     "tanb_engine_session_state": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_engine_profile": (_i32, [_vp, _i32]),
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
+    "tanb_convolution_process_mix_pcm16": (_i32, [_vp, _pp, _sz, ctypes.c_float, _u32p, _u32, _pp, _sz,
+                                                  ctypes.c_float, _sz, ctypes.POINTER(ctypes.c_int32), _szp]),
+    "tanb_converter_create": (_i32, [_vp, ctypes.POINTER(_vp)]),
+    "tanb_converter_release": (_i32, [_vp]),
+    "tanb_converter_short_to_float": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz, ctypes.c_float]),
+    "tanb_converter_float_to_short": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz, ctypes.c_float,
+                                             ctypes.POINTER(ctypes.c_int32)]),
+    "tanb_converter_short_to_float_batch": (_i32, [_vp, _pp, _sz, _sz, _pp, _sz, ctypes.c_float, _i32]),
+    "tanb_converter_float_to_short_batch": (_i32, [_vp, _pp, _sz, _sz, _pp, _sz, ctypes.c_float, _i32,
+                                                   ctypes.POINTER(ctypes.c_int32)]),
+    "tanb_converter_convert_device": (_i32, [_vp, _pp, _sz, _szp, _i32, _pp, _sz, _szp, _i32, _sz, ctypes.c_float,
+                                             _i32, ctypes.POINTER(ctypes.c_int32)]),
+    "tanb_converter_synchronize": (_i32, [_vp]),
+    "tanb_converter_stream": (_vp, [_vp]),
+    "tanb_mixer_create": (_i32, [_vp, _sz, _i32, ctypes.POINTER(_vp)]),
+    "tanb_mixer_release": (_i32, [_vp]),
+    "tanb_mixer_mix": (_i32, [_vp, _pp, _vp]),
+    "tanb_mixer_mix_device": (_i32, [_vp, _pp, _vp]),
+    "tanb_mixer_mix_device_strided": (_i32, [_vp, _vp, _vp, _sz]),
+    "tanb_mixer_synchronize": (_i32, [_vp]),
+    "tanb_mixer_stream": (_vp, [_vp]),
     "tanb_nu_schedule": (_i32, [_u32, _u32, _u32, _u32p, _u32p, _u32p]),
     "tanb_nu_create": (_i32, [_vp, _u32, _u32, _u32, _u32p, _u32p, _u32, ctypes.POINTER(_vp)]),
     "tanb_nu_release": (_i32, [_vp]),
@@ -301,6 +322,22 @@ class TANConvolution:
         rc = lib().tanb_convolution_process_direct(self._h, rir, rin, rout, numOfSamplesToProcess,
                                                    ctypes.byref(done), nz)
         return rc, done.value
+
+    def ProcessMixPcm16(self, x16, in_step: int, in_gain: float, group, ngroups: int, out16, out_step: int,
+                        out_gain: float, numOfSamplesToProcess: int):
+        """Fused int16 -> convolution -> mix -> int16 pipeline on host rows:
+        x16 (channels rows of int16, read with in_step), out16 (ngroups rows
+        of int16, written with out_step). Returns (rc, clipped, done)."""
+        ins = (ctypes.c_void_p * len(x16))(*[r.ctypes.data for r in x16])
+        outs = (ctypes.c_void_p * len(out16))(*[r.ctypes.data for r in out16])
+        g = np.ascontiguousarray(np.asarray(group, dtype=np.uint32))
+        clip = ctypes.c_int32(0)
+        done = ctypes.c_size_t(0)
+        rc = lib().tanb_convolution_process_mix_pcm16(self._h, ins, in_step, in_gain,
+                                                      g.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), ngroups,
+                                                      outs, out_step, out_gain, numOfSamplesToProcess,
+                                                      ctypes.byref(clip), ctypes.byref(done))
+        return rc, bool(clip.value), done.value
 
     def ProcessFinalize(self) -> int:
         return lib().tanb_convolution_process_finalize(self._h)

@@ -114,6 +114,12 @@ struct tanb_convolution {
 
   cudaEvent_t ev_stage = nullptr, ev_ir = nullptr, ev_out = nullptr;
 
+  // fused PCM pipeline (tanb_convolution_process_mix_pcm16), allocated on first use
+  float* d_mix_scratch = nullptr;   // [C][B] channel outputs
+  int* d_mix_table = nullptr;       // chan_group[C], gstart[C + 1], gchan[C], count[C]
+  int* h_clip = nullptr;            // host-mapped clip flag
+  std::vector<uint32_t> mix_groups; // group map the table holds
+
   // TIME_DOMAIN method state (history of `length` samples per channel)
   bool td = false;
   float* td_hist = nullptr;    // [C][length]
@@ -206,6 +212,13 @@ void free_all(tanb_convolution* v) {
   cudaFree(v->d_stage);
   cudaFree(v->d_ir);
   cudaFree(v->d_uctl);
+  cudaFree(v->d_mix_scratch);
+  cudaFree(v->d_mix_table);
+  cudaFreeHost(v->h_clip);
+  v->d_mix_scratch = nullptr;
+  v->d_mix_table = nullptr;
+  v->h_clip = nullptr;
+  v->mix_groups.clear();
   cudaFreeHost(v->h_stage);
   cudaFreeHost(v->h_out);
   cudaFreeHost(v->h_ir);
@@ -414,8 +427,71 @@ int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_
   return nrun;
 }
 
+// Rows and rules of the fused PCM pipeline (tanb_convolution_process_mix_pcm16).
+struct PcmIO {
+  const int16_t* const* in;
+  size_t in_step;
+  float in_gain;
+  const uint32_t* group;
+  uint32_t ngroups;
+  int16_t* const* out;
+  size_t out_step;
+  float out_gain;
+};
+
+// Device table of the group map (channels of each group in ascending order)
+// and the fused pipeline's scratch; uploaded when the map changes.
+cudaError_t ensure_mix(tanb_convolution* v, const PcmIO& pcm, tanb::MixEpi* epi) {
+  const int C = v->C, B = v->B;
+  cudaError_t e;
+  if (!v->d_mix_scratch && (e = cudaMalloc(&v->d_mix_scratch, (size_t)C * B * sizeof(float))) != cudaSuccess) return e;
+  if (!v->d_mix_table) {
+    if ((e = cudaMalloc(&v->d_mix_table, (size_t)(4 * C + 1) * sizeof(int))) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(v->d_mix_table, 0, (size_t)(4 * C + 1) * sizeof(int), v->stream)) != cudaSuccess)
+      return e;
+  }
+  if (!v->h_clip && (e = cudaHostAlloc(reinterpret_cast<void**>(&v->h_clip), sizeof(int), cudaHostAllocMapped)) !=
+                        cudaSuccess)
+    return e;
+  int* chan_group = v->d_mix_table;
+  int* gstart = chan_group + C;
+  int* gchan = gstart + C + 1;
+  unsigned* count = reinterpret_cast<unsigned*>(gchan + C);
+  std::vector<uint32_t> map(pcm.group, pcm.group + C);
+  map.push_back(pcm.ngroups);
+  if (map != v->mix_groups) {
+    std::vector<int> t(3 * C + 1);
+    int* hg = t.data();
+    int* hs = hg + C;
+    int* hc = hs + C + 1;
+    std::vector<int> fill(pcm.ngroups + 1, 0);
+    for (int c = 0; c < C; ++c) {
+      hg[c] = (int)pcm.group[c];
+      fill[pcm.group[c] + 1] += 1;
+    }
+    for (uint32_t g = 0; g < pcm.ngroups; ++g) fill[g + 1] += fill[g];
+    for (uint32_t g = 0; g <= pcm.ngroups; ++g) hs[g] = fill[g];
+    for (int c = 0; c < C; ++c) hc[fill[pcm.group[c]]++] = c;  // ascending within each group
+    if ((e = cudaMemcpyAsync(chan_group, hg, t.size() * sizeof(int), cudaMemcpyHostToDevice, v->stream)) !=
+        cudaSuccess)
+      return e;
+    if ((e = cudaStreamSynchronize(v->stream)) != cudaSuccess) return e;  // t is pageable and local
+    v->mix_groups = map;
+  }
+  epi->active = 1;
+  epi->in_scale = pcm.in_gain / 32767;
+  epi->out_scale = 32767 * pcm.out_gain;
+  epi->chan_group = chan_group;
+  epi->gstart = gstart;
+  epi->gchan = gchan;
+  epi->count = count;
+  epi->scratch = v->d_mix_scratch;
+  epi->clip = v->h_clip;
+  return cudaSuccess;
+}
+
 int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
-                       size_t n, const uint32_t* flags, size_t* done) {
+                       size_t n, const uint32_t* flags, size_t* done, const PcmIO* pcm = nullptr) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
   std::lock_guard<std::mutex> lock(v->mu);
   if (done) *done = 0;
@@ -430,6 +506,11 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   size_t nblocks = n / (size_t)B;
   size_t processed = 0;
   int32_t status = TANB_OK;
+  tanb::MixEpi epi;
+  if (pcm) {
+    TANB_CUDA(ensure_mix(v, *pcm, &epi));
+    *v->h_clip = 0;
+  }
   std::vector<uint8_t> run(C), flush(C);
   std::vector<std::vector<uint8_t>> run_b(kMaxBlocksPerChunk, std::vector<uint8_t>(C));
   std::vector<std::vector<int>> flush_b(kMaxBlocksPerChunk);
@@ -465,13 +546,21 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         // go through pinned staging that the head kernel reads and writes in
         // place (mapped host memory under unified addressing): no separate
         // host<->device copies per block.
-        if (in_mem == Mem::Host) {
+        if (pcm) {
+          // int16 samples, converted by the head kernel as it loads them
+          int16_t* row = reinterpret_cast<int16_t*>(v->stage_in(v->h_stage, b, c));
+          const int16_t* src = pcm->in[c] + blk * B * pcm->in_step;
+          for (int i = 0; i < B; ++i) row[i] = src[(size_t)i * pcm->in_step];
+          din[c] = v->stage_in(v->h_stage, b, c);
+        } else if (in_mem == Mem::Host) {
           din[c] = in[c] ? v->stage_in(v->h_stage, b, c) : nullptr;
           if (run[c] && in[c]) std::memcpy(v->stage_in(v->h_stage, b, c), in[c] + blk * B, B * sizeof(float));
         } else {
           din[c] = in[c] ? in[c] + blk * B : nullptr;
         }
-        if (out_mem == Mem::Host) {
+        if (pcm) {
+          dout[c] = v->d_mix_scratch + (size_t)c * B;
+        } else if (out_mem == Mem::Host) {
           dout[c] = v->h_out + ((size_t)b * C + c) * B;
         } else {
           dout[c] = out[c] ? out[c] + blk * B : nullptr;
@@ -498,7 +587,9 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         ref.in = v->desc_in(v->d_stage, b);
         ref.out = v->desc_out(v->d_stage, b);
       }
-      TANB_CUDA(counted(v, tanb_convolution::kHead, [&] { return tanb::launch_head(v->ds, ref, cur_b[b], v->stream); }));
+      if (pcm) epi.out16 = reinterpret_cast<int16_t*>(v->h_out + (size_t)b * C * B);  // [ngroups][B] of block b
+      TANB_CUDA(counted(v, tanb_convolution::kHead,
+                        [&] { return tanb::launch_head(v->ds, ref, cur_b[b], v->stream, epi); }));
       const bool last = (b == nb - 1);
       if (last) {
         v->last_desc = dctl;
@@ -523,10 +614,20 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     if (out_mem == Mem::Host) {
       TANB_CUDA(cudaEventSynchronize(v->ev_out));
       if (*v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
-      for (int b = 0; b < nb; ++b)
-        for (int c = 0; c < C; ++c)
-          if (run_b[b][c] && out[c])
-            std::memcpy(out[c] + (processed + b) * B, v->h_out + ((size_t)b * C + c) * B, B * sizeof(float));
+      if (pcm) {
+        for (int b = 0; b < nb; ++b) {
+          const int16_t* st = reinterpret_cast<const int16_t*>(v->h_out + (size_t)b * C * B);
+          for (uint32_t g = 0; g < pcm->ngroups; ++g) {
+            int16_t* dst = pcm->out[g] + (processed + b) * B * pcm->out_step;
+            for (int i = 0; i < B; ++i) dst[(size_t)i * pcm->out_step] = st[(size_t)g * B + i];
+          }
+        }
+      } else {
+        for (int b = 0; b < nb; ++b)
+          for (int c = 0; c < C; ++c)
+            if (run_b[b][c] && out[c])
+              std::memcpy(out[c] + (processed + b) * B, v->h_out + ((size_t)b * C + c) * B, B * sizeof(float));
+      }
     }
     processed += nb;
     if (v->finalize_mode && processed < nblocks && status == TANB_OK) {
@@ -917,6 +1018,40 @@ int32_t tanb_convolution_process_host_to_device(tanb_convolution* v, const float
 int32_t tanb_convolution_process_device(tanb_convolution* v, const float* const* in, float* const* out, size_t n,
                                         const uint32_t* flags, size_t* done) {
   return process_common(v, Mem::Device, in, Mem::Device, out, n, flags, done);
+}
+
+int32_t tanb_convolution_process_mix_pcm16(tanb_convolution* v, const int16_t* const* in, size_t in_step,
+                                           float in_gain, const uint32_t* group, uint32_t ngroups,
+                                           int16_t* const* out, size_t out_step, float out_gain, size_t n,
+                                           int32_t* clipped, size_t* done) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  if (done) *done = 0;
+  if (clipped) *clipped = 0;
+  if (!in || !out || !group) return fail(TANB_INVALID_ARG, "null buffer or group map");
+  if (!(in_gain > 0) || !(out_gain > 0)) return fail(TANB_INVALID_ARG, "conversion gains must be > 0");
+  int C = 0;
+  {
+    std::lock_guard<std::mutex> lock(v->mu);
+    if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "Process before Init");
+    if (v->td) return fail(TANB_NOT_SUPPORTED, "the fused PCM pipeline runs the partitioned methods");
+    C = v->C;
+  }
+  if (ngroups == 0 || ngroups > (uint32_t)C) return fail(TANB_INVALID_ARG, "ngroups must be in [1, channels]");
+  std::vector<int> members(ngroups, 0);
+  for (int c = 0; c < C; ++c) {
+    if (!in[c]) return fail(TANB_INVALID_ARG, "input row %d == NULL", c);
+    if (group[c] >= ngroups) return fail(TANB_INVALID_ARG, "group[%d] = %u out of range", c, group[c]);
+    members[group[c]] += 1;
+  }
+  for (uint32_t g = 0; g < ngroups; ++g) {
+    if (!out[g]) return fail(TANB_INVALID_ARG, "output row %u == NULL", g);
+    if (!members[g]) return fail(TANB_INVALID_ARG, "output group %u has no channel", g);
+  }
+  const PcmIO pcm{in, in_step, in_gain, group, ngroups, out, out_step, out_gain};
+  const int32_t r = process_common(v, Mem::Host, reinterpret_cast<const float* const*>(in), Mem::Host,
+                                   reinterpret_cast<float* const*>(out), n, nullptr, done, &pcm);
+  if (r == TANB_OK && clipped) *clipped = (v->h_clip && *v->h_clip) ? 1 : 0;
+  return r;
 }
 
 int32_t tanb_convolution_process_direct(tanb_convolution* v, const float* const* ir, const float* const* in,

@@ -84,6 +84,25 @@ struct BlockRef {
   float* const* out = nullptr;
 };
 
+// Fused PCM pipeline in the head kernel (tanb_convolution_process_mix_pcm16).
+// Inputs are int16 rows converted with in_scale (the host short->float
+// converter's rule); each channel's output row (the descriptor's out: device
+// scratch) is mixed into its group by the last head CTA of that group to finish
+// (sum from 0 in ascending channel order, the device mixer's rule) and converted
+// to int16 with out_scale (the device float->short rule) into out16 + g * B.
+struct MixEpi {
+  int active = 0;
+  float in_scale = 0.f;            // gain / 32767
+  float out_scale = 0.f;           // 32767 * gain
+  const int* chan_group = nullptr; // [C]
+  const int* gstart = nullptr;     // [ngroups + 1] into gchan
+  const int* gchan = nullptr;      // [C] channels of each group, ascending
+  unsigned* count = nullptr;       // [ngroups] head CTAs of the group done this block
+  const float* scratch = nullptr;  // [C][B] channel outputs
+  int16_t* out16 = nullptr;        // [ngroups][B]
+  int* clip = nullptr;             // set when a sample was clamped
+};
+
 // Where the IR-spectrum kernel reads row j (the IR of channel chans[j]):
 // ptrs[j] when ptrs (a device array) is set, else base + j * stride. Samples
 // at and after n read as zero, so rows need no padding to P*B.
@@ -103,7 +122,8 @@ cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* c
 // delay-line slot `cur`, multiply with partition 0, add the precomputed tail,
 // inverse FFT, overlap-save output (and the crossfade on swap channels).
 // `in[c]` / `out[c]` are device pointers to channel c's B input / output samples.
-cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st);
+cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st,
+                        const MixEpi& epi = MixEpi{});
 
 // Tail multiply-accumulate for the block after the one whose spectrum sits in
 // delay-line slot `cur`:

@@ -104,9 +104,39 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   }
 }
 
+// Fused PCM epilogue (MixEpi): the channel's output row is in epi.scratch; the
+// last head CTA of the channel's group sums the group's rows and converts.
+// The counter is an atomic taken once per CTA after a fence: no CTA waits.
+template <int M, int T>
+__device__ __forceinline__ void mix_epilogue(const MixEpi& epi, int c) {
+  __shared__ int last;
+  const int g = epi.chan_group[c];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned members = (unsigned)(epi.gstart[g + 1] - epi.gstart[g]);
+    last = (atomicAdd(epi.count + g, 1u) == members - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  bool clip = false;
+  for (int i = threadIdx.x; i < M; i += T) {
+    float sum = 0.f;
+    for (int j = epi.gstart[g]; j < epi.gstart[g + 1]; ++j)
+      sum = __fadd_rn(sum, __ldcg(epi.scratch + (size_t)epi.gchan[j] * M + i));
+    float f = __fmul_rn(sum, epi.out_scale);
+    if (f > 32767.f) { f = 32767.f; clip = true; }
+    if (f < -32768.f) { f = -32768.f; clip = true; }
+    epi.out16[(size_t)g * M + i] = (int16_t)((f != f) ? 0 : __float2int_rz(f));
+  }
+  if (clip) atomicOr(epi.clip, 1);
+  if (threadIdx.x == 0) epi.count[g] = 0u;  // every member has counted itself
+}
+
 template <int LOG2M, class D>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T)
-    head_kernel(DevState s, const __grid_constant__ D desc, int cur) {
+    head_kernel(DevState s, const __grid_constant__ D desc, int cur, MixEpi epi) {
   using S = FftShape<LOG2M>;
   constexpr int M = S::M, T = S::T, KP = S::KP;
   extern __shared__ float2 sm[];
@@ -152,11 +182,15 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   // frame [x_{k-1}, x_k] packed as complex pairs; 8-byte loads where the
   // caller's row allows (rows in pinned host staging are read over the bus)
   const bool x_vec = x && (reinterpret_cast<uintptr_t>(x) & 7) == 0;
+  const int16_t* x16 = epi.active ? reinterpret_cast<const int16_t*>(x) : nullptr;
   for (int n = threadIdx.x; n < M; n += T) {
     if (n < M / 2) {
       z[n] = reinterpret_cast<const float2*>(prev)[n];
     } else if (!x) {
       z[n] = make_float2(0.f, 0.f);
+    } else if (x16) {
+      const int k = 2 * (n - M / 2);
+      z[n] = make_float2(__fmul_rn((float)x16[k], epi.in_scale), __fmul_rn((float)x16[k + 1], epi.in_scale));
     } else if (x_vec) {
       z[n] = reinterpret_cast<const float2*>(x)[n - M / 2];
     } else {
@@ -224,6 +258,7 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
       y[i + 1] = o.y;
     }
   }
+  if (epi.active) mix_epilogue<M, T>(epi, c);
 }
 
 // One float4 = two packed bins. u == 0 holds the packed (DC, Nyquist) pair.
@@ -447,13 +482,13 @@ cudaError_t launch_ir_t(const DevState& s, const IrRows& ir, const int* chans, i
 }
 
 template <int LOG2M>
-cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, cudaStream_t st) {
+cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, cudaStream_t st, const MixEpi& epi) {
   using S = FftShape<LOG2M>;
   const size_t smem = (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2);
   if (d.param)
-    head_kernel<LOG2M, ParDesc><<<s.C, S::T, smem, st>>>(s, ParDesc{*d.param}, cur);
+    head_kernel<LOG2M, ParDesc><<<s.C, S::T, smem, st>>>(s, ParDesc{*d.param}, cur, epi);
   else
-    head_kernel<LOG2M, DevDesc><<<s.C, S::T, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, cur);
+    head_kernel<LOG2M, DevDesc><<<s.C, S::T, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, cur, epi);
   return cudaGetLastError();
 }
 
@@ -546,8 +581,8 @@ cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* c
   TANB_DISPATCH_LOG2(s.log2B, launch_ir_t, s, ir, chans, nch, ctl, st);
 }
 
-cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st) {
-  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, d, cur, st);
+cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st, const MixEpi& epi) {
+  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, d, cur, st, epi);
 }
 
 cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, MacTiling t,
