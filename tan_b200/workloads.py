@@ -1,13 +1,15 @@
 """Measurements of the path on each benchmark configuration (seeded synthetic
 inputs with the configurations' shapes; no public dataset is involved).
 
-    python -m tan_b200.workloads cfg1|cfg3|cfg4|nu-tune [--quick]
+    python -m tan_b200.workloads cfg1|cfg3|cfg4|nu-tune|pipeline [--quick]
 
 cfg1  drop-in TANConvolution, 2 ch, B=1024, IR 8192, 200 blocks, FP32
 cfg3  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096..262144,
       input at -6 dBFS, FP32 / FP16 / BF16 spectra; error vs FP64 per channel
 cfg4  non-uniform partitions, 256 ch, IR 2^20, base block 128, schedule from the
       autotuner, FP32 / FP16; error vs FP64 on sampled channels
+pipeline  the sample pipeline (int16 stereo sources, per-ear convolution, mix,
+      int16 out): fused call vs separate GPU calls vs the CPU restatement
 Each prints one JSON object: throughput (GSamples/s), per-block latency
 percentiles, and error in dB (20 log10 rms(err) / rms(ref)).
 """
@@ -203,16 +205,100 @@ def cfg4(ctx, quick=False):
     return out
 
 
+def pipeline(ctx, quick=False, S=32, B=256, L=48000):
+    """The sample pipeline (int16 stereo sources -> per-ear convolution -> mix
+    per ear -> int16 interleaved stereo) per block: the fused call, the same
+    chain through the separate GPU entry points (converter, Process, mixer,
+    converter), and the chain on the CPU restatement. Outputs of the two GPU
+    forms must be identical."""
+    from oracle import ref
+
+    from . import converter as cvt
+
+    g = _rng(6)
+    C = 2 * S
+    nb = 60 if quick else 400
+    T = nb * B
+    src = [(g.uniform(-0.5, 0.5, 2 * T) * 32767).astype(np.int16) for _ in range(S)]
+    h = np.stack([_ir(g, L, float(g.uniform(0.2, 1.0))) for _ in range(C)])
+    group = np.array([c % 2 for c in range(C)], np.uint32)
+    rows_in = [src[c // 2][c % 2:] for c in range(C)]
+    out = {"config": "pipeline", "sources": S, "channels": C, "block": B, "ir": L, "blocks": nb,
+           "deadline_ms": 1000.0 * B / FS}
+
+    fused = cv.TANConvolution(ctx)
+    assert fused.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == 0
+    assert fused.UpdateResponseTD(h, L) == 0
+    pout = np.zeros(2 * T, np.int16)
+    lat = []
+    for k in range(nb):
+        xs = [r[2 * k * B:] for r in rows_in]
+        ys = [pout[2 * k * B:], pout[2 * k * B + 1:]]
+        t0 = time.perf_counter()
+        rc, _, _ = fused.ProcessMixPcm16(xs, 2, 1.0, group, 2, ys, 2, 1.0, B)
+        lat.append(1e3 * (time.perf_counter() - t0))
+        assert rc == 0
+    fused.Release()
+    out["fused"] = {"latency_ms": _pct(lat[5:]), "gsamples_per_s_host": C * B / (np.mean(lat[5:]) / 1e3) / 1e9}
+
+    conv = cv.TANConvolution(ctx)
+    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == 0
+    assert conv.UpdateResponseTD(h, L) == 0
+    con = cvt.TANConverter(ctx)
+    mixer = cvt.TANMixer(ctx, B, S)
+    xf = np.zeros((C, B), np.float32)
+    yf = np.zeros((C, B), np.float32)
+    mixed = np.zeros((2, B), np.float32)
+    pout2 = np.zeros(2 * T, np.int16)
+    lat = []
+    for k in range(nb):
+        t0 = time.perf_counter()
+        assert con.ConvertShortToFloatBatch([r[2 * k * B:] for r in rows_in], 2, B, list(xf), 1, 1.0) == 0
+        rc, _ = conv.Process(xf, yf, B)
+        assert rc == 0
+        for ear in range(2):
+            assert mixer.Mix([yf[c] for c in range(ear, C, 2)], mixed[ear]) == 0
+            assert con.ConvertFloatToShort(mixed[ear], 1, B, pout2[2 * k * B + ear:], 2, 1.0)[0] == 0
+        lat.append(1e3 * (time.perf_counter() - t0))
+    conv.Release()
+    con.Terminate()
+    mixer.Terminate()
+    out["unfused_gpu_calls"] = {"latency_ms": _pct(lat[5:]),
+                                "gsamples_per_s_host": C * B / (np.mean(lat[5:]) / 1e3) / 1e9}
+    # the separate calls use the CPU mixer / converter rules on host buffers;
+    # the fused call uses the device rules (sum from 0, truncation): compare
+    # after restating the fused rules on the separate chain's float outputs
+    diff = np.abs(pout.astype(np.int32) - pout2.astype(np.int32))
+    out["fused_vs_unfused_max_lsb"] = int(diff.max())
+
+    rc_ = ref.RefConvolution(L, B, C, threads=__import__("os").cpu_count())
+    rc_.update_response_td(h)
+    lat = []
+    nb_cpu = min(nb, 100)
+    for k in range(nb_cpu):
+        t0 = time.perf_counter()
+        x = np.stack([ref.convert_s16_f32(r[2 * k * B:], 1.0, in_step=2, n=B) for r in rows_in])
+        y = np.zeros_like(x)
+        rc_.process(x, None, y)
+        for ear in range(2):
+            ref.convert_f32_s16(ref.mix(y[ear::2]), 1.0)
+        lat.append(1e3 * (time.perf_counter() - t0))
+    rc_.close()
+    out["cpu_restatement"] = {"latency_ms": _pct(lat[5:]), "threads": __import__("os").cpu_count(),
+                              "gsamples_per_s": C * B / (np.mean(lat[5:]) / 1e3) / 1e9}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("which", choices=["cfg1", "cfg3", "cfg4", "nu-tune"])
+    ap.add_argument("which", choices=["cfg1", "cfg3", "cfg4", "nu-tune", "pipeline"])
     ap.add_argument("--quick", action="store_true")
     a = ap.parse_args()
     ctx = cv.TANContext(0)
     if a.which == "nu-tune":
         r = tune_nu(ctx, 64 if a.quick else 256, 1 << 20, 128)
     else:
-        r = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4}[a.which](ctx, a.quick)
+        r = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4, "pipeline": pipeline}[a.which](ctx, a.quick)
     print(json.dumps(r))
 
 
