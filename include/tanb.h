@@ -380,6 +380,45 @@ int32_t tanb_mixer_synchronize(tanb_mixer* mixer);
 void* tanb_mixer_stream(tanb_mixer* mixer);
 
 /* ---------------------------------------------------------------------------
+ * GPU-resident IR producer: left / right impulse responses of a shoebox room
+ * written into device memory, ready for tanb_convolution_update_response_td_device
+ * (the GPU path of TrueAudioVR::generateRoomResponse with GENROOM_USE_GPU_MEM,
+ * samples/src/TrueAudioVR/TrueAudioVR.h:153-155, TrueAudioVR.cpp:659-786;
+ * kernels Kernels/GenerateRoomResponse.cl:206-321, Kernels/Fill.cl).
+ * ------------------------------------------------------------------------- */
+typedef struct {                 /* RoomDefinition (TrueAudioVR.h:101-106), meters */
+  float width, height, length;
+  float damp_left, damp_right, damp_top, damp_bottom, damp_front, damp_back; /* (0, 1] */
+} tanb_room;
+typedef struct {                 /* MonoSource (TrueAudioVR.h:69-72) */
+  float x, y, z;
+} tanb_source;
+typedef struct {                 /* StereoListener + HeadModel (TrueAudioVR.h:62-81) */
+  float head_x, head_y, head_z, ear_spacing;
+  float yaw, pitch, roll;        /* degrees */
+  int32_t filter_length;         /* <= 64 */
+  float low_pass[64], high_pass[64];
+} tanb_listener;
+enum { TANB_GENROOM_LIMIT_BOUNCES = 0x40 }; /* TrueAudioVR.h:55 */
+
+typedef struct tanb_room_generator tanb_room_generator;
+/* Workspace for responses of up to max_length samples. */
+int32_t tanb_room_generator_create(tanb_context* ctx, int32_t max_length, tanb_room_generator** generator);
+int32_t tanb_room_generator_release(tanb_room_generator* generator);
+/* Writes `length` samples of the left and right responses to the device
+ * buffers `left` / `right`, asynchronously on `stream` (a cudaStream_t; null:
+ * the generator's stream), after any earlier call of this generator. With
+ * TANB_GENROOM_LIMIT_BOUNCES at most max_bounces images per axis and side.
+ * Results are reproducible bit for bit (exact 64-bit fixed-point sums). */
+int32_t tanb_room_response(tanb_room_generator* generator, const tanb_room* room, const tanb_source* source,
+                           const tanb_listener* ears, int32_t sample_rate, int32_t length, float* left,
+                           float* right, uint32_t flags, int32_t max_bounces, void* stream);
+/* Image sources per ear of the last call. */
+int64_t tanb_room_images(tanb_room_generator* generator);
+int32_t tanb_room_generator_synchronize(tanb_room_generator* generator);
+void* tanb_room_generator_stream(tanb_room_generator* generator);
+
+/* ---------------------------------------------------------------------------
  * Non-uniformly partitioned convolution: the TAN_CONVOLUTION_METHOD_*_NONUNIFORM
  * family (CPU variant ConvolutionImpl.cpp:224-246, 2416-2428; GPU two-stream
  * engine tan/tanlibrary/src/Graal2/Reverberate.cpp), with a level schedule of

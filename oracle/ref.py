@@ -62,6 +62,8 @@ def lib() -> ctypes.CDLL:
         L.tanref_mix.restype = None
         L.tanref_mix_dev.argtypes = [fp, sz, i32, sz, fp]
         L.tanref_mix_dev.restype = None
+        L.tanref_room_response.argtypes = [fp, fp, fp, i32, i32, i32, fp, fp, i32, i32, fp, fp]
+        L.tanref_room_response.restype = ctypes.c_long
         L.tanref_irfft.argtypes = [i32, fp, fp, fp]
         _lib = L
     return _lib
@@ -216,3 +218,40 @@ def mix(x: np.ndarray, device: bool = False) -> np.ndarray:
     else:
         lib().tanref_mix(_ptrs([x[c] for c in range(C)]), C, n, py)
     return y
+
+
+# --- Room response producer restatement -----------------------------------------
+
+
+def room_response(room, source, ears, rate: int, length: int, low_pass, high_pass, flags: int = 0,
+                  max_bounces: int = 0):
+    """Left / right IRs of a shoebox room (the GPU path of
+    TrueAudioVR::generateRoomResponse). room: (width, height, length, damp left,
+    right, top, bottom, front, back); source: (x, y, z); ears: (head x, y, z,
+    ear spacing, yaw, pitch, roll). Returns (left, right, images per ear)."""
+    fp = ctypes.POINTER(ctypes.c_float)
+    r = np.ascontiguousarray(room, np.float32)
+    s = np.ascontiguousarray(source, np.float32)
+    e = np.ascontiguousarray(ears, np.float32)
+    lp = np.ascontiguousarray(low_pass, np.float32)
+    hp = np.ascontiguousarray(high_pass, np.float32)
+    left = np.zeros(length, np.float32)
+    right = np.zeros(length, np.float32)
+    n = lib().tanref_room_response(r.ctypes.data_as(fp), s.ctypes.data_as(fp), e.ctypes.data_as(fp), rate, length,
+                                   lp.size, lp.ctypes.data_as(fp), hp.ctypes.data_as(fp), flags, max_bounces,
+                                   left.ctypes.data_as(fp), right.ctypes.data_as(fp))
+    return left, right, int(n)
+
+
+def simple_head_filters(ear_spacing: float = 0.16, n: int = 64, rate: int = 48000):
+    """The head-shadow low-pass / complementary high-pass pair of
+    TrueAudioVR::generateSimpleHeadRelatedTransform (TrueAudioVR.cpp:361-411),
+    with numpy's FFT in place of TAN's: a test input for the room producer."""
+    corner = np.float32(343.0 / (1.10 * ear_spacing))
+    f = np.array([(j // 2) / (n * (1.0 / rate)) for j in range(n)], np.float32)
+    d = corner / (corner + f)
+    spec = np.fft.fft(np.eye(1, n, 0)[0]) * d
+    low = np.real(np.fft.ifft(spec)).astype(np.float32)
+    high = -low
+    high[0] += 1.0
+    return low, high.astype(np.float32)

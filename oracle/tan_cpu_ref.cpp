@@ -45,6 +45,7 @@
 #include <immintrin.h>
 #include <omp.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -560,6 +561,130 @@ void tanref_convert_f32_s16_dev(const float* in, size_t in_step, size_t n, int16
     out[i * out_step] = (f != f) ? 0 : (int16_t)f;
   }
   if (clipped) *clipped = clip ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Room response producer: the GPU path of TrueAudioVR::generateRoomResponse
+// (samples/src/TrueAudioVR/TrueAudioVR.cpp:659-786 with GENROOM_USE_GPU_MEM;
+// kernels Kernels/GenerateRoomResponse.cl:206-321 and Kernels/Fill.cl).
+// Differences from the reference, all deliberate: damp^k for the integer wall
+// counts k by repeated multiplication (the kernel's native_powr is
+// implementation-defined), sqrt correctly rounded (native_sqrt), sums in 64
+// bits (the kernel's int32 can wrap) converted as signed (Fill.cl converts
+// them as unsigned, which turns negative sums into large positive values).
+// ---------------------------------------------------------------------------
+static float pow_int(float b, int k) {
+  float r = 1.0f;
+  for (int i = 0; i < k; ++i) r = r * b;
+  return r;
+}
+
+// One ear: the kernel's per-image work over its grid. Returns the image count.
+static long room_ear(const float* room, const float* src, float hx, float hy, float hz, float evx, float evy, float evz,
+                     float earV, float maxGain, float dMin, int rate, int length, int hrtfLength, int filterLength,
+                     const float* lpF, const float* hpF, int numRefX, int numRefY, int numRefZ, int64_t* acc) {
+  const float W = room[0], H = room[1], L = room[2];
+  const float dRight = room[4], dLeft = room[3], dTop = room[5], dBottom = room[6], dFront = room[7],
+              dBack = room[8];
+  const float kF2I = 67108864.0f;
+  auto up4 = [](int n) { return (n % 4) ? n + 4 - n % 4 : n; };  // the NDRange rounding (local size 4)
+  const int gx = up4(numRefX), gy = up4(numRefY), gz = up4(numRefZ);
+  long images = 0;
+  for (int z = 0; z < gz && z <= numRefZ; ++z)
+    for (int y = 0; y < gy && y <= numRefY; ++y)
+      for (int x = 0; x < gx && x <= numRefX; ++x) {
+        ++images;
+        const int ix = x - numRefX / 2, iy = y - numRefY / 2, iz = z - numRefZ / 2;
+        float a = (ix % 2 == 0) ? (float)ix : (float)(ix + 1);
+        float b = (ix % 2 == 0) ? 1.0f : -1.0f;
+        const float rx = a * W + b * src[0];
+        a = (iy % 2 == 0) ? (float)iy : (float)(iy + 1);
+        b = (iy % 2 == 0) ? 1.0f : -1.0f;
+        const float ry = a * H + b * src[1];
+        a = (iz % 2 == 0) ? (float)iz : (float)(iz + 1);
+        b = (iz % 2 == 0) ? 1.0f : -1.0f;
+        const float rz = a * L + b * src[2];
+        const int kxl = ix > 0 ? ix / 2 : std::abs(ix - 1) / 2, kyb = iy > 0 ? iy / 2 : std::abs(iy - 1) / 2,
+                  kzb = iz > 0 ? iz / 2 : std::abs(iz - 1) / 2;
+        const int kxr = ix > 0 ? (ix + 1) / 2 : std::abs(ix) / 2, kyt = iy > 0 ? (iy + 1) / 2 : std::abs(iy) / 2,
+                  kzf = iz > 0 ? (iz + 1) / 2 : std::abs(iz) / 2;
+        float amp = pow_int(dRight, kxr);
+        amp = amp * pow_int(dLeft, kxl);
+        amp = amp * pow_int(dTop, kyt);
+        amp = amp * pow_int(dBottom, kyb);
+        amp = amp * pow_int(dFront, kzf);
+        amp = amp * pow_int(dBack, kzb);
+        const float dx = rx - hx, dy = ry - hy, dz = rz - hz;
+        const float d = std::sqrt(dx * dx + dy * dy + dz * dz);
+        const int fi = 1 + (int)((d / 340.0f) * (float)rate);
+        if (fi >= length) continue;
+        const float dr = (d <= dMin) ? maxGain : maxGain * dMin / d;
+        const int len = std::min(filterLength, length - fi);
+        const float dp = evx * dx + evy * dy + evz * dz;
+        const float cosA = dp / (earV * d);
+        const float hf = (cosA + 1.0f) / 2.0f;
+        if (fi < hrtfLength) {
+          for (int i = 0; i < len; ++i) acc[fi + i] += (int64_t)(int32_t)(kF2I * amp * dr * (lpF[i] + hf * hpF[i]));
+        } else {
+          acc[fi] += (int64_t)(int32_t)(kF2I * amp * dr);
+        }
+      }
+  return images;
+}
+
+// room[9]: width, height, length, damp left, right, top, bottom, front, back.
+// src[3]; ears[7]: head x, y, z, ear spacing, yaw, pitch, roll (degrees).
+// Returns the number of images per ear (-1: invalid room).
+long tanref_room_response(const float* room_in, const float* src_in, const float* ears, int rate, int length,
+                          int filterLength, const float* lowPass, const float* highPass, int flags, int maxBounces,
+                          float* left, float* right) {
+  float room[9];
+  std::memcpy(room, room_in, sizeof(room));
+  float src[3] = {src_in[0], src_in[1], src_in[2]};
+  // TrueAudioVR.cpp:663-668: source clamped into the room
+  src[0] = std::min(std::max(src[0], 0.0f), room[0]);
+  src[1] = std::min(std::max(src[1], 0.0f), room[1]);
+  src[2] = std::min(std::max(src[2], 0.0f), room[2]);
+  // :670-689 ear offsets and orientation vectors, rotated by yaw / pitch / roll
+  const float es = ears[3];
+  // left / right ear offsets, then left / right ear vectors (earVzL = -earDxL, earVzR = earDxR)
+  float e[4][3] = {{es / 2, 0.0f, 0.0f}, {-es / 2, 0.0f, 0.0f}, {es / 2, 0.0f, -(es / 2)}, {-es / 2, 0.0f, -es / 2}};
+  const float pi = (float)3.141592653589793;
+  const float sY = std::sin(ears[4] * pi / 180), cY = std::cos(ears[4] * pi / 180);
+  const float sP = std::sin(ears[5] * pi / 180), cP = std::cos(ears[5] * pi / 180);
+  const float sR = std::sin(ears[6] * pi / 180), cR = std::cos(ears[6] * pi / 180);
+  const float m[3][3] = {{cR * cY - sR * sP * sY, -sR * cP, cR * sY + sR * sP * cY},
+                         {sR * cY + cR * sP * sY, cR * cP, sR * sY - cR * sP * cY},
+                         {-cP * sY, sP, cP * cY}};
+  for (auto& v : e) {
+    const float x = v[0], y = v[1], z = v[2];
+    v[0] = x * m[0][0] + y * m[0][1] + z * m[0][2];
+    v[1] = x * m[1][0] + y * m[1][1] + z * m[1][2];
+    v[2] = x * m[2][0] + y * m[2][1] + z * m[2][2];
+  }
+  const int nSW = (int)((room[0] / 340.0f) * rate), nSH = (int)((room[1] / 340.0f) * rate),
+            nSL = (int)((room[2] / 340.0f) * rate);
+  if (nSW <= 0 || nSH <= 0 || nSL <= 0) return -1;
+  int nW = 1 + length / nSW, nH = 1 + length / nSH, nL = 1 + length / nSL;
+  if (flags & 0x40) {  // GENROOM_LIMIT_BOUNCES
+    nW = std::min(nW, maxBounces);
+    nH = std::min(nH, maxBounces);
+    nL = std::min(nL, maxBounces);
+  }
+  const int hrtfLength = 2 * (nSW + nSH + nSL);
+  long images = 0;
+  for (int ch = 0; ch < 2; ++ch) {
+    const float* d = e[ch];
+    const float* v = e[2 + ch];
+    const float hx = ears[0] + d[0], hy = ears[1] + d[1], hz = ears[2] + d[2];
+    const float earV = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    std::vector<int64_t> acc(length, 0);
+    images = room_ear(room, src, hx, hy, hz, v[0], v[1], v[2], earV, 2.0f, 2 * es, rate, length, hrtfLength,
+                      filterLength, lowPass, highPass, 2 * nW, 2 * nH, 2 * nL, acc.data());
+    float* out = ch == 0 ? left : right;
+    for (int i = 0; i < length; ++i) out[i] = (float)acc[i] / 67108864.0f;
+  }
+  return images;
 }
 
 // TANMixerImpl::Mix(float**, float*) MixerImpl.cpp:226-250: out = in[0], then

@@ -107,6 +107,12 @@ SIGNATURES = {
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_convolution_process_mix_pcm16": (_i32, [_vp, _pp, _sz, ctypes.c_float, _u32p, _u32, _pp, _sz,
                                                   ctypes.c_float, _sz, ctypes.POINTER(ctypes.c_int32), _szp]),
+    "tanb_room_generator_create": (_i32, [_vp, _i32, ctypes.POINTER(_vp)]),
+    "tanb_room_generator_release": (_i32, [_vp]),
+    "tanb_room_response": (_i32, [_vp, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _u32, _i32, _vp]),
+    "tanb_room_images": (ctypes.c_int64, [_vp]),
+    "tanb_room_generator_synchronize": (_i32, [_vp]),
+    "tanb_room_generator_stream": (_vp, [_vp]),
     "tanb_converter_create": (_i32, [_vp, ctypes.POINTER(_vp)]),
     "tanb_converter_release": (_i32, [_vp]),
     "tanb_converter_short_to_float": (_i32, [_vp, _vp, _sz, _sz, _vp, _sz, ctypes.c_float]),
