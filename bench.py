@@ -266,7 +266,7 @@ def size_floor(torch, stream, flush_l2, nbytes, dev, reps=50):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            torch.sum(buf, dtype=torch.float32, out=out)
+            torch.sum(buf, 0, out=out)
             b.record(stream)
             b.synchronize()
             if r >= 3:

@@ -100,6 +100,7 @@ struct tanb_convolution {
   float* h_out = nullptr;
   const ChanCtl* last_desc = nullptr;  // device descriptor of the last head (for ProcessFinalize)
   int last_cur = 0;
+  int64_t blocks = 0;  // blocks processed: the parity selects the tail row
   // per-block descriptors passed as kernel parameters (C <= kParamChannels)
   std::vector<tanb::ParamDesc> pdesc;
   tanb::ParamDesc last_pdesc{};
@@ -276,20 +277,23 @@ cudaError_t flush_channel(tanb_convolution* v, int c) {
   if ((e = cudaMemsetAsync(v->ds.fdl + (size_t)c * P * B, 0, P * B * sizeof(float2), v->stream)) != cudaSuccess)
     return e;
   if ((e = cudaMemsetAsync(v->ds.prev + (size_t)c * B, 0, B * sizeof(float), v->stream)) != cudaSuccess) return e;
-  return cudaMemsetAsync(v->ds.tail + (size_t)c * 2 * B, 0, 2 * B * sizeof(float2), v->stream);
+  return cudaMemsetAsync(v->ds.tail + (size_t)c * 3 * B, 0, 3 * B * sizeof(float2), v->stream);
 }
 
 int32_t run_pending_finalize(tanb_convolution* v) {
   if (!v->finalize_due) return TANB_OK;
   v->finalize_due = false;
-  if (v->P <= 1) return TANB_OK;
+  if (v->P <= 2) return TANB_OK;  // no partitions beyond the head's two
   tanb::BlockRef ref;
   if (v->last_is_param)
     ref.param = &v->last_pdesc;
   else
     ref.ctl = v->last_desc;
   TANB_CUDA(counted(v, tanb_convolution::kTail,
-                    [&] { return tanb::launch_tail(v->ds, ref, 0, v->last_cur, v->tiling, v->stream); }));
+                    [&] {
+                      return tanb::launch_tail(v->ds, ref, 0, v->last_cur, (int)(v->blocks & 1), v->tiling,
+                                               v->stream);
+                    }));
   return TANB_OK;
 }
 
@@ -373,12 +377,12 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   TANB_CUDA(counted(v, tanb_convolution::kIr,
                     [&] { return tanb::launch_ir_spectrum(v->ds, rows, d_uch, nch, d_uctl, v->stream); }));
   // tail of the pending IR for the next block, from the current delay line
-  if (v->P > 1)
+  if (v->P > 2)
     TANB_CUDA(counted(v, tanb_convolution::kTail,
                       [&] {
                         tanb::BlockRef ref;
                         ref.ctl = d_uctl;
-                        return tanb::launch_tail(v->ds, ref, 1, v->cur, v->tiling, v->stream);
+                        return tanb::launch_tail(v->ds, ref, 1, v->cur, 2, v->tiling, v->stream);
                       }));
   if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) TANB_CUDA(cudaStreamSynchronize(v->stream));
   return TANB_OK;
@@ -588,8 +592,9 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         ref.out = v->desc_out(v->d_stage, b);
       }
       if (pcm) epi.out16 = reinterpret_cast<int16_t*>(v->h_out + (size_t)b * C * B);  // [ngroups][B] of block b
+      const int parity = (int)((v->blocks + b) & 1);
       TANB_CUDA(counted(v, tanb_convolution::kHead,
-                        [&] { return tanb::launch_head(v->ds, ref, cur_b[b], v->stream, epi); }));
+                        [&] { return tanb::launch_head(v->ds, ref, cur_b[b], parity, v->stream, epi); }));
       const bool last = (b == nb - 1);
       if (last) {
         v->last_desc = dctl;
@@ -599,11 +604,12 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       }
       if (last && v->finalize_mode) {
         v->finalize_due = true;
-      } else if (P > 1) {
-        // Directly behind the head (programmatic serialization): the tail
-        // streams partitions 2..P-1 while the head runs.
+      } else if (P > 2) {
+        // Directly behind the head (programmatic serialization): the next
+        // block's partitions >= 2 share no data with this head, so the two run
+        // side by side.
         TANB_CUDA(counted(v, tanb_convolution::kTail, [&] {
-          return tanb::launch_tail(v->ds, ref, 0, cur_b[b], v->tiling, v->stream, true);
+          return tanb::launch_tail(v->ds, ref, 0, cur_b[b], parity ^ 1, v->tiling, v->stream, true);
         }));
       }
     }
@@ -630,6 +636,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       }
     }
     processed += nb;
+    v->blocks += nb;
     if (v->finalize_mode && processed < nblocks && status == TANB_OK) {
       if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
     }
@@ -929,7 +936,7 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
     if ((e = dev_alloc(v, &v->ds.H, Cs * 2 * Ps * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->ds.fdl, Cs * Ps * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->ds.prev, Cs * Bs)) != cudaSuccess) break;
-    if ((e = dev_alloc(v, &v->ds.tail, Cs * 2 * Bs)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->ds.tail, Cs * 3 * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_tw, 2 * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_stage, kMaxBlocksPerChunk * v->desc_bytes)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_ir, Cs * Ps * Bs)) != cudaSuccess) break;
@@ -979,6 +986,7 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
   v->available.assign(C, 0);
   v->flushed.assign(C, 0);
   v->cur = 0;
+  v->blocks = 0;
   v->initialized = true;
   return TANB_OK;
 }

@@ -119,23 +119,25 @@ cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* c
                                const ChanCtl* ctl, cudaStream_t st);
 
 // Head of one block for every running channel: FFT of [prev, x], insert into
-// delay-line slot `cur`, multiply with partition 0, add the precomputed tail,
-// inverse FFT, overlap-save output (and the crossfade on swap channels).
+// delay-line slot `cur`, multiply with partitions 0 and 1 (X_k, X_{k-1}), add
+// the block's tail (row `parity` = block index & 1, and row 2 for a pending IR
+// on swap channels), inverse FFT, overlap-save output (and the crossfade).
 // `in[c]` / `out[c]` are device pointers to channel c's B input / output samples.
-cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st,
+cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, int parity, cudaStream_t st,
                         const MixEpi& epi = MixEpi{});
 
-// Tail multiply-accumulate for the block after the one whose spectrum sits in
-// delay-line slot `cur`:
-//   tail[c][which] = sum_{i=1}^{P-1} FDL[c][(cur + i - 1) mod P] * H[c][slot][i]
-// which = 0: running channels, slot = swap ? slot_new : slot_cur
-// which = 1: channels with swap set (pending IR), slot = slot_new
-// pdl: launch with programmatic stream serialization. Only for a launch that
-// directly follows launch_head of the same block in the stream: the kernel
-// then streams partitions 2..P-1 while the head runs and waits for it before
-// partition 1 and before writing the tail buffer. Any other predecessor may
-// write what partitions >= 2 read, so every other launch passes false.
-cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, MacTiling t,
+// Tail multiply-accumulate, partitions 2..P-1, for the block after the one
+// whose spectrum sits in delay-line slot `cur`:
+//   tail[c][trow] = sum_{i=2}^{P-1} FDL[c][(cur + i - 1) mod P] * H[c][slot][i]
+// which = 0: running channels, slot = swap ? slot_new : slot_cur, trow = the
+//            next block's parity
+// which = 1: channels with swap set (pending IR), slot = slot_new, trow = 2;
+//            `cur` is then the newest slot before the coming block
+// It reads only X_{k-1} and older and writes a row the head of block k does not
+// read, so it shares no data with that head. pdl: launch with programmatic
+// stream serialization, directly behind the head of the same block (the two
+// then run side by side); every other launch passes false.
+cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, int trow, MacTiling t,
                         cudaStream_t st, bool pdl = false);
 
 // Per-channel descriptor of one TIME_DOMAIN call.

@@ -27,12 +27,12 @@ namespace {
 // Programmatic dependent launch (sm_90+): a kernel launched with
 // cudaLaunchAttributeProgrammaticStreamSerialization may begin once every CTA
 // of the kernel before it in the stream has executed launch_dependents (or
-// exited); griddepcontrol.wait then blocks until that kernel has completed and
-// its memory operations are visible. Without the attribute both are no-ops.
+// exited). The head triggers at once; the tail launched behind it shares no
+// data with it, so it never has to wait for the head grid. Without the
+// attribute this is a no-op.
 __device__ __forceinline__ void griddep_launch_dependents() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
-__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Launch of `kernel`, with programmatic stream serialization when `pdl` is set.
 template <class... KArgs, class... Args>
@@ -136,14 +136,14 @@ __device__ __forceinline__ void mix_epilogue(const MixEpi& epi, int c) {
 
 template <int LOG2M, class D>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T)
-    head_kernel(DevState s, const __grid_constant__ D desc, int cur, MixEpi epi) {
+    head_kernel(DevState s, const __grid_constant__ D desc, int cur, int parity, MixEpi epi) {
   using S = FftShape<LOG2M>;
   constexpr int M = S::M, T = S::T, KP = S::KP;
   extern __shared__ float2 sm[];
   float2* z = sm;       // old / only IR
   float2* z2 = sm + M;  // new IR on a swap block
-  // The tail launched behind this kernel may start now: it reads nothing this
-  // kernel writes until its grid-dependency wait.
+  // The tail launched behind this kernel (the next block's partitions >= 2)
+  // shares no data with it and may start at once.
   griddep_launch_dependents();
   const int c = blockIdx.x;
   const ChanCtl cc = desc.get_ctl(c);
@@ -154,8 +154,12 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   float* prev = s.prev + (size_t)c * M;
   const float2* h0 = s.H + h_index(s, c, cc.slot_cur, 0);
   const float2* h1 = s.H + h_index(s, c, cc.slot_new, 0);
-  const float2* t0 = s.tail + (size_t)c * 2 * M;
-  const float2* t1 = t0 + M;
+  // tails of this block (partitions >= 2): the IR in use, by block parity, and
+  // a pending IR's; partition 1 multiplies X_{k-1}, in the next delay-line slot
+  const float2* t0 = s.tail + ((size_t)c * 3 + parity) * M;
+  const float2* t1 = s.tail + ((size_t)c * 3 + 2) * M;
+  const bool p1 = s.P > 1;
+  const float2* xp = s.fdl + ((size_t)c * s.P + (cur + 1) % s.P) * M;
 
   // twiddles into shared memory (small transforms), coalesced float4 loads
   const float2* tw = s.tw;
@@ -175,6 +179,10 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
       const int km = (k == 0) ? 0 : M - k;
       pt[q][0] = t0[k];
       pt[q][1] = t0[km];
+      if (p1) {
+        pt[q][0] = (k == 0) ? c_mac_dc(pt[q][0], xp[0], h0[M]) : c_mac(pt[q][0], xp[k], h0[M + k]);
+        if (k != 0) pt[q][1] = c_mac(pt[q][1], xp[km], h0[M + km]);
+      }
       ph[q][0] = h0[k];
       ph[q][1] = h0[km];
     }
@@ -213,7 +221,10 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
       const float2 X = rfft_post_dc(z[0]);
       F[0] = X;
       z[0] = irfft_pre_dc(c_mac_dc(pt[q][0], X, ph[q][0]), inv_n);
-      if (swap) z2[0] = irfft_pre_dc(c_mac_dc(t1[0], X, h1[0]), inv_n);
+      if (swap) {
+        const float2 u = p1 ? c_mac_dc(t1[0], xp[0], h1[M]) : t1[0];
+        z2[0] = irfft_pre_dc(c_mac_dc(u, X, h1[0]), inv_n);
+      }
     } else {
       const int km = M - k;
       const float2 wk = tw[k], wm = tw[km];
@@ -227,8 +238,10 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
       z[k] = irfft_pre(Ak, Am, wk, inv_n);
       if (km != k) z[km] = irfft_pre(Am, Ak, wm, inv_n);
       if (swap) {
-        const float2 Bk = c_mac(t1[k], Xk, h1[k]);
-        const float2 Bm = c_mac(t1[km], Xm, h1[km]);
+        const float2 uk = p1 ? c_mac(t1[k], xp[k], h1[M + k]) : t1[k];
+        const float2 um = p1 ? c_mac(t1[km], xp[km], h1[M + km]) : t1[km];
+        const float2 Bk = c_mac(uk, Xk, h1[k]);
+        const float2 Bm = c_mac(um, Xm, h1[km]);
         z2[k] = irfft_pre(Bk, Bm, wk, inv_n);
         if (km != k) z2[km] = irfft_pre(Bm, Bk, wm, inv_n);
       }
@@ -271,7 +284,7 @@ __device__ __forceinline__ float4 mac4(float4 acc, float4 f, float4 h, bool dc) 
 
 template <int UX, int SY, int D, class DS>
 __global__ void __launch_bounds__(UX* SY)
-    tail_kernel(DevState s, const __grid_constant__ DS desc, int which, int cur) {
+    tail_kernel(DevState s, const __grid_constant__ DS desc, int which, int cur, int trow) {
   const int c = blockIdx.y;
   const ChanCtl cc = desc.get_ctl(c);
   if (which == 0 ? !cc.run : !cc.swap) return;
@@ -281,18 +294,16 @@ __global__ void __launch_bounds__(UX* SY)
   const int u = blockIdx.x * UX + tx;
   const int P = s.P;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  const bool act = u < U && P > 1;
+  const bool act = u < U && P > 2;
   const float4* Hc = reinterpret_cast<const float4*>(s.H + h_index(s, c, slot, 0)) + u;
   const float4* Fc = reinterpret_cast<const float4*>(s.fdl + (size_t)c * P * s.B) + u;
   const bool dc = (u == 0);
   if (act) {
-    const int nparts = P - 1;
+    const int nparts = P - 2;  // partitions 2 .. P-1
     const int chunk = (nparts + SY - 1) / SY;
-    const int i0 = 1 + ty * chunk;
+    const int i0 = 2 + ty * chunk;
     const int i1 = min(P, i0 + chunk);
-    // Partition 1 multiplies the spectrum the preceding head kernel inserts
-    // into slot `cur`; row ty == 0 adds it after the grid-dependency wait.
-    int i = (i0 == 1) ? 2 : i0;
+    int i = i0;
     int fs = (cur + i - 1) % P;
     for (; i + D <= i1; i += D) {
       float4 h[D], f[D];
@@ -312,11 +323,6 @@ __global__ void __launch_bounds__(UX* SY)
       acc = mac4(acc, f, h, dc);
     }
   }
-  // Waits for the head kernel of this block when launched behind it with
-  // programmatic serialization (returns at once otherwise): after this, its
-  // delay-line write is visible and its read of the tail buffer is done.
-  griddep_wait();
-  if (act && ty == 0) acc = mac4(acc, Fc[(size_t)cur * U], __ldg(Hc + (size_t)U), dc);
   if constexpr (SY > 1) {
     __shared__ float4 red[SY][UX];
     red[ty][tx] = acc;
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(UX* SY)
       acc.w += r.w;
     }
   }
-  if (u < U) reinterpret_cast<float4*>(s.tail + ((size_t)c * 2 + which) * s.B)[u] = acc;
+  if (u < U) reinterpret_cast<float4*>(s.tail + ((size_t)c * 3 + trow) * s.B)[u] = acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -380,7 +386,7 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 
 template <int BR, int RS, int NS, class DS>
 __global__ void __launch_bounds__(BR / 2)
-    tail_bulk_kernel(DevState s, const __grid_constant__ DS desc, int which, int cur) {
+    tail_bulk_kernel(DevState s, const __grid_constant__ DS desc, int which, int cur, int trow) {
   constexpr int U = BR / 2;                     // threads = float4 units of the slice
   constexpr uint32_t kRowBytes = BR * sizeof(float2);
   extern __shared__ __align__(128) unsigned char bulk_smem[];
@@ -390,19 +396,18 @@ __global__ void __launch_bounds__(BR / 2)
   const int c = blockIdx.y;
   const ChanCtl cc = desc.get_ctl(c);
   if (which == 0 ? !cc.run : !cc.swap) return;
-  griddep_wait();  // its first chunk holds partition 1 (see tail_kernel)
   const int slot = (which == 0) ? (cc.swap ? cc.slot_new : cc.slot_cur) : cc.slot_new;
   const int P = s.P;
   const int bin0 = blockIdx.x * BR;
   const int tid = threadIdx.x;
-  const int nparts = P - 1;
+  const int nparts = P - 2;  // partitions 2 .. P-1
   const int nchunks = (nparts + RS - 1) / RS;
   const float2* Hrow = s.H + h_index(s, c, slot, 0) + bin0;  // + i * B for partition i
   const float2* Frow = s.fdl + (size_t)c * P * s.B + bin0;    // + slot * B
 
   auto issue = [&](int q) {  // chunk q -> stage q % NS (thread 0 only)
     const int st = q % NS;
-    const int i0 = 1 + q * RS;
+    const int i0 = 2 + q * RS;
     const int rows = min(RS, P - i0);
     const uint32_t bar = smem_addr(&bars[st]);
     mbar_expect_tx(bar, 2u * rows * kRowBytes);
@@ -434,7 +439,7 @@ __global__ void __launch_bounds__(BR / 2)
       ok = false;
       break;
     }
-    const int rows = min(RS, P - (1 + q * RS));
+    const int rows = min(RS, P - (2 + q * RS));
     for (int r = 0; r < rows; ++r)
       acc = mac4(acc, fbuf[(st * RS + r) * U + tid], hbuf[(st * RS + r) * U + tid], dc);
     __syncthreads();  // every thread is done reading stage st
@@ -452,7 +457,7 @@ __global__ void __launch_bounds__(BR / 2)
     __syncthreads();
     return;
   }
-  reinterpret_cast<float4*>(s.tail + ((size_t)c * 2 + which) * s.B + bin0)[tid] = acc;
+  reinterpret_cast<float4*>(s.tail + ((size_t)c * 3 + trow) * s.B + bin0)[tid] = acc;
 }
 
 template <int BR, int RS, int NS>
@@ -482,13 +487,14 @@ cudaError_t launch_ir_t(const DevState& s, const IrRows& ir, const int* chans, i
 }
 
 template <int LOG2M>
-cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, cudaStream_t st, const MixEpi& epi) {
+cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, int parity, cudaStream_t st,
+                          const MixEpi& epi) {
   using S = FftShape<LOG2M>;
   const size_t smem = (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2);
   if (d.param)
-    head_kernel<LOG2M, ParDesc><<<s.C, S::T, smem, st>>>(s, ParDesc{*d.param}, cur, epi);
+    head_kernel<LOG2M, ParDesc><<<s.C, S::T, smem, st>>>(s, ParDesc{*d.param}, cur, parity, epi);
   else
-    head_kernel<LOG2M, DevDesc><<<s.C, S::T, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, cur, epi);
+    head_kernel<LOG2M, DevDesc><<<s.C, S::T, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, cur, parity, epi);
   return cudaGetLastError();
 }
 
@@ -507,18 +513,21 @@ cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, cudaStr
   }
 
 template <int UX, int SY, int D>
-cudaError_t launch_tail_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st, bool pdl) {
+cudaError_t launch_tail_t(const DevState& s, const BlockRef& d, int which, int cur, int trow, cudaStream_t st,
+                          bool pdl) {
   const int U = s.B >> 1;
   dim3 grid((U + UX - 1) / UX, s.C);
   dim3 block(UX, SY);
   if (d.param)
-    return launch_k(tail_kernel<UX, SY, D, ParDesc>, grid, block, 0, st, pdl, s, ParDesc{*d.param}, which, cur);
+    return launch_k(tail_kernel<UX, SY, D, ParDesc>, grid, block, 0, st, pdl, s, ParDesc{*d.param}, which, cur,
+                    trow);
   return launch_k(tail_kernel<UX, SY, D, DevDesc>, grid, block, 0, st, pdl, s, DevDesc{d.ctl, d.in, d.out}, which,
-                  cur);
+                  cur, trow);
 }
 
 template <int BR, int RS, int NS>
-cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int cur, cudaStream_t st, bool pdl) {
+cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int cur, int trow, cudaStream_t st,
+                          bool pdl) {
   if (s.B % BR != 0) return cudaErrorInvalidValue;
   constexpr int smem = bulk_smem_bytes<BR, RS, NS>();
   static cudaError_t attr = [] {
@@ -532,12 +541,12 @@ cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int c
   dim3 grid(s.B / BR, s.C);
   if (d.param)
     return launch_k(tail_bulk_kernel<BR, RS, NS, ParDesc>, grid, dim3(BR / 2), smem, st, pdl, s,
-                    ParDesc{*d.param}, which, cur);
+                    ParDesc{*d.param}, which, cur, trow);
   return launch_k(tail_bulk_kernel<BR, RS, NS, DevDesc>, grid, dim3(BR / 2), smem, st, pdl, s,
-                  DevDesc{d.ctl, d.in, d.out}, which, cur);
+                  DevDesc{d.ctl, d.in, d.out}, which, cur, trow);
 }
 
-using TailLauncher = cudaError_t (*)(const DevState&, const BlockRef&, int, int, cudaStream_t, bool);
+using TailLauncher = cudaError_t (*)(const DevState&, const BlockRef&, int, int, int, cudaStream_t, bool);
 struct TailEntry {
   MacTiling t;
   TailLauncher fn;
@@ -581,17 +590,18 @@ cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* c
   TANB_DISPATCH_LOG2(s.log2B, launch_ir_t, s, ir, chans, nch, ctl, st);
 }
 
-cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, cudaStream_t st, const MixEpi& epi) {
-  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, d, cur, st, epi);
+cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, int parity, cudaStream_t st,
+                        const MixEpi& epi) {
+  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, d, cur, parity, st, epi);
 }
 
-cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, MacTiling t,
+cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, int trow, MacTiling t,
                         cudaStream_t st, bool pdl) {
-  if (s.P <= 1) return cudaSuccess;
+  if (s.P <= 2) return cudaSuccess;
   for (int i = 0; i < kTailCount; ++i)
     if (kTail[i].t.ux == t.ux && kTail[i].t.sy == t.sy && kTail[i].t.depth == t.depth &&
         kTail[i].t.kind == t.kind)
-      return kTail[i].fn(s, d, which, cur, st, pdl);
+      return kTail[i].fn(s, d, which, cur, trow, st, pdl);
   return cudaErrorInvalidValue;
 }
 

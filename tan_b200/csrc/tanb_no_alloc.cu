@@ -111,7 +111,7 @@ extern "C" int32_t tanb_convolve_no_alloc(const float* in, const float* ir, floa
   const size_t o_fdl = o_H + up256(C * 2 * P * B * sizeof(float2));
   const size_t o_prev = o_fdl + up256(C * P * B * sizeof(float2));
   const size_t o_tail = o_prev + up256(C * B * sizeof(float));
-  const size_t o_irp = o_tail + up256(C * 2 * B * sizeof(float2));
+  const size_t o_irp = o_tail + up256(C * 3 * B * sizeof(float2));
   const size_t o_ctl = o_irp + up256(C * P * B * sizeof(float));
   const size_t o_rows = o_ctl + up256(C * sizeof(tanb::ChanCtl));
   const size_t o_chans = o_rows + up256(2 * C * sizeof(void*));
@@ -156,7 +156,7 @@ extern "C" int32_t tanb_convolve_no_alloc(const float* in, const float* ir, floa
   do {
     if ((e = cudaMemsetAsync(s.fdl, 0, C * P * B * sizeof(float2), st)) != cudaSuccess) break;
     if ((e = cudaMemsetAsync(s.prev, 0, C * B * sizeof(float), st)) != cudaSuccess) break;
-    if ((e = cudaMemsetAsync(s.tail, 0, C * 2 * B * sizeof(float2), st)) != cudaSuccess) break;
+    if ((e = cudaMemsetAsync(s.tail, 0, C * 3 * B * sizeof(float2), st)) != cudaSuccess) break;
     if ((e = cudaMemsetAsync(irp, 0, C * P * B * sizeof(float), st)) != cudaSuccess) break;
     if ((e = cudaMemcpy2DAsync(irp, P * B * sizeof(float), ir, ir_length * sizeof(float),
                                ir_length * sizeof(float), C, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
@@ -182,8 +182,8 @@ extern "C" int32_t tanb_convolve_no_alloc(const float* in, const float* ir, floa
       ref.ctl = ctl;
       ref.in = in_rows;
       ref.out = out_rows;
-      if ((e = tanb::launch_head(s, ref, cur, st)) != cudaSuccess) break;
-      e = tanb::launch_tail(s, ref, 0, cur, tanb::MacTiling{32, 8}, st, true);
+      if ((e = tanb::launch_head(s, ref, cur, (int)(b & 1), st)) != cudaSuccess) break;
+      e = tanb::launch_tail(s, ref, 0, cur, (int)((b + 1) & 1), tanb::MacTiling{32, 8}, st, true);
     }
   } while (0);
   if (e != cudaSuccess) {
