@@ -382,7 +382,7 @@ def run_ours(args):
     prof = conv.profile_read()
     tail = prof["tail"]
     tail_ms_avg = tail["ms"] / max(1, tail["timed"])
-    bytes_per_tail = C * ((P - 1) * B * 16 + B * 8)
+    bytes_per_tail = C * ((P - 2) * B * 16 + B * 8)  # partitions 2..P-1 of H and FDL, one tail row written
     peak, peak_kind = hbm_peak()
     achieved = bytes_per_tail / (tail_ms_avg / 1e3) / 1e9
     floor = size_floor(torch, stream, flush_l2, bytes_per_tail, dev)

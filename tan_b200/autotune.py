@@ -105,7 +105,7 @@ def tune(ctx, B: int, L: int, C: int, write: bool = True) -> dict:
     res = measure(ctx, B, L, C)
     best = min(res, key=lambda r: r[2])
     P = max(1, -(-L // B))
-    bytes_per_launch = C * ((P - 1) * B * 16 + B * 8)
+    bytes_per_launch = C * (max(0, P - 2) * B * 16 + B * 8)  # the tail streams partitions 2..P-1
     entry = {"index": best[0], "tiling": list(best[1]), "block_us": best[2], "tail_us": best[3],
              "gbs": bytes_per_launch / (best[3] * 1e-6) / 1e9,
              "all": [{"index": i, "tiling": list(t), "block_us": b, "tail_us": us} for i, t, b, us in res]}
