@@ -161,17 +161,46 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   const bool p1 = s.P > 1;
   const float2* xp = s.fdl + ((size_t)c * s.P + (cur + 1) % s.P) * M;
 
-  // twiddles into shared memory (small transforms), coalesced float4 loads
-  const float2* tw = s.tw;
-  if constexpr (S::TW_SMEM) {
-    float2* tws = sm + 2 * M;
-    for (int j = threadIdx.x; j < M; j += T)
-      reinterpret_cast<float4*>(tws)[j] = __ldg(reinterpret_cast<const float4*>(s.tw) + j);
-    tw = tws;
+  // Every global load of the prologue is issued before any of them is used,
+  // so the block waits for one memory round trip instead of one per phase:
+  // first the frame (caller rows may sit in pinned host memory, the longest
+  // latency), then the twiddles, then the tail, partitions 0 and 1 and X_{k-1}.
+  // frame [x_{k-1}, x_k] packed as complex pairs; 8-byte loads where the
+  // caller's row allows
+  const bool x_vec = x && (reinterpret_cast<uintptr_t>(x) & 7) == 0;
+  const int16_t* x16 = epi.active ? reinterpret_cast<const int16_t*>(x) : nullptr;
+  constexpr int E = M / T;
+  float2 zr[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int n = threadIdx.x + e * T;
+    if (n < M / 2) {
+      zr[e] = reinterpret_cast<const float2*>(prev)[n];
+    } else if (!x) {
+      zr[e] = make_float2(0.f, 0.f);
+    } else if (x16) {
+      const int k = 2 * (n - M / 2);
+      zr[e] = make_float2(__fmul_rn((float)x16[k], epi.in_scale), __fmul_rn((float)x16[k + 1], epi.in_scale));
+    } else if (x_vec) {
+      zr[e] = reinterpret_cast<const float2*>(x)[n - M / 2];
+    } else {
+      const float* src = x + 2 * (n - M / 2);
+      zr[e] = make_float2(src[0], src[1]);
+    }
   }
-  // prefetch the tail and partition 0 of this thread's bin pairs; they do not
-  // depend on the transform, so their latency hides behind it
-  float2 pt[KP][2], ph[KP][2];
+  // twiddles (staged in shared memory for small transforms), float4 loads
+  const float2* tw = s.tw;
+  float4 twr[S::TW_SMEM ? E : 1];
+  if constexpr (S::TW_SMEM) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) twr[e] = __ldg(reinterpret_cast<const float4*>(s.tw) + threadIdx.x + e * T);
+  }
+  // tail and partition 0 of this thread's bin pairs, and the partition-1
+  // product's operands; they do not depend on the transform. At 1024 threads
+  // (64 registers each) the partition-1 product is taken as its operands
+  // arrive, so that the prefetch fits in registers.
+  constexpr bool kHoldP1 = T < 1024;
+  float2 pt[KP][2], ph[KP][2], px[kHoldP1 ? KP : 1][2], p1h[kHoldP1 ? KP : 1][2];
 #pragma unroll
   for (int q = 0; q < KP; ++q) {
     const int k = threadIdx.x + q * T;
@@ -179,31 +208,39 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
       const int km = (k == 0) ? 0 : M - k;
       pt[q][0] = t0[k];
       pt[q][1] = t0[km];
-      if (p1) {
+      ph[q][0] = h0[k];
+      ph[q][1] = h0[km];
+      if constexpr (kHoldP1) {
+        if (p1) {
+          px[q][0] = xp[k];
+          px[q][1] = xp[km];
+          p1h[q][0] = h0[M + k];
+          p1h[q][1] = h0[M + km];
+        }
+      } else if (p1) {
         pt[q][0] = (k == 0) ? c_mac_dc(pt[q][0], xp[0], h0[M]) : c_mac(pt[q][0], xp[k], h0[M + k]);
         if (k != 0) pt[q][1] = c_mac(pt[q][1], xp[km], h0[M + km]);
       }
-      ph[q][0] = h0[k];
-      ph[q][1] = h0[km];
     }
   }
-  // frame [x_{k-1}, x_k] packed as complex pairs; 8-byte loads where the
-  // caller's row allows (rows in pinned host staging are read over the bus)
-  const bool x_vec = x && (reinterpret_cast<uintptr_t>(x) & 7) == 0;
-  const int16_t* x16 = epi.active ? reinterpret_cast<const int16_t*>(x) : nullptr;
-  for (int n = threadIdx.x; n < M; n += T) {
-    if (n < M / 2) {
-      z[n] = reinterpret_cast<const float2*>(prev)[n];
-    } else if (!x) {
-      z[n] = make_float2(0.f, 0.f);
-    } else if (x16) {
-      const int k = 2 * (n - M / 2);
-      z[n] = make_float2(__fmul_rn((float)x16[k], epi.in_scale), __fmul_rn((float)x16[k + 1], epi.in_scale));
-    } else if (x_vec) {
-      z[n] = reinterpret_cast<const float2*>(x)[n - M / 2];
-    } else {
-      const float* src = x + 2 * (n - M / 2);
-      z[n] = make_float2(src[0], src[1]);
+  if constexpr (S::TW_SMEM) {
+    float2* tws = sm + 2 * M;
+#pragma unroll
+    for (int e = 0; e < E; ++e) reinterpret_cast<float4*>(tws)[threadIdx.x + e * T] = twr[e];
+    tw = tws;
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) z[threadIdx.x + e * T] = zr[e];
+  if constexpr (kHoldP1) {
+    if (p1) {
+#pragma unroll
+      for (int q = 0; q < KP; ++q) {
+        const int k = threadIdx.x + q * T;
+        if (k <= M / 2) {
+          pt[q][0] = (k == 0) ? c_mac_dc(pt[q][0], px[q][0], p1h[q][0]) : c_mac(pt[q][0], px[q][0], p1h[q][0]);
+          if (k != 0) pt[q][1] = c_mac(pt[q][1], px[q][1], p1h[q][1]);
+        }
+      }
     }
   }
   __syncthreads();
