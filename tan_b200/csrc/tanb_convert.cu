@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "../../include/tanb.h"
+#include "tanb_host_pool.h"
 #include "tanb_internal.h"
 
 namespace tanb {
@@ -195,7 +196,7 @@ int32_t host_convert(tanb_converter* cv, const Tin* const* in, size_t in_step, s
   CV_CUDA(cv->stage_out.reserve((size_t)count * n * sizeof(Tout)));
   Tin* sin = static_cast<Tin*>(cv->stage_in.p);
   Tout* sout = static_cast<Tout*>(cv->stage_out.p);
-  for (int r = 0; r < count; ++r) std::memcpy(sin + (size_t)r * span, in[r], span * sizeof(Tin));
+  for (int r = 0; r < count; ++r) tanb::copy_for_device(sin + (size_t)r * span, in[r], span * sizeof(Tin));
   for (int r0 = 0; r0 < count; r0 += kMaxRows) {
     const int rows = std::min(kMaxRows, count - r0);
     RowTable t{};
@@ -451,7 +452,7 @@ int32_t tanb_mixer_mix(tanb_mixer* m, const float* const* in, float* out) {
   float* sout = static_cast<float*>(m->stage_out.p);
   std::vector<const float*> rows(C);
   for (size_t c = 0; c < C; ++c) {
-    std::memcpy(sin + c * n, in[c], n * sizeof(float));
+    tanb::copy_for_device(sin + c * n, in[c], n * sizeof(float));
     rows[c] = sin + c * n;
   }
   CV_CUDA(mix_rows(m, rows.data(), sout, 1));

@@ -344,10 +344,10 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
       const int j0 = (int)((long long)nch * q / groups), j1 = (int)((long long)nch * (q + 1) / groups);
       if (groups > 1) {
         tanb::host_parallel_for(j1 - j0, [&](int r) {
-          std::memcpy(v->h_ir + (size_t)(j0 + r) * n, ir[chans[j0 + r]], row_bytes);
+          tanb::copy_for_device(v->h_ir + (size_t)(j0 + r) * n, ir[chans[j0 + r]], row_bytes);
         });
       } else {
-        for (int j = j0; j < j1; ++j) std::memcpy(v->h_ir + (size_t)j * n, ir[chans[j]], row_bytes);
+        for (int j = j0; j < j1; ++j) tanb::copy_for_device(v->h_ir + (size_t)j * n, ir[chans[j]], row_bytes);
       }
       TANB_CUDA(cudaMemcpyAsync(v->d_ir + (size_t)j0 * n, v->h_ir + (size_t)j0 * n, (size_t)(j1 - j0) * row_bytes,
                                 cudaMemcpyHostToDevice, v->stream));
@@ -687,7 +687,7 @@ int32_t td_update(tanb_convolution* v, Mem mem, const float* const* ir, size_t n
     float* dst = td_ir_row(v, v->slot_new[c], c);
     if (mem == Mem::Host) {
       float* row = v->h_td + (size_t)c * len;
-      if (n) std::memcpy(row, ir[c], n * sizeof(float));
+      if (n) tanb::copy_for_device(row, ir[c], n * sizeof(float));
       std::memset(row + n, 0, (len - n) * sizeof(float));
       TANB_CUDA(cudaMemcpyAsync(dst, row, len * sizeof(float), cudaMemcpyHostToDevice, v->stream));
     } else {
@@ -757,7 +757,7 @@ int32_t td_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem 
     t.fade0 = v->td_fade < 0 ? 0 : v->td_fade;
     if (in_mem == Mem::Host) {
       t.in = in[c] ? v->td_io + c * len : nullptr;
-      if (in[c] && run[c]) std::memcpy(h_in + c * len, in[c], ns * sizeof(float));
+      if (in[c] && run[c]) tanb::copy_for_device(h_in + c * len, in[c], ns * sizeof(float));
     } else {
       t.in = in[c];
     }
@@ -800,11 +800,11 @@ int32_t td_process_direct(tanb_convolution* v, const float* const* ir, const flo
     const int first = nz ? nz[2 * c] : 0, last = nz ? nz[2 * c + 1] : (int)len;
     float* row = v->h_td + c * len;
     if (last > first) {
-      std::memcpy(row + first, ir[c] + first, (last - first) * sizeof(float));
+      tanb::copy_for_device(row + first, ir[c] + first, (last - first) * sizeof(float));
       TANB_CUDA(cudaMemcpyAsync(v->td_dir + c * len + first, row + first, (last - first) * sizeof(float),
                                 cudaMemcpyHostToDevice, v->stream));
     }
-    std::memcpy(h_in + c * len, in[c], n * sizeof(float));
+    tanb::copy_for_device(h_in + c * len, in[c], n * sizeof(float));
     tanb::TdChan& t = v->h_tdchan[c];
     t = tanb::TdChan{};
     t.run = 1;

@@ -529,7 +529,7 @@ static int32_t engine_update(tanb_engine* e, int32_t session, const float* const
     for (int j = 0; j < s.C; ++j) e->h_upd[j].src = ir[j];
   } else if (n) {
     // compact staging (row stride n) copied on the host pool, one transfer
-    auto copy_row = [&](int j) { std::memcpy(e->h_ir + (size_t)j * n, ir[j], n * sizeof(float)); };
+    auto copy_row = [&](int j) { tanb::copy_for_device(e->h_ir + (size_t)j * n, ir[j], n * sizeof(float)); };
     if ((size_t)s.C * n * sizeof(float) >= (1u << 20))
       tanb::host_parallel_for(s.C, copy_row);
     else

@@ -2,7 +2,8 @@
 // index at a time through an atomic counter; workers sleep on a condition
 // variable between jobs. Jobs are serialised by a mutex, so concurrent API
 // calls from several threads take turns. In a process forked after the pool
-// started, jobs run serially on the caller.
+// started, jobs run serially on the caller. copy_for_device streams large
+// copies into pinned memory past the CPU caches.
 #include "tanb_host_pool.h"
 
 #include <algorithm>
@@ -12,7 +13,13 @@
 #include <thread>
 #include <vector>
 
+#include <cstdint>
+#include <cstring>
+
 #include <unistd.h>
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 namespace tanb {
 namespace {
@@ -101,5 +108,34 @@ void host_parallel_for(int n, const std::function<void(int)>& fn) {
 }
 
 int host_pool_threads() { return pool().threads(); }
+
+void copy_for_device(void* dst, const void* src, size_t bytes) {
+#if defined(__x86_64__)
+  if (bytes >= 4096) {
+    auto* d = static_cast<uint8_t*>(dst);
+    auto* s = static_cast<const uint8_t*>(src);
+    const size_t lead = (16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15;
+    std::memcpy(d, s, lead);
+    d += lead;
+    s += lead;
+    bytes -= lead;
+    const size_t body = bytes & ~size_t(63);
+    for (size_t i = 0; i < body; i += 64) {
+      const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i*>(s + i));
+      const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i*>(s + i + 16));
+      const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i*>(s + i + 32));
+      const __m128i e = _mm_loadu_si128(reinterpret_cast<const __m128i*>(s + i + 48));
+      _mm_stream_si128(reinterpret_cast<__m128i*>(d + i), a);
+      _mm_stream_si128(reinterpret_cast<__m128i*>(d + i + 16), b);
+      _mm_stream_si128(reinterpret_cast<__m128i*>(d + i + 32), c);
+      _mm_stream_si128(reinterpret_cast<__m128i*>(d + i + 48), e);
+    }
+    std::memcpy(d + body, s + body, bytes - body);
+    _mm_sfence();  // the stores are visible before anything this thread does next
+    return;
+  }
+#endif
+  std::memcpy(dst, src, bytes);
+}
 
 }  // namespace tanb

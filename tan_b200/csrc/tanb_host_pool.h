@@ -15,4 +15,12 @@ void host_parallel_for(int n, const std::function<void(int)>& fn);
 // Worker threads of the pool (0 until first use), for reporting.
 int host_pool_threads();
 
+// memcpy into pinned memory that the device reads next (a host-to-device copy
+// or a kernel reading mapped host memory). On x86-64, copies of 4 KiB and more
+// use non-temporal stores, followed by a store fence: lines written through
+// the cache stay dirty there, and a device read of dirty lines is served from
+// the CPU's caches at a fraction of the bus rate (a 16 MiB upload measured
+// 2.2x slower end to end); non-temporal stores leave nothing in the cache.
+void copy_for_device(void* dst, const void* src, size_t bytes);
+
 }  // namespace tanb

@@ -2,7 +2,9 @@
 compiler and driven without a GPU: every index runs exactly once for any job
 size, jobs from several threads at once do not mix, and a child forked after
 the pool started runs its jobs serially instead of waiting on threads it does
-not have."""
+not have. copy_for_device (the streaming copy into staging memory) copies every
+byte for any size and any source / destination alignment, and writes nothing
+outside the destination range."""
 import os
 import shutil
 import subprocess
@@ -12,6 +14,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 DRIVER = r"""
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <thread>
@@ -29,8 +32,26 @@ static int check(int n) {
   return 0;
 }
 
+static int check_copy() {
+  std::vector<unsigned char> src(70000), dst(70000 + 64);
+  for (size_t i = 0; i < src.size(); ++i) src[i] = (unsigned char)(i * 131u + 7u);
+  for (size_t n : {0u, 1u, 15u, 4095u, 4096u, 4097u, 4160u, 65536u + 13u})
+    for (int so = 0; so < 3; ++so)
+      for (int doff = 0; doff < 19; doff += 3) {
+        std::fill(dst.begin(), dst.end(), (unsigned char)0xA5);
+        tanb::copy_for_device(dst.data() + 16 + doff, src.data() + so, n);
+        for (size_t i = 0; i < dst.size(); ++i) {
+          const bool in = i >= (size_t)(16 + doff) && i < 16 + doff + n;
+          const unsigned char want = in ? src[so + i - 16 - doff] : (unsigned char)0xA5;
+          if (dst[i] != want) return 1;
+        }
+      }
+  return 0;
+}
+
 int main() {
   int bad = 0;
+  bad += 1000 * check_copy();
   for (int n : {0, 1, 2, 3, 7, 64, 1000, 4097}) bad += check(n);
   std::vector<std::thread> ts;
   std::atomic<int> tbad{0};
