@@ -103,7 +103,8 @@ struct tanb_convolution {
   int64_t blocks = 0;  // blocks processed: the parity selects the tail row
   // per-block descriptors passed as kernel parameters (C <= kParamChannels)
   std::vector<tanb::ParamDesc> pdesc;
-  tanb::ParamDesc last_pdesc{};
+  std::vector<tanb::StageDesc> sdesc;
+  tanb::CtlParam last_ctlp{};
   bool last_is_param = false;
 
   // UpdateResponseTD staging: IR rows [C][P*B], then ChanCtl[C] + int[C]
@@ -286,7 +287,7 @@ int32_t run_pending_finalize(tanb_convolution* v) {
   if (v->P <= 2) return TANB_OK;  // no partitions beyond the head's two
   tanb::BlockRef ref;
   if (v->last_is_param)
-    ref.param = &v->last_pdesc;
+    ref.ctlp = &v->last_ctlp;
   else
     ref.ctl = v->last_desc;
   TANB_CUDA(counted(v, tanb_convolution::kTail,
@@ -521,7 +522,11 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   std::vector<int> cur_b(kMaxBlocksPerChunk);
 
   const bool param = C <= tanb::kParamChannels;
+  // rows in the object's staging (host rows, the fused pipeline's int16 rows
+  // and its scratch outputs): two base pointers describe every channel
+  const bool staged = param && (pcm || (in_mem == Mem::Host && out_mem == Mem::Host));
   if (param && v->pdesc.size() < (size_t)kMaxBlocksPerChunk) v->pdesc.resize(kMaxBlocksPerChunk);
+  if (staged && v->sdesc.size() < (size_t)kMaxBlocksPerChunk) v->sdesc.resize(kMaxBlocksPerChunk);
   while (processed < nblocks && status == TANB_OK) {
     int nb = (int)std::min<size_t>(kMaxBlocksPerChunk, nblocks - processed);
     TANB_CUDA(cudaEventSynchronize(v->ev_stage));
@@ -534,14 +539,18 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         status = fail(TANB_WRONG_STATE, "no running channels");
         break;
       }
-      ChanCtl* ctl = param ? v->pdesc[b].ctl : v->desc_ctl(v->h_stage, b);
-      const float** din = param ? v->pdesc[b].in : v->desc_in(v->h_stage, b);
-      float** dout = param ? v->pdesc[b].out : v->desc_out(v->h_stage, b);
+      tanb::ParamDesc* pd = param ? &v->pdesc[b] : nullptr;
+      tanb::StageDesc* sd = staged ? &v->sdesc[b] : nullptr;
+      ChanCtl* ctl = param ? nullptr : v->desc_ctl(v->h_stage, b);
+      const float** din = param ? nullptr : v->desc_in(v->h_stage, b);
+      float** dout = param ? nullptr : v->desc_out(v->h_stage, b);
       flush_b[b].clear();
       for (int c = 0; c < C; ++c) {
         if (flush[c]) flush_b[b].push_back(c);
         const int sw = (v->pending[c] && run[c]) ? 1 : 0;
-        ctl[c] = ChanCtl{run[c], sw, v->active[c], v->slot_new[c]};
+        const ChanCtl cc{run[c], sw, v->active[c], v->slot_new[c]};
+        const float* x = nullptr;
+        float* y = nullptr;
         if (sw) {
           v->active[c] = v->slot_new[c];
           v->pending[c] = 0;
@@ -555,20 +564,36 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
           int16_t* row = reinterpret_cast<int16_t*>(v->stage_in(v->h_stage, b, c));
           const int16_t* src = pcm->in[c] + blk * B * pcm->in_step;
           for (int i = 0; i < B; ++i) row[i] = src[(size_t)i * pcm->in_step];
-          din[c] = v->stage_in(v->h_stage, b, c);
+          x = v->stage_in(v->h_stage, b, c);
         } else if (in_mem == Mem::Host) {
-          din[c] = in[c] ? v->stage_in(v->h_stage, b, c) : nullptr;
+          x = in[c] ? v->stage_in(v->h_stage, b, c) : nullptr;
           if (run[c] && in[c]) std::memcpy(v->stage_in(v->h_stage, b, c), in[c] + blk * B, B * sizeof(float));
         } else {
-          din[c] = in[c] ? in[c] + blk * B : nullptr;
+          x = in[c] ? in[c] + blk * B : nullptr;
         }
         if (pcm) {
-          dout[c] = v->d_mix_scratch + (size_t)c * B;
+          y = v->d_mix_scratch + (size_t)c * B;
         } else if (out_mem == Mem::Host) {
-          dout[c] = v->h_out + ((size_t)b * C + c) * B;
+          y = v->h_out + ((size_t)b * C + c) * B;
         } else {
-          dout[c] = out[c] ? out[c] + blk * B : nullptr;
+          y = out[c] ? out[c] + blk * B : nullptr;
         }
+        if (sd) {
+          sd->c.ctl[c] = tanb::pack_ctl(cc, x != nullptr);
+        } else if (pd) {
+          pd->c.ctl[c] = tanb::pack_ctl(cc, x != nullptr);
+          pd->in[c] = x;
+          pd->out[c] = y;
+        } else {
+          ctl[c] = cc;
+          din[c] = x;
+          dout[c] = y;
+        }
+      }
+      if (sd) {
+        sd->in = v->stage_in(v->h_stage, b, 0);
+        sd->out = pcm ? v->d_mix_scratch : v->h_out + (size_t)b * C * B;
+        sd->stride = B;
       }
       run_b[b] = run;
       v->cur = (v->cur - 1 + P) % P;
@@ -584,7 +609,9 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       for (int c : flush_b[b]) TANB_CUDA(flush_channel(v, c));
       const ChanCtl* dctl = v->desc_ctl(v->d_stage, b);
       tanb::BlockRef ref;
-      if (param) {
+      if (staged) {
+        ref.stage = &v->sdesc[b];
+      } else if (param) {
         ref.param = &v->pdesc[b];
       } else {
         ref.ctl = dctl;
@@ -599,7 +626,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       if (last) {
         v->last_desc = dctl;
         v->last_is_param = param;
-        if (param) v->last_pdesc = v->pdesc[b];
+        if (param) v->last_ctlp = staged ? v->sdesc[b].c : v->pdesc[b].c;
         v->last_cur = cur_b[b];
       }
       if (last && v->finalize_mode) {

@@ -67,21 +67,47 @@ MacTiling mac_tiling(int index);
 
 // Per-block descriptors of up to kParamChannels channels, passed to the head
 // and tail kernels as a kernel parameter (no copy to device memory and no
-// dependent global load before a CTA knows its channel's state).
+// dependent global load before a CTA knows its channel's state). The launch
+// cost grows with the parameter size (two launches with 4 KiB of parameters
+// took 11.9 us to enqueue against 4.8 us with 256 B), so a channel's state is
+// one byte, the tail gets only those bytes, and host rows in the object's
+// staging are described by two base pointers instead of pointer tables.
 constexpr int kParamChannels = 128;
+enum : uint8_t { kCtlRun = 1, kCtlSwap = 2, kCtlSlotCur = 4, kCtlSlotNew = 8, kCtlHasIn = 16 };
+inline uint8_t pack_ctl(const ChanCtl& c, bool has_in) {
+  return (uint8_t)((c.run ? kCtlRun : 0) | (c.swap ? kCtlSwap : 0) | (c.slot_cur ? kCtlSlotCur : 0) |
+                   (c.slot_new ? kCtlSlotNew : 0) | (has_in ? kCtlHasIn : 0));
+}
+struct CtlParam {
+  uint8_t ctl[kParamChannels];
+};
+// Caller rows: per-channel pointers.
 struct ParamDesc {
-  ChanCtl ctl[kParamChannels];
+  CtlParam c;
   const float* in[kParamChannels];
   float* out[kParamChannels];
 };
+// Rows in staging: channel c reads in + c * stride (when kCtlHasIn is set)
+// and writes out + c * stride.
+struct StageDesc {
+  CtlParam c;
+  const float* in;
+  float* out;
+  long long stride;
+};
 
-// Where a launch finds its per-channel descriptors: a ParamDesc (host copy,
-// passed by value) or device arrays.
+// Where a launch finds its per-channel descriptors: a ParamDesc or StageDesc
+// (host copy, passed by value), a CtlParam (tail launches that need only the
+// channel states), or device arrays.
 struct BlockRef {
   const ParamDesc* param = nullptr;
+  const StageDesc* stage = nullptr;
+  const CtlParam* ctlp = nullptr;
   const ChanCtl* ctl = nullptr;
   const float* const* in = nullptr;
   float* const* out = nullptr;
+  // the channel states of a parameter descriptor, whichever kind it is
+  const CtlParam* ctl_param() const { return param ? &param->c : stage ? &stage->c : ctlp; }
 };
 
 // Fused PCM pipeline in the head kernel (tanb_convolution_process_mix_pcm16).

@@ -60,11 +60,27 @@ struct DevDesc {
   __device__ __forceinline__ const float* get_in(int c) const { return in[c]; }
   __device__ __forceinline__ float* get_out(int c) const { return out[c]; }
 };
+__device__ __forceinline__ ChanCtl unpack_ctl(uint8_t b) {
+  return ChanCtl{(b & kCtlRun) ? 1 : 0, (b & kCtlSwap) ? 1 : 0, (b & kCtlSlotCur) ? 1 : 0, (b & kCtlSlotNew) ? 1 : 0};
+}
 struct ParDesc {
   ParamDesc p;
-  __device__ __forceinline__ ChanCtl get_ctl(int c) const { return p.ctl[c]; }
+  __device__ __forceinline__ ChanCtl get_ctl(int c) const { return unpack_ctl(p.c.ctl[c]); }
   __device__ __forceinline__ const float* get_in(int c) const { return p.in[c]; }
   __device__ __forceinline__ float* get_out(int c) const { return p.out[c]; }
+};
+struct StgDesc {
+  StageDesc p;
+  __device__ __forceinline__ ChanCtl get_ctl(int c) const { return unpack_ctl(p.c.ctl[c]); }
+  __device__ __forceinline__ const float* get_in(int c) const {
+    return (p.c.ctl[c] & kCtlHasIn) ? p.in + c * p.stride : nullptr;
+  }
+  __device__ __forceinline__ float* get_out(int c) const { return p.out + c * p.stride; }
+};
+// Channel states only (the tail reads no rows).
+struct CtlDesc {
+  CtlParam p;
+  __device__ __forceinline__ ChanCtl get_ctl(int c) const { return unpack_ctl(p.ctl[c]); }
 };
 
 
@@ -510,6 +526,8 @@ cudaError_t set_attrs() {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(head_kernel<LOG2M, ParDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(head_kernel<LOG2M, StgDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(ir_spectrum_kernel<LOG2M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (1 << LOG2M) * (int)sizeof(float2));
 }
@@ -528,7 +546,9 @@ cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, int par
                           const MixEpi& epi) {
   using S = FftShape<LOG2M>;
   const size_t smem = (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2);
-  if (d.param)
+  if (d.stage)
+    head_kernel<LOG2M, StgDesc><<<s.C, S::T, smem, st>>>(s, StgDesc{*d.stage}, cur, parity, epi);
+  else if (d.param)
     head_kernel<LOG2M, ParDesc><<<s.C, S::T, smem, st>>>(s, ParDesc{*d.param}, cur, parity, epi);
   else
     head_kernel<LOG2M, DevDesc><<<s.C, S::T, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, cur, parity, epi);
@@ -555,9 +575,8 @@ cudaError_t launch_tail_t(const DevState& s, const BlockRef& d, int which, int c
   const int U = s.B >> 1;
   dim3 grid((U + UX - 1) / UX, s.C);
   dim3 block(UX, SY);
-  if (d.param)
-    return launch_k(tail_kernel<UX, SY, D, ParDesc>, grid, block, 0, st, pdl, s, ParDesc{*d.param}, which, cur,
-                    trow);
+  if (const CtlParam* cp = d.ctl_param())
+    return launch_k(tail_kernel<UX, SY, D, CtlDesc>, grid, block, 0, st, pdl, s, CtlDesc{*cp}, which, cur, trow);
   return launch_k(tail_kernel<UX, SY, D, DevDesc>, grid, block, 0, st, pdl, s, DevDesc{d.ctl, d.in, d.out}, which,
                   cur, trow);
 }
@@ -571,14 +590,14 @@ cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int c
     cudaError_t e = cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS, DevDesc>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS, ParDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS, CtlDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem);
   }();
   if (attr != cudaSuccess) return attr;
   dim3 grid(s.B / BR, s.C);
-  if (d.param)
-    return launch_k(tail_bulk_kernel<BR, RS, NS, ParDesc>, grid, dim3(BR / 2), smem, st, pdl, s,
-                    ParDesc{*d.param}, which, cur, trow);
+  if (const CtlParam* cp = d.ctl_param())
+    return launch_k(tail_bulk_kernel<BR, RS, NS, CtlDesc>, grid, dim3(BR / 2), smem, st, pdl, s, CtlDesc{*cp},
+                    which, cur, trow);
   return launch_k(tail_bulk_kernel<BR, RS, NS, DevDesc>, grid, dim3(BR / 2), smem, st, pdl, s,
                   DevDesc{d.ctl, d.in, d.out}, which, cur, trow);
 }
