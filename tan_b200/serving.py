@@ -244,6 +244,48 @@ def capacity(ctx, form="batched", C=4, L=65536, block=256, spectrum=eng.SPECTRUM
             "ir_length": L, "block": block, "deadline_ms": deadline, "p99_at": {str(k): v for k, v in last.items()}}
 
 
+def mac_roofline(ctx, channels, C=4, L=48000, block=256, spectrum=eng.SPECTRUM_FP32, blocks=48,
+                 seed=20261203 + 5):
+    """Device time of the engine's block launch with `channels` resident
+    channels (sessions of C channels, IR length L): CUDA events around each
+    block on the engine's stream, inputs and outputs in device memory. The
+    working set (IR spectra and delay lines of every channel) is far larger
+    than L2, so every block streams it from HBM. Returns the algorithmic bytes
+    of one launch (IR spectra, delay line, partial rows, I/O) and the mean
+    launch time."""
+    import torch
+
+    g = np.random.Generator(np.random.PCG64(seed))
+    pool = IRPool(g, n=4, length=L)
+    nsess = max(1, channels // C)
+    e = eng.Engine(ctx, block, spectrum, budget_bytes=170 << 30, max_channels=nsess * C + 8)
+    try:
+        for i in range(nsess):
+            rc, s = e.open_session(C, L)
+            if rc != cv.AMF_OK:
+                raise RuntimeError("open_session failed after %d sessions" % i)
+            s.update_response_td(pool.get(g, C, L), block_until_ready=True)
+        n = nsess * C
+        d_in = torch.empty((n, block), dtype=torch.float32, device="cuda").uniform_(-1, 1)
+        d_out = torch.empty_like(d_in)
+        for _ in range(5):
+            assert e.process_device(d_in.data_ptr(), d_out.data_ptr()) == cv.AMF_OK
+        e.synchronize()
+        e.profile(True)
+        e.profile_read()
+        for _ in range(blocks):
+            assert e.process_device(d_in.data_ptr(), d_out.data_ptr()) == cv.AMF_OK
+        p = e.profile_read()
+        e.profile(False)
+        info = e.info()
+    finally:
+        e.release()
+    us = 1000.0 * p["block_ms"] / max(1, p["timed"])
+    return {"channels": n, "ir_length": L, "block": block, "bytes_per_launch": int(info["block_bytes"]),
+            "avg_launch_us": us, "launches_timed": int(p["timed"]),
+            "achieved_gbs": info["block_bytes"] / (us * 1e-6) / 1e9}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--seconds", type=float, default=30.0)
