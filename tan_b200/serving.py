@@ -296,10 +296,14 @@ def main():
     ap.add_argument("--form", choices=["batched", "plain"], default="batched")
     ap.add_argument("--ir-length", type=int, default=65536)
     ap.add_argument("--channels", type=int, default=4)
+    ap.add_argument("--mac-roofline", type=int, default=0, metavar="CHANNELS",
+                    help="time the engine's block launch with this many resident channels")
     a = ap.parse_args()
     spec = {"fp32": eng.SPECTRUM_FP32, "fp16": eng.SPECTRUM_FP16, "bf16": eng.SPECTRUM_BF16}[a.spectrum]
     ctx = cv.TANContext(0)
-    if a.capacity:
+    if a.mac_roofline:
+        r = mac_roofline(ctx, a.mac_roofline, a.channels, a.ir_length, spectrum=spec)
+    elif a.capacity:
         r = capacity(ctx, a.form, a.channels, a.ir_length, spectrum=spec)
     else:
         r = serve(ctx, a.seconds, a.rate, spectrum=spec, budget=int(a.budget_gb * (1 << 30)))

@@ -223,6 +223,58 @@ def test_finalize_mode_and_device_buffers_match_host_path(tan_ctx):
         c_.Release()
 
 
+@pytest.mark.parametrize("C", [128, 160])
+def test_channel_counts_around_the_parameter_descriptor_limit(tan_ctx, C):
+    """Up to 128 channels the per-block channel states travel as kernel
+    parameters; beyond that as device tables. Both match the restatement with
+    channel flags and an IR swap, and the host, host-to-device and device
+    overloads give the same samples (multi-block calls included)."""
+    import torch
+
+    g = H.rng(700 + C)
+    B, L, nb = 256, 3000, 12
+    x = H.noise(g, C, nb * B)
+    h0, h1 = H.irs(g, C, L), H.irs(g, C, L)
+    events = {0: (h0, None), 5: (h1, None)}
+    flags = []
+    for k in range(nb):
+        f = np.zeros(C, np.uint32)
+        if 2 <= k < 9:
+            f[7] = 1  # STOP_INPUT: rings out
+        if k == 6:
+            f[C - 1] = 2  # FLUSH_STREAM
+        flags.append(f)
+    gpu = make(tan_ctx, L, B, C)
+    y, codes = H.run_stream(gpu, x, B, events, flags_per_block=flags)
+    assert all(c == 0 for c in codes)
+    oracle = ref.RefConvolution(L, B, C, threads=4)
+    yr, _ = H.run_stream(oracle, x, B, events, flags_per_block=flags)
+    assert H.rel_err(y, yr) < TOL
+    # no flags: host rows in 4-block calls vs device and host-to-device overloads
+    host = make(tan_ctx, L, B, C)
+    y0, codes = H.run_stream(host, x, B, events, per_call_blocks=4)
+    assert all(c == 0 for c in codes)
+    dev = make(tan_ctx, L, B, C)
+    hyb = make(tan_ctx, L, B, C)
+    xd = torch.from_numpy(x).cuda()
+    yd, yh = torch.zeros_like(xd), torch.zeros_like(xd)
+    for k0, k1 in ((0, 5), (5, nb)):
+        h = events[k0][0]
+        assert dev.UpdateResponseTDDevice(torch.from_numpy(h).cuda(), L) == 0
+        assert hyb.UpdateResponseTD(h, L) == 0
+        rc, done = dev.ProcessDevice([xd[c, k0 * B:k1 * B] for c in range(C)],
+                                     [yd[c, k0 * B:k1 * B] for c in range(C)], (k1 - k0) * B)
+        assert rc == 0 and done == (k1 - k0) * B
+        rc, done = hyb.ProcessHostToDevice(np.ascontiguousarray(x[:, k0 * B:k1 * B]),
+                                           [yh[c, k0 * B:k1 * B] for c in range(C)], (k1 - k0) * B)
+        assert rc == 0 and done == (k1 - k0) * B
+    assert dev.Synchronize() == 0 and hyb.Synchronize() == 0
+    assert np.array_equal(yd.cpu().numpy(), y0)
+    assert np.array_equal(yh.cpu().numpy(), y0)
+    for c_ in (gpu, host, dev, hyb):
+        c_.Release()
+
+
 def test_multi_block_calls_equal_single_block_calls(tan_ctx):
     g = H.rng(8)
     C, B, L, nb = 2, 128, 4096, 40
