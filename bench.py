@@ -90,10 +90,15 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50",
                  "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region is short: start it once sampling is running
+            t_end = time.time() + 3.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()
         except Exception:
             self.proc = None
         return self

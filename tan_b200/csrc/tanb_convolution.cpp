@@ -602,9 +602,14 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     }
     nb = filled;
     if (nb == 0) break;
-    if (!param)
+    // ev_stage guards the host descriptor tables until their upload has run;
+    // ev_out guards the host staging rows until the heads have read and
+    // written them. A call on device rows with parameter descriptors uses
+    // neither and records no event.
+    if (!param) {
       TANB_CUDA(cudaMemcpyAsync(v->d_stage, v->h_stage, nb * v->desc_bytes, cudaMemcpyHostToDevice, v->stream));
-    TANB_CUDA(cudaEventRecord(v->ev_stage, v->stream));
+      TANB_CUDA(cudaEventRecord(v->ev_stage, v->stream));
+    }
     for (int b = 0; b < nb; ++b) {
       for (int c : flush_b[b]) TANB_CUDA(flush_channel(v, c));
       const ChanCtl* dctl = v->desc_ctl(v->d_stage, b);
@@ -643,7 +648,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     // Outputs are final after the heads; in the default mode the last tail,
     // which overlaps its head, completes before this event as well. The
     // staged inputs and outputs are free again once it has completed.
-    TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
+    if (pcm || in_mem == Mem::Host || out_mem == Mem::Host) TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
     if (out_mem == Mem::Host) {
       TANB_CUDA(cudaEventSynchronize(v->ev_out));
       if (*v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);

@@ -34,20 +34,42 @@ __device__ __forceinline__ void griddep_launch_dependents() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Launch of `kernel`, with programmatic stream serialization when `pdl` is set.
+// Preferred shared-memory / L1 split (percent of the maximum shared memory)
+// of a block's head and tail launches. Both carry the same value: an SM whose
+// split has been set for one kernel cannot take CTAs of a kernel that asks
+// for another split until it drains, and with the head's dynamic shared
+// memory and the tail's small static buffers the driver's own choices differ
+// (measured: the tail behind a head with 16 KB of dynamic shared memory ended
+// 4 us later than the tail alone; with equal preferences, at the same time).
+// 50% holds a head of up to 64 KB beside the tail's CTAs; the 128 KB head of
+// 8192-sample blocks takes all of it. A kernel that needs more shared memory
+// than its preference gets more regardless.
+int pair_carveout(int log2B) { return log2B >= 13 ? 100 : 50; }
+
+// Launch of `kernel`, with programmatic stream serialization when `pdl` is set
+// and a preferred shared-memory split when `carveout` >= 0.
 template <class... KArgs, class... Args>
 cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
-                     Args&&... args) {
+                     int carveout, Args&&... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute attr[2];
+  int n = 0;
+  if (pdl) {
+    attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[n].val.programmaticStreamSerializationAllowed = 1;
+    ++n;
+  }
+  if (carveout >= 0) {
+    attr[n].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+    attr[n].val.sharedMemCarveout = (unsigned)carveout;
+    ++n;
+  }
   cfg.attrs = attr;
-  cfg.numAttrs = pdl ? 1 : 0;
+  cfg.numAttrs = n;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
@@ -546,13 +568,15 @@ cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, int par
                           const MixEpi& epi) {
   using S = FftShape<LOG2M>;
   const size_t smem = (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2);
+  const int cv = pair_carveout(LOG2M);
   if (d.stage)
-    head_kernel<LOG2M, StgDesc><<<s.C, S::T, smem, st>>>(s, StgDesc{*d.stage}, cur, parity, epi);
-  else if (d.param)
-    head_kernel<LOG2M, ParDesc><<<s.C, S::T, smem, st>>>(s, ParDesc{*d.param}, cur, parity, epi);
-  else
-    head_kernel<LOG2M, DevDesc><<<s.C, S::T, smem, st>>>(s, DevDesc{d.ctl, d.in, d.out}, cur, parity, epi);
-  return cudaGetLastError();
+    return launch_k(head_kernel<LOG2M, StgDesc>, dim3(s.C), dim3(S::T), smem, st, false, cv, s, StgDesc{*d.stage},
+                    cur, parity, epi);
+  if (d.param)
+    return launch_k(head_kernel<LOG2M, ParDesc>, dim3(s.C), dim3(S::T), smem, st, false, cv, s, ParDesc{*d.param},
+                    cur, parity, epi);
+  return launch_k(head_kernel<LOG2M, DevDesc>, dim3(s.C), dim3(S::T), smem, st, false, cv, s,
+                  DevDesc{d.ctl, d.in, d.out}, cur, parity, epi);
 }
 
 #define TANB_DISPATCH_LOG2(L2, FN, ...)                          \
@@ -576,8 +600,10 @@ cudaError_t launch_tail_t(const DevState& s, const BlockRef& d, int which, int c
   dim3 grid((U + UX - 1) / UX, s.C);
   dim3 block(UX, SY);
   if (const CtlParam* cp = d.ctl_param())
-    return launch_k(tail_kernel<UX, SY, D, CtlDesc>, grid, block, 0, st, pdl, s, CtlDesc{*cp}, which, cur, trow);
-  return launch_k(tail_kernel<UX, SY, D, DevDesc>, grid, block, 0, st, pdl, s, DevDesc{d.ctl, d.in, d.out}, which,
+    return launch_k(tail_kernel<UX, SY, D, CtlDesc>, grid, block, 0, st, pdl, pair_carveout(s.log2B), s,
+                    CtlDesc{*cp}, which, cur, trow);
+  return launch_k(tail_kernel<UX, SY, D, DevDesc>, grid, block, 0, st, pdl, pair_carveout(s.log2B), s,
+                  DevDesc{d.ctl, d.in, d.out}, which,
                   cur, trow);
 }
 
@@ -596,9 +622,9 @@ cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int c
   if (attr != cudaSuccess) return attr;
   dim3 grid(s.B / BR, s.C);
   if (const CtlParam* cp = d.ctl_param())
-    return launch_k(tail_bulk_kernel<BR, RS, NS, CtlDesc>, grid, dim3(BR / 2), smem, st, pdl, s, CtlDesc{*cp},
+    return launch_k(tail_bulk_kernel<BR, RS, NS, CtlDesc>, grid, dim3(BR / 2), smem, st, pdl, pair_carveout(s.log2B), s, CtlDesc{*cp},
                     which, cur, trow);
-  return launch_k(tail_bulk_kernel<BR, RS, NS, DevDesc>, grid, dim3(BR / 2), smem, st, pdl, s,
+  return launch_k(tail_bulk_kernel<BR, RS, NS, DevDesc>, grid, dim3(BR / 2), smem, st, pdl, pair_carveout(s.log2B), s,
                   DevDesc{d.ctl, d.in, d.out}, which, cur, trow);
 }
 
