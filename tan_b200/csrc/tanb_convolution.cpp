@@ -17,12 +17,17 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
+
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 #include "../../include/tanb.h"
 #include "tanb_host_pool.h"
@@ -111,6 +116,15 @@ struct tanb_convolution {
   float* h_ir = nullptr;
   float* d_ir = nullptr;
   int* h_err = nullptr;  // host-mapped error word written by kernels (DevState::err)
+  // head completion for host-row calls (tanb::HeadSignal): the count lives in
+  // device memory, the flag in mapped host memory; head_seq numbers launches
+  unsigned* d_head_count = nullptr;
+  long long* h_head_flag = nullptr;
+  long long* d_head_flag = nullptr;
+  long long head_seq = 0;
+  // host staging rows may still be in use by heads whose completion this
+  // object has not observed (ev_out covers them)
+  bool staging_busy = false;
   uint8_t* h_uctl = nullptr;
   uint8_t* d_uctl = nullptr;
 
@@ -212,6 +226,8 @@ void free_all(tanb_convolution* v) {
   cudaFree(v->ds.tail);
   cudaFree(v->d_tw);
   cudaFree(v->d_stage);
+  cudaFree(v->d_head_count);
+  v->d_head_count = nullptr;
   cudaFree(v->d_ir);
   cudaFree(v->d_uctl);
   cudaFree(v->d_mix_scratch);
@@ -227,6 +243,9 @@ void free_all(tanb_convolution* v) {
   cudaFreeHost(v->h_uctl);
   cudaFreeHost(v->h_err);
   v->h_err = nullptr;
+  cudaFreeHost(v->h_head_flag);
+  v->h_head_flag = v->d_head_flag = nullptr;
+  v->staging_busy = false;
   cudaFree(v->td_hist);
   cudaFree(v->td_ir);
   cudaFree(v->td_dir);
@@ -432,6 +451,31 @@ int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_
   return nrun;
 }
 
+// Waits until the head launch numbered `seq` has signalled (tanb::HeadSignal).
+// Spins on the mapped flag; every 256 polls it also asks whether ev_out (behind
+// the tail launched after that head) has completed, so a failed launch or a
+// missing signal ends the wait with an error instead of spinning on.
+int32_t wait_heads(tanb_convolution* v, long long seq) {
+  volatile long long* flag = v->h_head_flag;
+  for (unsigned n = 1;; ++n) {
+    if (*flag >= seq) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      return TANB_OK;
+    }
+    if ((n & 255) == 0) {
+      const cudaError_t e = cudaEventQuery(v->ev_out);
+      if (e == cudaSuccess) {
+        if (*flag >= seq) continue;
+        return fail(TANB_FAIL, "head launch %lld completed without signalling", seq);
+      }
+      if (e != cudaErrorNotReady) return fail(TANB_FAIL, "head wait: %s", cudaGetErrorString(e));
+    }
+#if defined(__x86_64__)
+    _mm_pause();
+#endif
+  }
+}
+
 // Rows and rules of the fused PCM pipeline (tanb_convolution_process_mix_pcm16).
 struct PcmIO {
   const int16_t* const* in;
@@ -525,12 +569,16 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   // rows in the object's staging (host rows, the fused pipeline's int16 rows
   // and its scratch outputs): two base pointers describe every channel
   const bool staged = param && (pcm || (in_mem == Mem::Host && out_mem == Mem::Host));
+  const bool host_out = out_mem == Mem::Host;  // outputs are read back from host staging
   if (param && v->pdesc.size() < (size_t)kMaxBlocksPerChunk) v->pdesc.resize(kMaxBlocksPerChunk);
   if (staged && v->sdesc.size() < (size_t)kMaxBlocksPerChunk) v->sdesc.resize(kMaxBlocksPerChunk);
   while (processed < nblocks && status == TANB_OK) {
     int nb = (int)std::min<size_t>(kMaxBlocksPerChunk, nblocks - processed);
     TANB_CUDA(cudaEventSynchronize(v->ev_stage));
-    TANB_CUDA(cudaEventSynchronize(v->ev_out));
+    if (v->staging_busy) {
+      TANB_CUDA(cudaEventSynchronize(v->ev_out));
+      v->staging_busy = false;
+    }
     int filled = 0;
     for (int b = 0; b < nb; ++b) {
       const size_t blk = processed + b;
@@ -625,8 +673,10 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       }
       if (pcm) epi.out16 = reinterpret_cast<int16_t*>(v->h_out + (size_t)b * C * B);  // [ngroups][B] of block b
       const int parity = (int)((v->blocks + b) & 1);
+      tanb::HeadSignal sig;
+      if (host_out) sig = tanb::HeadSignal{v->d_head_count, v->d_head_flag, ++v->head_seq};
       TANB_CUDA(counted(v, tanb_convolution::kHead,
-                        [&] { return tanb::launch_head(v->ds, ref, cur_b[b], parity, v->stream, epi); }));
+                        [&] { return tanb::launch_head(v->ds, ref, cur_b[b], parity, v->stream, epi, sig); }));
       const bool last = (b == nb - 1);
       if (last) {
         v->last_desc = dctl;
@@ -648,9 +698,15 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     // Outputs are final after the heads; in the default mode the last tail,
     // which overlaps its head, completes before this event as well. The
     // staged inputs and outputs are free again once it has completed.
-    if (pcm || in_mem == Mem::Host || out_mem == Mem::Host) TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
-    if (out_mem == Mem::Host) {
-      TANB_CUDA(cudaEventSynchronize(v->ev_out));
+    if (pcm || in_mem == Mem::Host || out_mem == Mem::Host) {
+      TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
+      v->staging_busy = true;
+    }
+    if (host_out) {
+      // the outputs are final once the last head has signalled; the tail
+      // launched behind it keeps running while they are scattered
+      if (wait_heads(v, v->head_seq) != TANB_OK) return TANB_FAIL;
+      v->staging_busy = false;
       if (*v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
       if (pcm) {
         for (int b = 0; b < nb; ++b) {
@@ -971,6 +1027,7 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
     if ((e = dev_alloc(v, &v->ds.tail, Cs * 3 * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_tw, 2 * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_stage, kMaxBlocksPerChunk * v->desc_bytes)) != cudaSuccess) break;
+    if ((e = dev_alloc(v, &v->d_head_count, 1)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_ir, Cs * Ps * Bs)) != cudaSuccess) break;
     if ((e = dev_alloc(v, &v->d_uctl, uctl_bytes(C))) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_stage, stage_bytes)) != cudaSuccess) break;
@@ -978,6 +1035,7 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
     if ((e = cudaMallocHost(&v->h_ir, Cs * Ps * Bs * sizeof(float))) != cudaSuccess) break;
     if ((e = cudaMallocHost(&v->h_uctl, uctl_bytes(C))) != cudaSuccess) break;
     if ((e = cudaHostAlloc(&v->h_err, sizeof(int), cudaHostAllocMapped)) != cudaSuccess) break;
+    if ((e = cudaHostAlloc(&v->h_head_flag, sizeof(long long), cudaHostAllocMapped)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_stage, cudaEventDisableTiming)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_ir, cudaEventDisableTiming)) != cudaSuccess) break;
     if ((e = cudaEventCreateWithFlags(&v->ev_out, cudaEventDisableTiming)) != cudaSuccess) break;
@@ -1006,9 +1064,12 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
   v->ds.C = C;
   v->ds.tw = v->d_tw;
   *v->h_err = tanb::kErrNone;
-  if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&v->ds.err), v->h_err, 0)) != cudaSuccess) {
+  *v->h_head_flag = 0;
+  v->head_seq = 0;
+  if ((e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&v->ds.err), v->h_err, 0)) != cudaSuccess ||
+      (e = cudaHostGetDevicePointer(reinterpret_cast<void**>(&v->d_head_flag), v->h_head_flag, 0)) != cudaSuccess) {
     free_all(v);
-    return fail(TANB_FAIL, "mapped error word: %s", cudaGetErrorString(e));
+    return fail(TANB_FAIL, "mapped host words: %s", cudaGetErrorString(e));
   }
   v->tiling = default_tiling(B, v->P);
   v->active.assign(C, 0);

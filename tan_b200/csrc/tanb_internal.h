@@ -129,6 +129,17 @@ struct MixEpi {
   int* clip = nullptr;             // set when a sample was clamped
 };
 
+// Completion signal of a head launch for host-row calls: every CTA fences its
+// output stores system-wide and counts itself in `count` (device memory, zero
+// between launches); the last one resets the count and stores `seq` into
+// `flag` (mapped host memory). The host then reads the outputs without waiting
+// for the tail launched behind the head. seq == 0: no signal.
+struct HeadSignal {
+  unsigned* count = nullptr;
+  long long* flag = nullptr;
+  long long seq = 0;
+};
+
 // Where the IR-spectrum kernel reads row j (the IR of channel chans[j]):
 // ptrs[j] when ptrs (a device array) is set, else base + j * stride. Samples
 // at and after n read as zero, so rows need no padding to P*B.
@@ -150,7 +161,7 @@ cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* c
 // on swap channels), inverse FFT, overlap-save output (and the crossfade).
 // `in[c]` / `out[c]` are device pointers to channel c's B input / output samples.
 cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, int parity, cudaStream_t st,
-                        const MixEpi& epi = MixEpi{});
+                        const MixEpi& epi = MixEpi{}, const HeadSignal& sig = HeadSignal{});
 
 // Tail multiply-accumulate, partitions 2..P-1, for the block after the one
 // whose spectrum sits in delay-line slot `cur`:

@@ -173,16 +173,12 @@ __device__ __forceinline__ void mix_epilogue(const MixEpi& epi, int c) {
 }
 
 template <int LOG2M, class D>
-__global__ void __launch_bounds__(FftShape<LOG2M>::T)
-    head_kernel(DevState s, const __grid_constant__ D desc, int cur, int parity, MixEpi epi) {
+__device__ __forceinline__ void head_body(const DevState& s, const D& desc, int cur, int parity, const MixEpi& epi) {
   using S = FftShape<LOG2M>;
   constexpr int M = S::M, T = S::T, KP = S::KP;
   extern __shared__ float2 sm[];
   float2* z = sm;       // old / only IR
   float2* z2 = sm + M;  // new IR on a swap block
-  // The tail launched behind this kernel (the next block's partitions >= 2)
-  // shares no data with it and may start at once.
-  griddep_launch_dependents();
   const int c = blockIdx.x;
   const ChanCtl cc = desc.get_ctl(c);
   if (!cc.run) return;
@@ -347,6 +343,25 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
     }
   }
   if (epi.active) mix_epilogue<M, T>(epi, c);
+}
+
+template <int LOG2M, class D>
+__global__ void __launch_bounds__(FftShape<LOG2M>::T)
+    head_kernel(DevState s, const __grid_constant__ D desc, int cur, int parity, MixEpi epi, HeadSignal sig) {
+  // The tail launched behind this kernel (the next block's partitions >= 2)
+  // shares no data with it and may start at once.
+  griddep_launch_dependents();
+  head_body<LOG2M>(s, desc, cur, parity, epi);
+  if (sig.seq == 0) return;
+  // Every CTA, running or not, counts itself once its output stores are
+  // visible to the host; the last one raises the flag.
+  __threadfence_system();
+  __syncthreads();
+  if (threadIdx.x == 0 && atomicAdd(sig.count, 1u) == gridDim.x - 1) {
+    *sig.count = 0u;
+    __threadfence_system();
+    *reinterpret_cast<volatile long long*>(sig.flag) = sig.seq;
+  }
 }
 
 // One float4 = two packed bins. u == 0 holds the packed (DC, Nyquist) pair.
@@ -565,18 +580,18 @@ cudaError_t launch_ir_t(const DevState& s, const IrRows& ir, const int* chans, i
 
 template <int LOG2M>
 cudaError_t launch_head_t(const DevState& s, const BlockRef& d, int cur, int parity, cudaStream_t st,
-                          const MixEpi& epi) {
+                          const MixEpi& epi, const HeadSignal& sig) {
   using S = FftShape<LOG2M>;
   const size_t smem = (S::TW_SMEM ? 4 : 2) * S::M * sizeof(float2);
   const int cv = pair_carveout(LOG2M);
   if (d.stage)
     return launch_k(head_kernel<LOG2M, StgDesc>, dim3(s.C), dim3(S::T), smem, st, false, cv, s, StgDesc{*d.stage},
-                    cur, parity, epi);
+                    cur, parity, epi, sig);
   if (d.param)
     return launch_k(head_kernel<LOG2M, ParDesc>, dim3(s.C), dim3(S::T), smem, st, false, cv, s, ParDesc{*d.param},
-                    cur, parity, epi);
+                    cur, parity, epi, sig);
   return launch_k(head_kernel<LOG2M, DevDesc>, dim3(s.C), dim3(S::T), smem, st, false, cv, s,
-                  DevDesc{d.ctl, d.in, d.out}, cur, parity, epi);
+                  DevDesc{d.ctl, d.in, d.out}, cur, parity, epi, sig);
 }
 
 #define TANB_DISPATCH_LOG2(L2, FN, ...)                          \
@@ -673,8 +688,8 @@ cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* c
 }
 
 cudaError_t launch_head(const DevState& s, const BlockRef& d, int cur, int parity, cudaStream_t st,
-                        const MixEpi& epi) {
-  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, d, cur, parity, st, epi);
+                        const MixEpi& epi, const HeadSignal& sig) {
+  TANB_DISPATCH_LOG2(s.log2B, launch_head_t, s, d, cur, parity, st, epi, sig);
 }
 
 cudaError_t launch_tail(const DevState& s, const BlockRef& d, int which, int cur, int trow, MacTiling t,
