@@ -255,7 +255,11 @@ cudaError_t commit_updates(tanb_engine* e) {
   return cudaSuccess;
 }
 
-int tail_ctas(const tanb_engine* e) { return (int)std::min<size_t>(e->tail_grid, e->nitems_hwm); }
+// Item CTAs of the block launch: three quarters of the resident capacity, so
+// that head CTAs fit beside them on every SM.
+int tail_ctas(const tanb_engine* e) {
+  return (int)std::min<size_t>(e->tail_grid - e->tail_grid / 4, e->nitems_hwm);
+}
 
 // Enqueues one block: the single launch over all slots and work items (in and
 // out: device rows or the pinned host buffers).

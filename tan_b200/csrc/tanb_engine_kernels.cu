@@ -5,12 +5,13 @@
 //                      partition, optional FP16/BF16 quantisation with a
 //                      power-of-two per-partition scale, stored in the idle slot
 //                      (runs on the engine's update stream)
-//   eng_block_kernel   per block: CTAs [0, nslots) are the heads of the channel
-//                      slots (as the single-object head, with the tail from the
-//                      channel's partial-sum rows plus the partition-1 product
-//                      computed here); the remaining CTAs are a persistent grid
-//                      over work items (channel, partition range within
-//                      [2, P)) writing the partial sums of the NEXT block. Those
+//   eng_block_kernel   per block: the first CTAs are a persistent grid over
+//                      work items (channel, partition range within [2, P))
+//                      writing the partial sums of the NEXT block; the last
+//                      nslots CTAs are the heads of the channel slots (as the
+//                      single-object head, with the tail from the channel's
+//                      partial-sum rows plus the partition-1 product computed
+//                      here), dispatched into the slots the items leave. Items
 //                      read only delay-line slots X_{k-1} and older, which no
 //                      head writes, and write the other parity's rows, which no
 //                      head reads, so heads and tail items run side by side in
@@ -364,15 +365,18 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   __shared__ int last;
   const long long k = *sync.block;  // blocks processed before this one
   const int parity = (int)(k & 1);
-  if ((int)blockIdx.x < nslots) {
-    const int c = blockIdx.x;
+  // CTAs [0, stride) stream the work items and are dispatched first; the
+  // heads follow and take the SM slots the item CTAs leave free, so heads and
+  // items run side by side from the start of the launch.
+  const int stride = (int)gridDim.x - nslots;
+  if ((int)blockIdx.x >= stride) {
+    const int c = (int)blockIdx.x - stride;
     const EngChan ch = chans[c];
     if (ch.run)
       eng_head<LOG2M, SPEC>(ch, sm, in_base ? in_base + (size_t)c * ld : nullptr, out_base + (size_t)c * ld, tw,
                             parity);
   } else {
-    const int stride = (int)gridDim.x - nslots;
-    for (int it = (int)blockIdx.x - nslots; it < nitems; it += stride) {
+    for (int it = (int)blockIdx.x; it < nitems; it += stride) {
       const EngItem w = items[it];
       if (w.chan < 0) continue;
       const EngChan ch = chans[w.chan];
