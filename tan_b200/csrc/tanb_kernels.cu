@@ -142,6 +142,14 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   }
 }
 
+// Swap-block output samples i and i + 1 (one packed pair): the new IR's output
+// weighted by i / M, the old one's by (M - i) / M (ConvolutionImpl.cpp:1395-1407).
+__device__ __forceinline__ float2 crossfade_pair(float2 o, float2 yn, int i, float step, int M) {
+  const float a0 = step * (float)i, b0 = step * (float)(M - i);
+  const float a1 = step * (float)(i + 1), b1 = step * (float)(M - i - 1);
+  return make_float2(yn.x * a0 + o.x * b0, yn.y * a1 + o.y * b1);
+}
+
 // Fused PCM epilogue (MixEpi): the channel's output row is in epi.scratch; the
 // last head CTA of the channel's group sums the group's rows and converts.
 // The counter is an atomic taken once per CTA after a fence: no CTA waits.
@@ -199,27 +207,44 @@ __device__ __forceinline__ void head_body(const DevState& s, const D& desc, int 
   // so the block waits for one memory round trip instead of one per phase:
   // first the frame (caller rows may sit in pinned host memory, the longest
   // latency), then the twiddles, then the tail, partitions 0 and 1 and X_{k-1}.
-  // frame [x_{k-1}, x_k] packed as complex pairs; 8-byte loads where the
-  // caller's row allows
+  // frame [x_{k-1}, x_k] packed as complex pairs. 16-byte loads of two pairs
+  // when the caller's row allows (history rows and staging rows always do):
+  // half the requests, which counts when the row is read over the host bus.
   const bool x_vec = x && (reinterpret_cast<uintptr_t>(x) & 7) == 0;
   const int16_t* x16 = epi.active ? reinterpret_cast<const int16_t*>(x) : nullptr;
+  const bool x_v4 = !x16 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;  // also when x is null
   constexpr int E = M / T;
   float2 zr[E];
+  if (x_v4) {
+    // pair index q = threadIdx.x + j * T holds z[2q], z[2q + 1]
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int n = threadIdx.x + e * T;
-    if (n < M / 2) {
-      zr[e] = reinterpret_cast<const float2*>(prev)[n];
-    } else if (!x) {
-      zr[e] = make_float2(0.f, 0.f);
-    } else if (x16) {
-      const int k = 2 * (n - M / 2);
-      zr[e] = make_float2(__fmul_rn((float)x16[k], epi.in_scale), __fmul_rn((float)x16[k + 1], epi.in_scale));
-    } else if (x_vec) {
-      zr[e] = reinterpret_cast<const float2*>(x)[n - M / 2];
-    } else {
-      const float* src = x + 2 * (n - M / 2);
-      zr[e] = make_float2(src[0], src[1]);
+    for (int j = 0; j < E / 2; ++j) {
+      const int q = threadIdx.x + j * T;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (q < M / 4)
+        v = reinterpret_cast<const float4*>(prev)[q];
+      else if (x)
+        v = reinterpret_cast<const float4*>(x)[q - M / 4];
+      zr[2 * j] = make_float2(v.x, v.y);
+      zr[2 * j + 1] = make_float2(v.z, v.w);
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int n = threadIdx.x + e * T;
+      if (n < M / 2) {
+        zr[e] = reinterpret_cast<const float2*>(prev)[n];
+      } else if (!x) {
+        zr[e] = make_float2(0.f, 0.f);
+      } else if (x16) {
+        const int k = 2 * (n - M / 2);
+        zr[e] = make_float2(__fmul_rn((float)x16[k], epi.in_scale), __fmul_rn((float)x16[k + 1], epi.in_scale));
+      } else if (x_vec) {
+        zr[e] = reinterpret_cast<const float2*>(x)[n - M / 2];
+      } else {
+        const float* src = x + 2 * (n - M / 2);
+        zr[e] = make_float2(src[0], src[1]);
+      }
     }
   }
   // twiddles (staged in shared memory for small transforms), float4 loads
@@ -263,8 +288,15 @@ __device__ __forceinline__ void head_body(const DevState& s, const D& desc, int 
     for (int e = 0; e < E; ++e) reinterpret_cast<float4*>(tws)[threadIdx.x + e * T] = twr[e];
     tw = tws;
   }
+  if (x_v4) {
 #pragma unroll
-  for (int e = 0; e < E; ++e) z[threadIdx.x + e * T] = zr[e];
+    for (int j = 0; j < E / 2; ++j)
+      reinterpret_cast<float4*>(z)[threadIdx.x + j * T] =
+          make_float4(zr[2 * j].x, zr[2 * j].y, zr[2 * j + 1].x, zr[2 * j + 1].y);
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) z[threadIdx.x + e * T] = zr[e];
+  }
   if constexpr (kHoldP1) {
     if (p1) {
 #pragma unroll
@@ -278,7 +310,8 @@ __device__ __forceinline__ void head_body(const DevState& s, const D& desc, int 
     }
   }
   __syncthreads();
-  for (int n = threadIdx.x; n < M / 2; n += T) reinterpret_cast<float2*>(prev)[n] = z[n + M / 2];
+  for (int q = threadIdx.x; q < M / 4; q += T)
+    reinterpret_cast<float4*>(prev)[q] = reinterpret_cast<const float4*>(z + M / 2)[q];
 
   fft_inplace<LOG2M, false>(z, tw);
 
@@ -326,20 +359,28 @@ __device__ __forceinline__ void head_body(const DevState& s, const D& desc, int 
   if (!y) return;
   const float step = 1.0f / (float)M;
   const bool y_vec = (reinterpret_cast<uintptr_t>(y) & 7) == 0;
-  for (int m = M / 2 + threadIdx.x; m < M; m += T) {
-    const int i = 2 * (m - M / 2);
-    float2 o = z[m];
-    if (swap) {
-      const float2 yn = z2[m];
-      const float a0 = step * (float)i, b0 = step * (float)(M - i);
-      const float a1 = step * (float)(i + 1), b1 = step * (float)(M - i - 1);
-      o = make_float2(yn.x * a0 + o.x * b0, yn.y * a1 + o.y * b1);
+  if ((reinterpret_cast<uintptr_t>(y) & 15) == 0) {
+    // two output pairs (samples 4q .. 4q + 3) per 16-byte store
+    for (int q = threadIdx.x; q < M / 4; q += T) {
+      const int m = M / 2 + 2 * q;
+      float2 o0 = z[m], o1 = z[m + 1];
+      if (swap) {
+        o0 = crossfade_pair(o0, z2[m], 4 * q, step, M);
+        o1 = crossfade_pair(o1, z2[m + 1], 4 * q + 2, step, M);
+      }
+      reinterpret_cast<float4*>(y)[q] = make_float4(o0.x, o0.y, o1.x, o1.y);
     }
-    if (y_vec) {
-      reinterpret_cast<float2*>(y)[i / 2] = o;
-    } else {
-      y[i] = o.x;
-      y[i + 1] = o.y;
+  } else {
+    for (int m = M / 2 + threadIdx.x; m < M; m += T) {
+      const int i = 2 * (m - M / 2);
+      float2 o = z[m];
+      if (swap) o = crossfade_pair(o, z2[m], i, step, M);
+      if (y_vec) {
+        reinterpret_cast<float2*>(y)[i / 2] = o;
+      } else {
+        y[i] = o.x;
+        y[i + 1] = o.y;
+      }
     }
   }
   if (epi.active) mix_epilogue<M, T>(epi, c);
