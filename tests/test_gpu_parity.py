@@ -275,6 +275,53 @@ def test_channel_counts_around_the_parameter_descriptor_limit(tan_ctx, C):
         c_.Release()
 
 
+def test_mixed_io_overloads_on_one_object_equal_host_only(tan_ctx):
+    """Host-row calls return once their heads have signalled, while the tail
+    behind them still runs; host-to-device and device calls in between reuse
+    the same staging rows. Alternating the overloads (single and multi-block
+    calls, an IR swap in the middle) gives the host-only samples exactly."""
+    import torch
+
+    g = H.rng(31)
+    C, B, L, nb = 5, 256, 6000, 24
+    x = H.noise(g, C, nb * B)
+    h0, h1 = H.irs(g, C, L), H.irs(g, C, L)
+    ref_conv = make(tan_ctx, L, B, C)
+    y0, codes = H.run_stream(ref_conv, x, B, {0: (h0, None), 11: (h1, None)}, per_call_blocks=1)
+    assert all(c == 0 for c in codes)
+    mix = make(tan_ctx, L, B, C)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros_like(xd)
+    y = np.zeros_like(y0)
+    plan = [(0, 1, "host"), (1, 3, "h2d"), (3, 6, "host"), (6, 7, "dev"), (7, 9, "host"), (9, 11, "h2d"),
+            (11, 12, "host"), (12, 15, "dev"), (15, 16, "h2d"), (16, 20, "host"), (20, 24, "dev")]
+    for k0, k1, kind in plan:
+        if k0 == 0:
+            assert mix.UpdateResponseTD(h0, L) == 0
+        if k0 == 11:
+            assert mix.UpdateResponseTD(h1, L) == 0
+        n = (k1 - k0) * B
+        xs = np.ascontiguousarray(x[:, k0 * B:k1 * B])
+        if kind == "host":
+            ys = np.zeros_like(xs)
+            rc, done = mix.Process(xs, ys, n)
+            y[:, k0 * B:k1 * B] = ys
+        elif kind == "h2d":
+            rc, done = mix.ProcessHostToDevice(xs, [yd[c, k0 * B:k1 * B] for c in range(C)], n)
+        else:
+            rc, done = mix.ProcessDevice([xd[c, k0 * B:k1 * B] for c in range(C)],
+                                         [yd[c, k0 * B:k1 * B] for c in range(C)], n)
+        assert rc == 0 and done == n
+    assert mix.Synchronize() == 0
+    yd_h = yd.cpu().numpy()
+    for k0, k1, kind in plan:
+        if kind != "host":
+            y[:, k0 * B:k1 * B] = yd_h[:, k0 * B:k1 * B]
+    assert np.array_equal(y, y0)
+    ref_conv.Release()
+    mix.Release()
+
+
 def test_multi_block_calls_equal_single_block_calls(tan_ctx):
     g = H.rng(8)
     C, B, L, nb = 2, 128, 4096, 40
