@@ -513,10 +513,15 @@ def run_ours(args):
 
         cp = serving.capacity(ctx, "plain", 4, 48000, 256, blocks=100)
         cb = serving.capacity(ctx, "batched", 4, 48000, 256, blocks=100)
+        c24 = serving.capacity(ctx, "batched", 4, 48000, 256, spectrum=eng.SPECTRUM_FP24, blocks=100)
         capacity = {"what": "max channels (sessions of 4 ch, IR 48000 = 1 s, block 256 @ 48 kHz) with p99 "
                             "block latency < 5.33 ms, host buffers, FP32",
                     "plain_fp32": cp["max_realtime_channels"], "batched_fp32": cb["max_realtime_channels"],
-                    "ratio": cb["max_realtime_channels"] / max(1, cp["max_realtime_channels"])}
+                    "ratio": cb["max_realtime_channels"] / max(1, cp["max_realtime_channels"]),
+                    "batched_fp24": c24["max_realtime_channels"],
+                    "fp24_what": "IR spectra and delay line stored in 24 bits (error vs FP64 about -100 dB, "
+                                 "tests/test_gpu_engine.py), FP32 accumulation",
+                    "ratio_fp24": c24["max_realtime_channels"] / max(1, cp["max_realtime_channels"])}
         # the MAC where its working set is far above L2: the batched engine's
         # block launch at the capacity found above
         rs = serving.mac_roofline(ctx, cb["max_realtime_channels"], 4, 48000, 256)

@@ -251,11 +251,14 @@ int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6],
  * ------------------------------------------------------------------------- */
 typedef struct tanb_engine tanb_engine;
 
-enum { TANB_SPECTRUM_FP32 = 0, TANB_SPECTRUM_FP16 = 1, TANB_SPECTRUM_BF16 = 2 };
+enum { TANB_SPECTRUM_FP32 = 0, TANB_SPECTRUM_FP16 = 1, TANB_SPECTRUM_BF16 = 2, TANB_SPECTRUM_FP24 = 3 };
 
 /* Creates an engine for blocks of `block` samples (power of two in
- * [128, 2048]). IR spectra are stored as `spectrum` (FP16 / BF16 with a
- * power-of-two scale per partition; accumulation is FP32). Sessions are
+ * [128, 2048]). IR spectra are stored as `spectrum`: FP16 / BF16 with a
+ * power-of-two scale per partition, or FP24 (engine only: FP32 rounded to a
+ * 15-bit fraction, 6 bytes per complex bin) for the IR spectra AND the input
+ * delay line, a quarter fewer streamed bytes than FP32 at an output error near
+ * -100 dB; accumulation is FP32 in every case. Sessions are
  * admitted while their device memory fits in `budget_bytes`; at most
  * `max_channels` channel slots. `partitions_per_item` (0: 32) sets the size of
  * the tail's work items. */

@@ -615,7 +615,8 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
           x = v->stage_in(v->h_stage, b, c);
         } else if (in_mem == Mem::Host) {
           x = in[c] ? v->stage_in(v->h_stage, b, c) : nullptr;
-          if (run[c] && in[c]) std::memcpy(v->stage_in(v->h_stage, b, c), in[c] + blk * B, B * sizeof(float));
+          if (run[c] && in[c])
+            tanb::copy_rows_for_device(v->stage_in(v->h_stage, b, c), in[c] + blk * B, B * sizeof(float));
         } else {
           x = in[c] ? in[c] + blk * B : nullptr;
         }
@@ -650,6 +651,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     }
     nb = filled;
     if (nb == 0) break;
+    tanb::copy_for_device_fence();  // staged rows are visible before the launches
     // ev_stage guards the host descriptor tables until their upload has run;
     // ev_out guards the host staging rows until the heads have read and
     // written them. A call on device rows with parameter descriptors uses

@@ -160,13 +160,16 @@ struct tanb_engine {
 
 namespace {
 
-size_t spec_bytes(int spec) { return spec == tanb::kSpecFP32 ? 8 : 4; }
+// Bytes per packed bin of an IR-spectrum row and of a delay-line row.
+size_t spec_bytes(int spec) { return spec == tanb::kSpecFP32 ? 8 : spec == tanb::kSpecFP24 ? 6 : 4; }
+size_t fdl_bytes(int spec) { return spec == tanb::kSpecFP24 ? 6 : 8; }
+bool spec_scaled(int spec) { return spec == tanb::kSpecFP16 || spec == tanb::kSpecBF16; }
 
 size_t session_bytes(const tanb_engine* e, int C, int P, int nitem) {
   const size_t B = e->B;
   size_t per = align_up(2 * (size_t)P * B * spec_bytes(e->spec));        // H
-  if (e->spec != tanb::kSpecFP32) per += align_up(2 * (size_t)P * 4);     // scales
-  per += align_up((size_t)P * B * 8);                                    // fdl
+  if (spec_scaled(e->spec)) per += align_up(2 * (size_t)P * 4);          // scales
+  per += align_up((size_t)P * B * fdl_bytes(e->spec));                   // fdl
   per += align_up(B * 4);                                                // prev
   per += align_up(4 * (size_t)nitem * B * 8);                            // partials
   return per * C;
@@ -314,7 +317,7 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   *out = nullptr;
   if (block < 128 || block > 2048 || (block & (block - 1)))
     return efail(TANB_INVALID_ARG, "engine block must be a power of two in [128, 2048]");
-  if (spectrum > tanb::kSpecBF16) return efail(TANB_INVALID_ARG, "unknown spectrum type %u", spectrum);
+  if (spectrum > tanb::kSpecFP24) return efail(TANB_INVALID_ARG, "unknown spectrum type %u", spectrum);
   if (max_channels == 0) return efail(TANB_INVALID_ARG, "max_channels == 0");
   if (partitions_per_item == 0) partitions_per_item = 32;
   tanb_engine* e = new tanb_engine();
@@ -428,12 +431,12 @@ int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_
     EngChan ch{};
     ch.H = base;
     base += align_up(2 * (size_t)s.P * B * spec_bytes(e->spec));
-    if (e->spec != tanb::kSpecFP32) {
+    if (spec_scaled(e->spec)) {
       ch.scale = reinterpret_cast<float*>(base);
       base += align_up(2 * (size_t)s.P * 4);
     }
     ch.fdl = reinterpret_cast<float2*>(base);
-    base += align_up((size_t)s.P * B * 8);
+    base += align_up((size_t)s.P * B * fdl_bytes(e->spec));
     ch.prev = reinterpret_cast<float*>(base);
     base += align_up(B * 4);
     ch.part = reinterpret_cast<float2*>(base);
@@ -582,8 +585,11 @@ int32_t tanb_engine_write_input(tanb_engine* e, uint32_t first_slot, const float
   const uint32_t tasks = (count + kRowsPerTask - 1) / kRowsPerTask;
   auto copy = [&](int t) {
     const uint32_t r0 = (uint32_t)t * kRowsPerTask, r1 = std::min(count, r0 + kRowsPerTask);
+    // streaming stores: the heads read these rows over the bus, and rows
+    // left dirty in the CPU caches are read back far more slowly
     for (uint32_t r = r0; r < r1; ++r)
-      std::memcpy(e->h_in + (size_t)(first_slot + r) * B, src + (size_t)r * ld, B * sizeof(float));
+      tanb::copy_rows_for_device(e->h_in + (size_t)(first_slot + r) * B, src + (size_t)r * ld, B * sizeof(float));
+    tanb::copy_for_device_fence();
   };
   if ((size_t)count * B * sizeof(float) >= (1u << 20))
     tanb::host_parallel_for((int)tasks, copy);
@@ -644,7 +650,7 @@ int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
   if (!e || !out) return efail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(e->mu);
   int64_t chans = 0, bytes = 0, block_bytes = 0;
-  const int64_t B = e->B, sb = (int64_t)spec_bytes(e->spec);
+  const int64_t B = e->B, sb = (int64_t)spec_bytes(e->spec), xb = (int64_t)fdl_bytes(e->spec);
   for (auto& kv : e->sessions) {
     const Session& s = kv.second;
     chans += s.C;
@@ -653,8 +659,8 @@ int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
     // partitions [2, P) of IR spectrum and delay line and write their partial
     // rows; the head reads input, history, the partial rows, partitions 0 and
     // 1 of the spectrum and X_{k-1}, and writes output, history and X_k
-    const int64_t tail = (s.P > 2 ? (int64_t)(s.P - 2) * B * (sb + 8) : 0) + (int64_t)s.nitem * B * 8;
-    const int64_t head = 4 * B * 4 + (int64_t)s.nitem * B * 8 + (s.P > 1 ? 2 * B * sb + B * 8 : B * sb) + B * 8;
+    const int64_t tail = (s.P > 2 ? (int64_t)(s.P - 2) * B * (sb + xb) : 0) + (int64_t)s.nitem * B * 8;
+    const int64_t head = 4 * B * 4 + (int64_t)s.nitem * B * 8 + (s.P > 1 ? 2 * B * sb + B * xb : B * sb) + B * xb;
     block_bytes += (int64_t)s.C * (tail + head);
   }
   out[0] = (int64_t)e->sessions.size();

@@ -6,7 +6,7 @@
 
 namespace tanb {
 
-enum { kSpecFP32 = 0, kSpecFP16 = 1, kSpecBF16 = 2 };
+enum { kSpecFP32 = 0, kSpecFP16 = 1, kSpecBF16 = 2, kSpecFP24 = 3 };
 
 // One channel slot of the engine's device channel table. Pointers and sizes
 // are written by the host when a session opens; cur / active / pending are

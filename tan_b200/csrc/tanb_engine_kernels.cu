@@ -69,6 +69,74 @@ __device__ __forceinline__ size_t spec_index(const EngChan& ch, int slot, int pa
   return ((size_t)slot * ch.P + part) * B;
 }
 
+// FP16 / BF16 spectra carry a power-of-two scale per partition.
+template <int SPEC>
+constexpr bool kScaled = SPEC == kSpecFP16 || SPEC == kSpecBF16;
+
+// 24-bit storage (kSpecFP24): an FP32 value with its mantissa rounded to
+// nearest even at 15 bits (sign, 8-bit exponent, 15-bit fraction). A row of M
+// packed bins is a plane of M uint32 (the upper 16 bits of re and im) followed
+// by a plane of M uint16 (the next 8 bits of re and im): 6 M bytes, aligned
+// 8- and 4-byte loads for two bins. Used for IR spectra and delay-line rows.
+__device__ __forceinline__ unsigned f24_encode(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u + 0x7Fu + ((u >> 8) & 1u)) >> 8;
+}
+__device__ __forceinline__ float f24_decode(unsigned hi16, unsigned lo8) {
+  return __uint_as_float((hi16 << 16) | (lo8 << 8));
+}
+template <int M>
+__device__ __forceinline__ float2 f24_bin(const void* row, int k) {
+  const unsigned hi = reinterpret_cast<const unsigned*>(row)[k];
+  const unsigned lo = reinterpret_cast<const unsigned short*>(static_cast<const char*>(row) + 4 * M)[k];
+  return make_float2(f24_decode(hi & 0xFFFFu, lo & 0xFFu), f24_decode(hi >> 16, lo >> 8));
+}
+template <int M>
+__device__ __forceinline__ void f24_put(void* row, int k, float2 v) {
+  const unsigned re = f24_encode(v.x), im = f24_encode(v.y);
+  reinterpret_cast<unsigned*>(row)[k] = (re >> 8) | ((im >> 8) << 16);
+  reinterpret_cast<unsigned short*>(static_cast<char*>(row) + 4 * M)[k] =
+      (unsigned short)((re & 0xFFu) | ((im & 0xFFu) << 8));
+}
+// bins 2u and 2u + 1
+template <int M>
+__device__ __forceinline__ void f24_unit(const void* row, int u, float2& a, float2& b) {
+  const uint2 hi = __ldg(reinterpret_cast<const uint2*>(row) + u);
+  const unsigned lo = __ldg(reinterpret_cast<const unsigned*>(static_cast<const char*>(row) + 4 * M) + u);
+  a = make_float2(f24_decode(hi.x & 0xFFFFu, lo & 0xFFu), f24_decode(hi.x >> 16, (lo >> 8) & 0xFFu));
+  b = make_float2(f24_decode(hi.y & 0xFFFFu, (lo >> 16) & 0xFFu), f24_decode(hi.y >> 16, lo >> 24));
+}
+template <int M>
+__device__ __forceinline__ const void* f24_row(const void* base, size_t row) {
+  return static_cast<const char*>(base) + row * (size_t)(6 * M);
+}
+template <int M>
+__device__ __forceinline__ void* f24_row(void* base, size_t row) {
+  return static_cast<char*>(base) + row * (size_t)(6 * M);
+}
+
+// Delay-line slot rows: FP32 float2[M], or 24-bit rows with kSpecFP24.
+template <int SPEC, int M>
+__device__ __forceinline__ float2 x_bin(const float2* fdl, int slot, int k) {
+  if constexpr (SPEC == kSpecFP24) return f24_bin<M>(f24_row<M>(fdl, slot), k);
+  else return fdl[(size_t)slot * M + k];
+}
+template <int SPEC, int M>
+__device__ __forceinline__ void x_put(float2* fdl, int slot, int k, float2 v) {
+  if constexpr (SPEC == kSpecFP24) f24_put<M>(f24_row<M>(fdl, slot), k, v);
+  else fdl[(size_t)slot * M + k] = v;
+}
+template <int SPEC, int M>
+__device__ __forceinline__ float4 x_unit(const float2* fdl, int slot, int u) {
+  if constexpr (SPEC == kSpecFP24) {
+    float2 a, b;
+    f24_unit<M>(f24_row<M>(fdl, slot), u, a, b);
+    return make_float4(a.x, a.y, b.x, b.y);
+  } else {
+    return __ldg(reinterpret_cast<const float4*>(fdl) + (size_t)slot * (M / 2) + u);
+  }
+}
+
 // ---------------------------------------------------------------------------
 template <int LOG2M, int SPEC>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T)
@@ -109,7 +177,7 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   }
   __syncthreads();
   float scale = 1.0f;
-  if constexpr (SPEC != kSpecFP32) {
+  if constexpr (kScaled<SPEC>) {
     float mx = 0.f;
     for (int k = threadIdx.x; k < M; k += T) mx = fmaxf(mx, fmaxf(fabsf(sm[k].x), fabsf(sm[k].y)));
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -132,16 +200,23 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
     if (threadIdx.x == 0) ch.scale[(size_t)u.slot * ch.P + part] = scale;
   }
   const float inv = 1.0f / scale;  // exact: power of two
-  for (int k = threadIdx.x; k < M; k += T)
-    SpecT<SPEC>::put(ch.H, spec_index(ch, u.slot, part, M) + k, make_float2(sm[k].x * inv, sm[k].y * inv));
+  if constexpr (SPEC == kSpecFP24) {
+    void* row = f24_row<M>(ch.H, (size_t)u.slot * ch.P + part);
+    for (int k = threadIdx.x; k < M; k += T) f24_put<M>(row, k, sm[k]);
+  } else {
+    for (int k = threadIdx.x; k < M; k += T)
+      SpecT<SPEC>::put(ch.H, spec_index(ch, u.slot, part, M) + k, make_float2(sm[k].x * inv, sm[k].y * inv));
+  }
 }
 
 // ---------------------------------------------------------------------------
 // Two packed bins (one float4 of a delay-line row) per unit; spectra are float4
 // (FP32) or uint2 (two half2 / bfloat162) per unit.
-template <int SPEC>
+template <int SPEC, int M>
 __device__ __forceinline__ void load_h2(const void* H, size_t idx2, float2& a, float2& b) {
-  if constexpr (SPEC == kSpecFP32) {
+  if constexpr (SPEC == kSpecFP24) {
+    f24_unit<M>(f24_row<M>(H, idx2 / (M / 2)), (int)(idx2 % (M / 2)), a, b);
+  } else if constexpr (SPEC == kSpecFP32) {
     const float4 v = __ldg(reinterpret_cast<const float4*>(H) + idx2);
     a = make_float2(v.x, v.y);
     b = make_float2(v.z, v.w);
@@ -157,15 +232,19 @@ __device__ __forceinline__ void load_h2(const void* H, size_t idx2, float2& a, f
   }
 }
 
-template <int SPEC>
-__device__ __forceinline__ float2 spec_bin(const EngChan& ch, int slot, int part, int M, int k) {
-  float2 h = SpecT<SPEC>::get(ch.H, spec_index(ch, slot, part, M) + k);
-  if constexpr (SPEC != kSpecFP32) {
-    const float s = ch.scale[(size_t)slot * ch.P + part];
-    h.x *= s;
-    h.y *= s;
+template <int SPEC, int M>
+__device__ __forceinline__ float2 spec_bin(const EngChan& ch, int slot, int part, int k) {
+  if constexpr (SPEC == kSpecFP24) {
+    return f24_bin<M>(f24_row<M>(ch.H, (size_t)slot * ch.P + part), k);
+  } else {
+    float2 h = SpecT<SPEC>::get(ch.H, spec_index(ch, slot, part, M) + k);
+    if constexpr (kScaled<SPEC>) {
+      const float s = ch.scale[(size_t)slot * ch.P + part];
+      h.x *= s;
+      h.y *= s;
+    }
+    return h;
   }
-  return h;
 }
 
 // Partial-sum row of a channel: rows [2 parity][2 mode][nitem][M] float2; mode
@@ -182,9 +261,8 @@ __device__ __forceinline__ void eng_item(const EngChan& ch, const EngItem& w, in
                                          int mode) {
   constexpr int M = 1 << LOG2M, U = M / 2, T = M / 4, D = 2;
   const int P = ch.P;
-  const float4* F = reinterpret_cast<const float4*>(ch.fdl);
   const size_t hb = ((size_t)slot * P * M) / 2;  // unit index of (slot, partition 0)
-  const float* sc = (SPEC != kSpecFP32) ? ch.scale + (size_t)slot * P : nullptr;
+  const float* sc = kScaled<SPEC> ? ch.scale + (size_t)slot * P : nullptr;
   const int u0 = threadIdx.x, u1 = threadIdx.x + T;
   const bool dc = (u0 == 0);
   float2 a0 = make_float2(0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
@@ -196,18 +274,17 @@ __device__ __forceinline__ void eng_item(const EngChan& ch, const EngItem& w, in
     float s[D];
 #pragma unroll
     for (int q = 0; q < D; ++q) {
-      const size_t row = (size_t)fs * U;
-      f0[q] = __ldg(F + row + u0);
-      f1[q] = __ldg(F + row + u1);
+      f0[q] = x_unit<SPEC, M>(ch.fdl, fs, u0);
+      f1[q] = x_unit<SPEC, M>(ch.fdl, fs, u1);
       const size_t hrow = hb + (size_t)(i + q) * U;
-      load_h2<SPEC>(ch.H, hrow + u0, p0[q], q0[q]);
-      load_h2<SPEC>(ch.H, hrow + u1, p1[q], q1[q]);
-      s[q] = (SPEC != kSpecFP32) ? __ldg(sc + i + q) : 1.f;
+      load_h2<SPEC, M>(ch.H, hrow + u0, p0[q], q0[q]);
+      load_h2<SPEC, M>(ch.H, hrow + u1, p1[q], q1[q]);
+      s[q] = kScaled<SPEC> ? __ldg(sc + i + q) : 1.f;
       fs = (fs + 1 == P) ? 0 : fs + 1;
     }
 #pragma unroll
     for (int q = 0; q < D; ++q) {
-      if (SPEC != kSpecFP32) {
+      if (kScaled<SPEC>) {
         p0[q].x *= s[q]; p0[q].y *= s[q]; q0[q].x *= s[q]; q0[q].y *= s[q];
         p1[q].x *= s[q]; p1[q].y *= s[q]; q1[q].x *= s[q]; q1[q].y *= s[q];
       }
@@ -220,13 +297,12 @@ __device__ __forceinline__ void eng_item(const EngChan& ch, const EngItem& w, in
     }
   }
   for (; i < w.i1; ++i) {
-    const size_t row = (size_t)fs * U;
-    const float4 g0 = __ldg(F + row + u0), g1 = __ldg(F + row + u1);
+    const float4 g0 = x_unit<SPEC, M>(ch.fdl, fs, u0), g1 = x_unit<SPEC, M>(ch.fdl, fs, u1);
     float2 pa, qa, pb, qb;
     const size_t hrow = hb + (size_t)i * U;
-    load_h2<SPEC>(ch.H, hrow + u0, pa, qa);
-    load_h2<SPEC>(ch.H, hrow + u1, pb, qb);
-    if (SPEC != kSpecFP32) {
+    load_h2<SPEC, M>(ch.H, hrow + u0, pa, qa);
+    load_h2<SPEC, M>(ch.H, hrow + u1, pb, qb);
+    if (kScaled<SPEC>) {
       const float s = __ldg(sc + i);
       pa.x *= s; pa.y *= s; qa.x *= s; qa.y *= s;
       pb.x *= s; pb.y *= s; qb.x *= s; qb.y *= s;
@@ -276,8 +352,7 @@ __device__ __forceinline__ void eng_head(const EngChan& ch, float2* sm, const fl
   for (int n = threadIdx.x; n < M / 2; n += T) reinterpret_cast<float2*>(ch.prev)[n] = z[n + M / 2];
   fft_inplace<LOG2M, false>(z, tw);
 
-  float2* F = ch.fdl + (size_t)cur * M;
-  const float2* Fp = ch.fdl + (size_t)ch.cur * M;  // X_{k-1}: partition 1
+  // X_k goes into delay-line slot cur; X_{k-1} (partition 1) is in ch.cur
   const float inv_n = 1.0f / (float)(2 * M);
   const float2* pa = part_row(ch, parity, 0, 0, M);
   const float2* pb = part_row(ch, parity, 1, 0, M);
@@ -296,39 +371,39 @@ __device__ __forceinline__ void eng_head(const EngChan& ch, float2* sm, const fl
       }
     }
     if (P > 1) {
-      const float2 xk = Fp[k], xm = Fp[km];
-      const float2 hk = spec_bin<SPEC>(ch, slot_old, 1, M, k);
+      const float2 xk = x_bin<SPEC, M>(ch.fdl, ch.cur, k), xm = x_bin<SPEC, M>(ch.fdl, ch.cur, km);
+      const float2 hk = spec_bin<SPEC, M>(ch, slot_old, 1, k);
       if (k == 0) {
         tk = c_mac_dc(tk, xk, hk);
-        if (swap) uk = c_mac_dc(uk, xk, spec_bin<SPEC>(ch, slot_new, 1, M, 0));
+        if (swap) uk = c_mac_dc(uk, xk, spec_bin<SPEC, M>(ch, slot_new, 1, 0));
       } else {
         tk = c_mac(tk, xk, hk);
-        tm = c_mac(tm, xm, spec_bin<SPEC>(ch, slot_old, 1, M, km));
+        tm = c_mac(tm, xm, spec_bin<SPEC, M>(ch, slot_old, 1, km));
         if (swap) {
-          uk = c_mac(uk, xk, spec_bin<SPEC>(ch, slot_new, 1, M, k));
-          um = c_mac(um, xm, spec_bin<SPEC>(ch, slot_new, 1, M, km));
+          uk = c_mac(uk, xk, spec_bin<SPEC, M>(ch, slot_new, 1, k));
+          um = c_mac(um, xm, spec_bin<SPEC, M>(ch, slot_new, 1, km));
         }
       }
     }
     if (k == 0) {
       const float2 X = rfft_post_dc(z[0]);
-      F[0] = X;
-      z[0] = irfft_pre_dc(c_mac_dc(tk, X, spec_bin<SPEC>(ch, slot_old, 0, M, 0)), inv_n);
-      if (swap) z2[0] = irfft_pre_dc(c_mac_dc(uk, X, spec_bin<SPEC>(ch, slot_new, 0, M, 0)), inv_n);
+      x_put<SPEC, M>(ch.fdl, cur, 0, X);
+      z[0] = irfft_pre_dc(c_mac_dc(tk, X, spec_bin<SPEC, M>(ch, slot_old, 0, 0)), inv_n);
+      if (swap) z2[0] = irfft_pre_dc(c_mac_dc(uk, X, spec_bin<SPEC, M>(ch, slot_new, 0, 0)), inv_n);
     } else {
       const float2 wk = __ldg(tw + k), wm = __ldg(tw + km);
       const float2 a = z[k], b = z[km];
       const float2 Xk = rfft_post(a, b, wk);
       const float2 Xm = rfft_post(b, a, wm);
-      F[k] = Xk;
-      if (km != k) F[km] = Xm;
-      const float2 Ak = c_mac(tk, Xk, spec_bin<SPEC>(ch, slot_old, 0, M, k));
-      const float2 Am = c_mac(tm, Xm, spec_bin<SPEC>(ch, slot_old, 0, M, km));
+      x_put<SPEC, M>(ch.fdl, cur, k, Xk);
+      if (km != k) x_put<SPEC, M>(ch.fdl, cur, km, Xm);
+      const float2 Ak = c_mac(tk, Xk, spec_bin<SPEC, M>(ch, slot_old, 0, k));
+      const float2 Am = c_mac(tm, Xm, spec_bin<SPEC, M>(ch, slot_old, 0, km));
       z[k] = irfft_pre(Ak, Am, wk, inv_n);
       if (km != k) z[km] = irfft_pre(Am, Ak, wm, inv_n);
       if (swap) {
-        const float2 Bk = c_mac(uk, Xk, spec_bin<SPEC>(ch, slot_new, 0, M, k));
-        const float2 Bm = c_mac(um, Xm, spec_bin<SPEC>(ch, slot_new, 0, M, km));
+        const float2 Bk = c_mac(uk, Xk, spec_bin<SPEC, M>(ch, slot_new, 0, k));
+        const float2 Bm = c_mac(um, Xm, spec_bin<SPEC, M>(ch, slot_new, 0, km));
         z2[k] = irfft_pre(Bk, Bm, wk, inv_n);
         if (km != k) z2[km] = irfft_pre(Bm, Bk, wm, inv_n);
       }
@@ -443,7 +518,8 @@ cudaError_t attrs_all() {
   cudaError_t e;
   if ((e = attrs_t<LOG2M, kSpecFP32>()) != cudaSuccess) return e;
   if ((e = attrs_t<LOG2M, kSpecFP16>()) != cudaSuccess) return e;
-  return attrs_t<LOG2M, kSpecBF16>();
+  if ((e = attrs_t<LOG2M, kSpecBF16>()) != cudaSuccess) return e;
+  return attrs_t<LOG2M, kSpecFP24>();
 }
 
 template <int LOG2M, int SPEC>
@@ -476,18 +552,23 @@ cudaError_t commit_t(const EngChan* chans, const EngItem* items, int item0, int 
     case 7 * 4 + 0: return FN<7, 0>(__VA_ARGS__);                         \
     case 7 * 4 + 1: return FN<7, 1>(__VA_ARGS__);                         \
     case 7 * 4 + 2: return FN<7, 2>(__VA_ARGS__);                         \
+    case 7 * 4 + 3: return FN<7, 3>(__VA_ARGS__);                         \
     case 8 * 4 + 0: return FN<8, 0>(__VA_ARGS__);                         \
     case 8 * 4 + 1: return FN<8, 1>(__VA_ARGS__);                         \
     case 8 * 4 + 2: return FN<8, 2>(__VA_ARGS__);                         \
+    case 8 * 4 + 3: return FN<8, 3>(__VA_ARGS__);                         \
     case 9 * 4 + 0: return FN<9, 0>(__VA_ARGS__);                         \
     case 9 * 4 + 1: return FN<9, 1>(__VA_ARGS__);                         \
     case 9 * 4 + 2: return FN<9, 2>(__VA_ARGS__);                         \
+    case 9 * 4 + 3: return FN<9, 3>(__VA_ARGS__);                         \
     case 10 * 4 + 0: return FN<10, 0>(__VA_ARGS__);                       \
     case 10 * 4 + 1: return FN<10, 1>(__VA_ARGS__);                       \
     case 10 * 4 + 2: return FN<10, 2>(__VA_ARGS__);                       \
+    case 10 * 4 + 3: return FN<10, 3>(__VA_ARGS__);                       \
     case 11 * 4 + 0: return FN<11, 0>(__VA_ARGS__);                       \
     case 11 * 4 + 1: return FN<11, 1>(__VA_ARGS__);                       \
     case 11 * 4 + 2: return FN<11, 2>(__VA_ARGS__);                       \
+    case 11 * 4 + 3: return FN<11, 3>(__VA_ARGS__);                       \
     default: return cudaErrorInvalidValue;                                \
   }
 

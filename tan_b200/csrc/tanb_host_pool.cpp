@@ -109,9 +109,12 @@ void host_parallel_for(int n, const std::function<void(int)>& fn) {
 
 int host_pool_threads() { return pool().threads(); }
 
-void copy_for_device(void* dst, const void* src, size_t bytes) {
+namespace {
+
+// Non-temporal copy without a fence (x86-64); false if not applicable.
+bool stream_copy(void* dst, const void* src, size_t bytes, size_t min_bytes) {
 #if defined(__x86_64__)
-  if (bytes >= 4096) {
+  if (bytes >= min_bytes) {
     auto* d = static_cast<uint8_t*>(dst);
     auto* s = static_cast<const uint8_t*>(src);
     const size_t lead = (16 - (reinterpret_cast<uintptr_t>(d) & 15)) & 15;
@@ -131,11 +134,33 @@ void copy_for_device(void* dst, const void* src, size_t bytes) {
       _mm_stream_si128(reinterpret_cast<__m128i*>(d + i + 48), e);
     }
     std::memcpy(d + body, s + body, bytes - body);
-    _mm_sfence();  // the stores are visible before anything this thread does next
-    return;
+    return true;
   }
 #endif
-  std::memcpy(dst, src, bytes);
+  (void)dst;
+  (void)src;
+  (void)bytes;
+  (void)min_bytes;
+  return false;
+}
+
+}  // namespace
+
+void copy_for_device(void* dst, const void* src, size_t bytes) {
+  if (stream_copy(dst, src, bytes, 4096))
+    copy_for_device_fence();  // the stores are visible before anything this thread does next
+  else
+    std::memcpy(dst, src, bytes);
+}
+
+void copy_rows_for_device(void* dst, const void* src, size_t bytes) {
+  if (!stream_copy(dst, src, bytes, 256)) std::memcpy(dst, src, bytes);
+}
+
+void copy_for_device_fence() {
+#if defined(__x86_64__)
+  _mm_sfence();
+#endif
 }
 
 }  // namespace tanb

@@ -23,4 +23,9 @@ int host_pool_threads();
 // 2.2x slower end to end); non-temporal stores leave nothing in the cache.
 void copy_for_device(void* dst, const void* src, size_t bytes);
 
+// The same for many short rows: non-temporal stores from 256 bytes on and no
+// fence; the thread calls copy_for_device_fence() once after its last row.
+void copy_rows_for_device(void* dst, const void* src, size_t bytes);
+void copy_for_device_fence();
+
 }  // namespace tanb

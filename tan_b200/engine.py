@@ -16,6 +16,7 @@ from .convolution import AMF_OK, TANContext, TANError, lib
 SPECTRUM_FP32 = 0
 SPECTRUM_FP16 = 1
 SPECTRUM_BF16 = 2
+SPECTRUM_FP24 = 3  # IR spectra and delay line in 24 bits (engine only)
 
 
 class Session:

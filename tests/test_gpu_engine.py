@@ -2,8 +2,8 @@
 lengths (uneven partition counts) processed together must give, per session,
 the same output as that session alone through the single-object path
 (tolerance 1e-5 x rms), also when sessions open and close mid-stream; FP16 /
-BF16 spectra are measured against the FP64 statement in dB; admission is by
-the device-memory budget."""
+BF16 spectra and the 24-bit form (spectra and delay line) are measured
+against the FP64 statement in dB; admission is by the device-memory budget."""
 import numpy as np
 import pytest
 
@@ -83,6 +83,27 @@ def test_engine_mix_equals_alone(tan_ctx):
     engine.release()
 
 
+def test_engine_fp24_mix_equals_each_session_alone(tan_ctx):
+    """24-bit spectra and delay line: each session's samples in the mix are the
+    samples of that session alone in its own FP24 engine, bit for bit, and
+    within -90 dB of the FP64 statement."""
+    g = H.rng(36)
+    B, nb = 256, 30
+    specs = [(2, 3000, 0, [0, 17]), (1, 20000, 0, [0, 9]), (3, 65536, 3, [0, 11]), (2, 256, 0, [0, 20])]
+    sessions = make_sessions(g, B, specs, nb)
+    engine = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP24, budget_bytes=1 << 30, max_channels=64, partitions_per_item=16)
+    outs = run_engine(engine, sessions, nb)
+    engine.release()
+    for s, y in zip(sessions, outs):
+        solo = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP24, budget_bytes=1 << 28, max_channels=8, partitions_per_item=16)
+        ya = run_engine(solo, [dict(s, start=0)], nb - s["start"])[0]
+        solo.release()
+        assert np.array_equal(y, ya)
+        exp = fp64.stream_fp64(s["x"], B, [(k, {c: ir[c] for c in range(s["C"])}) for k, ir in s["events"].items()])
+        for c in range(s["C"]):
+            assert fp64.error_db(y[c], exp[c]) < -90
+
+
 def test_engine_churn_does_not_disturb_other_sessions(tan_ctx):
     g = H.rng(32)
     B, nb = 256, 36
@@ -100,7 +121,8 @@ def test_engine_churn_does_not_disturb_other_sessions(tan_ctx):
     engine.release()
 
 
-@pytest.mark.parametrize("spectrum,limit_db", [(eng.SPECTRUM_FP16, -60.0), (eng.SPECTRUM_BF16, -40.0)])
+@pytest.mark.parametrize("spectrum,limit_db", [(eng.SPECTRUM_FP16, -60.0), (eng.SPECTRUM_BF16, -40.0),
+                                               (eng.SPECTRUM_FP24, -90.0)])
 def test_engine_reduced_precision_spectra_error_db(tan_ctx, spectrum, limit_db):
     g = H.rng(33 + spectrum)
     B, nb = 256, 24

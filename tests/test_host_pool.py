@@ -2,9 +2,9 @@
 compiler and driven without a GPU: every index runs exactly once for any job
 size, jobs from several threads at once do not mix, and a child forked after
 the pool started runs its jobs serially instead of waiting on threads it does
-not have. copy_for_device (the streaming copy into staging memory) copies every
-byte for any size and any source / destination alignment, and writes nothing
-outside the destination range."""
+not have. copy_for_device and copy_rows_for_device (the streaming copies into
+staging memory) copy every byte for any size and any source / destination
+alignment, and write nothing outside the destination range."""
 import os
 import shutil
 import subprocess
@@ -35,11 +35,16 @@ static int check(int n) {
 static int check_copy() {
   std::vector<unsigned char> src(70000), dst(70000 + 64);
   for (size_t i = 0; i < src.size(); ++i) src[i] = (unsigned char)(i * 131u + 7u);
-  for (size_t n : {0u, 1u, 15u, 4095u, 4096u, 4097u, 4160u, 65536u + 13u})
+  for (size_t n : {0u, 1u, 15u, 255u, 256u, 300u, 4095u, 4096u, 4097u, 4160u, 65536u + 13u})
     for (int so = 0; so < 3; ++so)
       for (int doff = 0; doff < 19; doff += 3) {
         std::fill(dst.begin(), dst.end(), (unsigned char)0xA5);
-        tanb::copy_for_device(dst.data() + 16 + doff, src.data() + so, n);
+        if (so == 1) {
+          tanb::copy_rows_for_device(dst.data() + 16 + doff, src.data() + so, n);
+          tanb::copy_for_device_fence();
+        } else {
+          tanb::copy_for_device(dst.data() + 16 + doff, src.data() + so, n);
+        }
         for (size_t i = 0; i < dst.size(); ++i) {
           const bool in = i >= (size_t)(16 + doff) && i < 16 + doff + n;
           const unsigned char want = in ? src[so + i - 16 - doff] : (unsigned char)0xA5;
