@@ -148,7 +148,7 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
             "deadline_misses": int((lat > deadline_ms).sum()), "concurrent_channels_mean": float(np.mean(chans)),
             "concurrent_channels_max": int(np.max(chans)), "admitted": admitted, "refused": refused,
             "control_errors": errors[:5], "arena_bytes_end": info["arena_bytes"],
-            "spectrum": ["fp32", "fp16", "bf16"][spectrum]}
+            "spectrum": ["fp32", "fp16", "bf16", "fp24"][spectrum]}
 
 
 def _block_latencies_batched(ctx, nsess, C, L, block, spectrum, blocks, g, pool):
@@ -290,7 +290,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--seconds", type=float, default=30.0)
     ap.add_argument("--rate", type=float, default=20.0)
-    ap.add_argument("--spectrum", choices=["fp32", "fp16", "bf16"], default="fp32")
+    ap.add_argument("--spectrum", choices=["fp32", "fp16", "bf16", "fp24"], default="fp32")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--capacity", action="store_true")
     ap.add_argument("--form", choices=["batched", "plain"], default="batched")
@@ -299,7 +299,8 @@ def main():
     ap.add_argument("--mac-roofline", type=int, default=0, metavar="CHANNELS",
                     help="time the engine's block launch with this many resident channels")
     a = ap.parse_args()
-    spec = {"fp32": eng.SPECTRUM_FP32, "fp16": eng.SPECTRUM_FP16, "bf16": eng.SPECTRUM_BF16}[a.spectrum]
+    spec = {"fp32": eng.SPECTRUM_FP32, "fp16": eng.SPECTRUM_FP16, "bf16": eng.SPECTRUM_BF16,
+            "fp24": eng.SPECTRUM_FP24}[a.spectrum]
     ctx = cv.TANContext(0)
     if a.mac_roofline:
         r = mac_roofline(ctx, a.mac_roofline, a.channels, a.ir_length, spectrum=spec)

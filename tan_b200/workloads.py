@@ -96,7 +96,8 @@ def cfg3(ctx, quick=False):
     refs = {int(c): _conv64(x[c], irs[c]) for c in sample}
     out = {"config": "cfg3", "channels": C, "block": B, "ir_lengths": [int(lens.min()), int(np.median(lens)),
                                                                        int(lens.max())], "blocks": nb}
-    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp16", eng.SPECTRUM_FP16), ("bf16", eng.SPECTRUM_BF16)):
+    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp24", eng.SPECTRUM_FP24), ("fp16", eng.SPECTRUM_FP16),
+                       ("bf16", eng.SPECTRUM_BF16)):
         e = eng.Engine(ctx, B, spec, budget_bytes=60 << 30, max_channels=C)
         sess = []
         for c in range(C):
