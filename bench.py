@@ -179,7 +179,7 @@ def cpu_baseline(sample_s, threads=None):
     from oracle import ref
 
     threads = threads or os.cpu_count()
-    nb_max = 4000
+    nb_max = 100000  # the time bound (--cpu-sample-s) ends the sample first
     x, irs = make_inputs(0)
     g = np.random.Generator(np.random.PCG64(SEED + 7))
     xb = g.uniform(-1.0, 1.0, (C, 64 * B)).astype(np.float32)
