@@ -244,7 +244,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def read_traffic(name="tail_kernel_cfg2.txt"):
+def read_traffic(name="tail_kernel_64ch_b512_ir65536.txt"):
     """dram bytes per launch of the dominant kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
@@ -552,8 +552,8 @@ def run_ours(args):
             "l2": "flushed before every timed step (256 MiB write + 256 MiB read on the object's stream)",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": read_traffic("eng_block_kernel_cfg2.txt" if best is engine_path
-                                                 else "tail_kernel_cfg2.txt"),
+                         "traffic": read_traffic("eng_block_kernel_64ch_b512_ir65536.txt" if best is engine_path
+                                                 else "tail_kernel_64ch_b512_ir65536.txt"),
                          "kernel": "eng_block_kernel (heads + partition MAC work items, one launch per block)"
                          if best is engine_path else "tail_kernel (partition MAC)",
                          "peak_source": f"{peak_kind} hbm_gbs",

@@ -1,12 +1,12 @@
 """Measurements of the path on each benchmark configuration (seeded synthetic
 inputs with the configurations' shapes; no public dataset is involved).
 
-    python -m tan_b200.workloads cfg1|cfg3|cfg4|nu-tune|pipeline [--quick]
+    python -m tan_b200.workloads dropin_small|engine_uneven|nonuniform_long|nu-tune|pipeline [--quick]
 
-cfg1  drop-in TANConvolution, 2 ch, B=1024, IR 8192, 200 blocks, FP32
-cfg3  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096..262144,
-      input at -6 dBFS, FP32 / FP16 / BF16 spectra; error vs FP64 per channel
-cfg4  non-uniform partitions, 256 ch, IR 2^20, base block 128, schedule from the
+dropin_small  drop-in TANConvolution, 2 ch, B=1024, IR 8192, 200 blocks, FP32
+engine_uneven  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096..262144,
+      input at -6 dBFS, FP32 / FP24 / FP16 / BF16 spectra; error vs FP64 per channel
+nonuniform_long  non-uniform partitions, 256 ch, IR 2^20, base block 128, schedule from the
       autotuner, FP32 / FP16; error vs FP64 on sampled channels
 pipeline  the sample pipeline (int16 stereo sources, per-ear convolution, mix,
       int16 out): fused call vs separate GPU calls vs the CPU restatement
@@ -56,7 +56,7 @@ def _pct(a):
     return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "max": float(a.max())}
 
 
-def cfg1(ctx, quick=False):
+def dropin_small(ctx, quick=False):
     g = _rng(0)
     C, B, L, nb = 2, 1024, 8192, 200
     x = g.uniform(-1, 1, (C, nb * B)).astype(np.float32)
@@ -80,12 +80,12 @@ def cfg1(ctx, quick=False):
         ref = _conv64(x[c], h[c])
         ref[:B] *= np.arange(B) / B
         err.append(_db(y[c], ref))
-    return {"config": "cfg1", "channels": C, "block": B, "ir": L, "blocks": nb,
+    return {"config": "dropin_small", "channels": C, "block": B, "ir": L, "blocks": nb,
             "gsamples_per_s_host": C * B * nb / (sum(lat) / 1e3) / 1e9, "latency_ms": _pct(lat),
             "error_db_vs_fp64": err}
 
 
-def cfg3(ctx, quick=False):
+def engine_uneven(ctx, quick=False):
     g = _rng(2)
     C, B = (256 if quick else 1024), 256
     nb = 48
@@ -94,7 +94,7 @@ def cfg3(ctx, quick=False):
     irs = [_ir(g, int(L), float(g.uniform(0.2, 3.0))) for L in lens]
     sample = g.choice(C, 32, replace=False)
     refs = {int(c): _conv64(x[c], irs[c]) for c in sample}
-    out = {"config": "cfg3", "channels": C, "block": B, "ir_lengths": [int(lens.min()), int(np.median(lens)),
+    out = {"config": "engine_uneven", "channels": C, "block": B, "ir_lengths": [int(lens.min()), int(np.median(lens)),
                                                                        int(lens.max())], "blocks": nb}
     for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp24", eng.SPECTRUM_FP24), ("fp16", eng.SPECTRUM_FP16),
                        ("bf16", eng.SPECTRUM_BF16)):
@@ -169,7 +169,7 @@ def tune_nu(ctx, C, L, B0, max_blocks=(1024, 2048, 4096, 8192), mids=(1, 2), spe
     return res
 
 
-def cfg4(ctx, quick=False):
+def nonuniform_long(ctx, quick=False):
     g = _rng(3)
     C, L, B0 = (64 if quick else 256), 1 << 20, 128
     deadline = 1000.0 * B0 / FS
@@ -181,7 +181,7 @@ def cfg4(ctx, quick=False):
     irs = np.stack([_ir(g, L, 8.0) for _ in range(C)])
     sample = [0, C // 2, C - 1]
     refs = {c: _conv64(x[c], irs[c]) for c in sample}
-    out = {"config": "cfg4", "channels": C, "ir": L, "base_block": B0, "blocks": nb, "deadline_ms": deadline,
+    out = {"config": "nonuniform_long", "channels": C, "ir": L, "base_block": B0, "blocks": nb, "deadline_ms": deadline,
            "autotuner": [{"levels": r["levels"], "mean_ms": r["mean_ms"], "max_ms": r["max_ms"]} for r in cands],
            "schedule": best["levels"]}
     for name, spec in (("fp32", 0), ("fp16", 1)):
@@ -292,14 +292,15 @@ def pipeline(ctx, quick=False, S=32, B=256, L=48000):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("which", choices=["cfg1", "cfg3", "cfg4", "nu-tune", "pipeline"])
+    ap.add_argument("which", choices=["dropin_small", "engine_uneven", "nonuniform_long", "nu-tune", "pipeline"])
     ap.add_argument("--quick", action="store_true")
     a = ap.parse_args()
     ctx = cv.TANContext(0)
     if a.which == "nu-tune":
         r = tune_nu(ctx, 64 if a.quick else 256, 1 << 20, 128)
     else:
-        r = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4, "pipeline": pipeline}[a.which](ctx, a.quick)
+        r = {"dropin_small": dropin_small, "engine_uneven": engine_uneven, "nonuniform_long": nonuniform_long,
+             "pipeline": pipeline}[a.which](ctx, a.quick)
     print(json.dumps(r))
 
 

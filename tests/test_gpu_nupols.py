@@ -85,7 +85,7 @@ def test_nu_rejects_schedules_that_add_latency(tan_ctx):
 
 
 @pytest.mark.parametrize("C,levels,nb", [
-    (2, [(128, 2), (256, 1), (512, 1), (1024, 1), (2048, 1), (4096, 8)], 260),   # cfg4's shape, every level reached
+    (2, [(128, 2), (256, 1), (512, 1), (1024, 1), (2048, 1), (4096, 8)], 260),   # the 2^20-tap 256-channel schedule's shape, every level reached
     (2, [(128, 2), (256, 2), (512, 2), (1024, 2), (2048, 6)], 200),
     (64, [(128, 2), (256, 1), (512, 1), (1024, 5)], 64),
     (2, [(128, 2), (256, 1), (512, 1), (1024, 1), (2048, 1), (4096, 1), (8192, 4)], 400),

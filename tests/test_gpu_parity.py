@@ -42,7 +42,7 @@ def test_known_answer_delta_irs(tan_ctx):
     conv.Release()
 
 
-def test_cfg1_parity_with_restatement(tan_ctx):
+def test_two_channels_b1024_ir8192_parity_with_restatement(tan_ctx):
     """2 channels, B=1024, IR 8192 (8 partitions), 200 blocks, RT60 0.3 s."""
     g = H.rng(20261203 + 0)
     C, B, L, nb = 2, 1024, 8192, 200
@@ -61,7 +61,7 @@ def test_cfg1_parity_with_restatement(tan_ctx):
 
 
 def test_time_varying_swaps_parity(tan_ctx):
-    """cfg2 shape reduced in channels/blocks: B=512, IR 65536 (128 partitions),
+    """The 64-channel bench shape reduced in channels/blocks: B=512, IR 65536 (128 partitions),
     IR replaced every 32 blocks with a one-block crossfade."""
     g = H.rng(20261203 + 1)
     C, B, L, nb = 4, 512, 65536, 100
@@ -339,7 +339,7 @@ def test_multi_block_calls_equal_single_block_calls(tan_ctx):
     b.Release()
 
 
-def test_full_size_cfg2_properties(tan_ctx):
+def test_full_size_64ch_b512_ir65536_properties(tan_ctx):
     """64 channels, B=512, IR 65536: linearity and the delta-IR known answer at
     full size (size-independent properties; the oracle covers smaller sizes)."""
     g = H.rng(20261203 + 1)
