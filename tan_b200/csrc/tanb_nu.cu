@@ -17,9 +17,12 @@
 //   3. level 0's tail for block k+1;
 //   4. every level whose block completes: head (R2C, partition 0, tail, C2R,
 //      add into the output ring at its delayed position) and tail.
-// All kernels of a block are launched in level order; those of levels that
-// are not due exit at once, so the launch sequence is the same every block
-// (one CUDA graph). Contributions to a ring sample are added in a fixed order,
+// The kernels of a block are launched in level order, for the levels that are
+// due at that block only: with power-of-two block sizes the set of due levels
+// follows from the block index, so each set is one CUDA graph captured at
+// creation and the host launches the one for the block (the kernels check the
+// same condition and exit when their level is not due). Contributions to a
+// ring sample are added in a fixed order,
 // so results are deterministic. IR spectra are FP32, FP16 or BF16 with
 // per-partition power-of-two scales; accumulation is FP32.
 #include <cuda_bf16.h>
@@ -27,6 +30,7 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -420,7 +424,8 @@ struct tanb_nu {
   float* d_ir = nullptr;    // [C][L] staging for set_response
   long long k = 0;          // host mirror of the base block counter
   size_t dev_bytes = 0;
-  cudaGraphExec_t graph = nullptr;
+  // host-buffer block graphs, one per set of due levels (bit l: level l)
+  std::map<unsigned, cudaGraphExec_t> graphs;
   cudaEvent_t ev_out = nullptr;
 };
 
@@ -438,7 +443,8 @@ cudaError_t nu_alloc(tanb_nu* v, void** p, size_t bytes) {
 
 void nu_free(tanb_nu* v) {
   if (v->stream) cudaStreamSynchronize(v->stream);
-  if (v->graph) cudaGraphExecDestroy(v->graph);
+  for (auto& kv : v->graphs) cudaGraphExecDestroy(kv.second);
+  v->graphs.clear();
   for (void* p : v->allocs) cudaFree(p);
   v->allocs.clear();
   cudaFreeHost(v->h_in);
@@ -447,8 +453,20 @@ void nu_free(tanb_nu* v) {
   if (v->stream) cudaStreamDestroy(v->stream);
 }
 
-// Kernels of one base block in level order; input from `in` ([C][ld] or null).
-cudaError_t enqueue_nu_block(tanb_nu* v, const float* in, float* out, int ld, bool host) {
+// Levels whose block completes with base block k (bit l: level l; level 0,
+// whose block is the base block, always): N_l divides (k + 1) B0. With
+// power-of-two block sizes the pattern repeats every max N_l / B0 blocks.
+unsigned due_mask(const tanb::NuDev& d, long long k) {
+  unsigned m = 0;
+  for (int l = 0; l < d.nl; ++l)
+    if (((k + 1) * (long long)d.B0) % (1LL << d.lv[l].log2N) == 0) m |= 1u << l;
+  return m;
+}
+
+// Kernels of one base block in level order, for the levels in `due` (the
+// kernels check the same condition on the device counter); input from `in`
+// ([C][ld] or null).
+cudaError_t enqueue_nu_block(tanb_nu* v, const float* in, float* out, int ld, bool host, unsigned due) {
   const tanb::NuDev& d = v->d;
   cudaError_t r;
   if (host && (r = cudaMemcpyAsync(v->d_in, v->h_in, (size_t)d.C * d.B0 * sizeof(float), cudaMemcpyHostToDevice,
@@ -466,6 +484,7 @@ cudaError_t enqueue_nu_block(tanb_nu* v, const float* in, float* out, int ld, bo
   }
   if ((r = tanb::launch_nu_tail(d, 0, v->stream)) != cudaSuccess) return r;
   for (int l = 1; l < d.nl; ++l) {
+    if (!(due >> l & 1u)) continue;
     if ((r = tanb::launch_nu_head(d, l, nullptr, 0, v->stream)) != cudaSuccess) return r;
     if ((r = tanb::launch_nu_tail(d, l, v->stream)) != cudaSuccess) return r;
   }
@@ -473,21 +492,38 @@ cudaError_t enqueue_nu_block(tanb_nu* v, const float* in, float* out, int ld, bo
   return cudaGetLastError();
 }
 
-// The host-buffer block as one CUDA graph, captured once. Creation calls this
-// so that module loading, instantiation and the upload of the graph to the
-// device are not paid by the first audio block.
-cudaError_t ensure_graph(tanb_nu* v) {
-  if (v->graph) return cudaSuccess;
+// The host-buffer block as a CUDA graph holding only the due levels' kernels,
+// one graph per set of due levels, captured once. Creation calls this for
+// every set that one period of the schedule produces, so that module loading,
+// instantiation and the upload of the graphs to the device are not paid by
+// audio blocks.
+cudaError_t ensure_graph(tanb_nu* v, unsigned due) {
+  if (v->graphs.count(due)) return cudaSuccess;
   cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
   cudaError_t r = cudaStreamBeginCapture(v->stream, cudaStreamCaptureModeThreadLocal);
   if (r != cudaSuccess) return r;
-  r = enqueue_nu_block(v, v->d_in, v->d_out, v->d.B0, true);
+  r = enqueue_nu_block(v, v->d_in, v->d_out, v->d.B0, true, due);
   cudaError_t r2 = cudaStreamEndCapture(v->stream, &g);
   if (r == cudaSuccess) r = r2;
-  if (r == cudaSuccess) r = cudaGraphInstantiate(&v->graph, g, 0);
+  if (r == cudaSuccess) r = cudaGraphInstantiate(&ge, g, 0);
   if (g) cudaGraphDestroy(g);
-  if (r == cudaSuccess) r = cudaGraphUpload(v->graph, v->stream);
+  if (r == cudaSuccess) r = cudaGraphUpload(ge, v->stream);
+  if (r == cudaSuccess)
+    v->graphs[due] = ge;
+  else if (ge)
+    cudaGraphExecDestroy(ge);
   return r;
+}
+
+cudaError_t ensure_graphs(tanb_nu* v) {
+  long long period = 1;
+  for (int l = 0; l < v->d.nl; ++l) period = std::max(period, (1LL << v->d.lv[l].log2N) / v->d.B0);
+  for (long long k = 0; k < period; ++k) {
+    const cudaError_t r = ensure_graph(v, due_mask(v->d, k));
+    if (r != cudaSuccess) return r;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -597,7 +633,7 @@ int32_t tanb_nu_create(tanb_context* ctx, uint32_t channels, uint32_t ir_length,
   }
   if (e == cudaSuccess) e = cudaMallocHost(&v->h_in, C * d.B0 * sizeof(float));
   if (e == cudaSuccess) e = cudaMallocHost(&v->h_out, C * d.B0 * sizeof(float));
-  if (e == cudaSuccess) e = ensure_graph(v);
+  if (e == cudaSuccess) e = ensure_graphs(v);
   if (e == cudaSuccess) e = cudaStreamSynchronize(v->stream);
   if (e != cudaSuccess) {
     nu_free(v);
@@ -651,8 +687,9 @@ int32_t tanb_nu_process(tanb_nu* v) {
   if (!v) return nfail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(v->mu);
   NU_CUDA(cudaSetDevice(v->ctx->device));
-  NU_CUDA(ensure_graph(v));
-  NU_CUDA(cudaGraphLaunch(v->graph, v->stream));
+  const unsigned due = due_mask(v->d, v->k);
+  NU_CUDA(ensure_graph(v, due));
+  NU_CUDA(cudaGraphLaunch(v->graphs[due], v->stream));
   NU_CUDA(cudaEventSynchronize(v->ev_out));
   v->k += 1;
   return TANB_OK;
@@ -663,7 +700,7 @@ int32_t tanb_nu_process_device(tanb_nu* v, const float* in, float* out, uint32_t
   if (!v || !out) return nfail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(v->mu);
   NU_CUDA(cudaSetDevice(v->ctx->device));
-  NU_CUDA(enqueue_nu_block(v, in, out, ld ? (int)ld : v->d.B0, false));
+  NU_CUDA(enqueue_nu_block(v, in, out, ld ? (int)ld : v->d.B0, false, due_mask(v->d, v->k)));
   v->k += 1;
   return TANB_OK;
 }
