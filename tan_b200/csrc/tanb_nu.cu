@@ -11,12 +11,13 @@
 // [o_l + j N_l, o_l + (j+1) N_l), never before the base block that follows,
 // so only level 0 is on a block's critical path. Per base block k:
 //   1. the input block goes into a per-channel input ring;
-//   2. level 0: R2C of its 2B0 frame, multiply with partition 0, add its
-//      precomputed tail, C2R, add the output ring's block k (contributions of
-//      the larger levels, computed in earlier blocks) -> output; clear them;
-//   3. level 0's tail for block k+1;
-//   4. every level whose block completes: head (R2C, partition 0, tail, C2R,
-//      add into the output ring at its delayed position) and tail.
+//   2. level 0: R2C of its 2B0 frame, multiply with partitions 0 and 1 (the
+//      new spectrum and the previous one), add its precomputed tail, C2R, add
+//      the output ring's block k (contributions of the larger levels,
+//      computed in earlier blocks) -> output; clear them;
+//   3. level 0's tail (partitions 2..K-1) for block k+1, when K > 2;
+//   4. every level whose block completes: head (as 2, adding into the output
+//      ring at its delayed position) and tail (as 3).
 // The kernels of a block are launched in level order, for the levels that are
 // due at that block only: with power-of-two block sizes the set of due levels
 // follows from the block index, so each set is one CUDA graph captured at
@@ -135,27 +136,45 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   const size_t h0 = (size_t)c * K * M;
   const float s0c = (SPEC != 0) ? lv.scale[(size_t)c * K] : 1.f;
   const float2* t0 = lv.tail + (size_t)c * M;
+  // partition 1 (X_{j-1} * H_1) is taken here; the tail holds partitions >= 2
+  const bool p1 = K > 1 && j > 0;
+  const float2* Fp = lv.fdl + ((size_t)c * K + (p1 ? slot_of(j - 1, K) : 0)) * M;
+  const float s1c = (SPEC != 0 && K > 1) ? lv.scale[(size_t)c * K + 1] : 1.f;
   const float inv_n = 1.0f / (float)(2 * M);
   for (int kk = threadIdx.x; kk <= M / 2; kk += T) {
     if (kk == 0) {
       const float2 X = rfft_post_dc(z[0]);
+      float2 t = t0[0];
+      if (p1) {
+        float2 h1 = spec_get<SPEC>(lv.H, h0 + M);
+        h1.x *= s1c;
+        h1.y *= s1c;
+        t = c_mac_dc(t, Fp[0], h1);
+      }
       F[0] = X;
       float2 h = spec_get<SPEC>(lv.H, h0);
       h.x *= s0c;
       h.y *= s0c;
-      z[0] = irfft_pre_dc(c_mac_dc(t0[0], X, h), inv_n);
+      z[0] = irfft_pre_dc(c_mac_dc(t, X, h), inv_n);
     } else {
       const int km = M - kk;
       const float2 wk = tw[kk], wm = tw[km];
       const float2 a = z[kk], b = z[km];
       const float2 Xk = rfft_post(a, b, wk);
       const float2 Xm = rfft_post(b, a, wm);
+      float2 tk = t0[kk], tm = t0[km];
+      if (p1) {
+        float2 gk = spec_get<SPEC>(lv.H, h0 + M + kk), gm = spec_get<SPEC>(lv.H, h0 + M + km);
+        gk.x *= s1c; gk.y *= s1c; gm.x *= s1c; gm.y *= s1c;
+        tk = c_mac(tk, Fp[kk], gk);
+        tm = c_mac(tm, Fp[km], gm);
+      }
       F[kk] = Xk;
       if (km != kk) F[km] = Xm;
       float2 hk = spec_get<SPEC>(lv.H, h0 + kk), hm = spec_get<SPEC>(lv.H, h0 + km);
       hk.x *= s0c; hk.y *= s0c; hm.x *= s0c; hm.y *= s0c;
-      const float2 Ak = c_mac(t0[kk], Xk, hk);
-      const float2 Am = c_mac(t0[km], Xm, hm);
+      const float2 Ak = c_mac(tk, Xk, hk);
+      const float2 Am = c_mac(tm, Xm, hm);
       z[kk] = irfft_pre(Ak, Am, wk, inv_n);
       if (km != kk) z[km] = irfft_pre(Am, Ak, wm, inv_n);
     }
@@ -185,8 +204,9 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
   }
 }
 
-// Tail of level L for its next block: sum_{i=1}^{K-1} FDL[(cur + i - 1) mod K] * H_i
-// (cur = slot of the block just inserted). One CTA per (channel, 2*UX-bin
+// Tail of level L for its next block: sum_{i=2}^{K-1} FDL[(cur + i - 1) mod K] * H_i
+// (cur = slot of the block just inserted); partition 1 belongs to the head,
+// so the tail reads no spectrum the head writes. One CTA per (channel, 2*UX-bin
 // slice), partitions split over SY warps, reduced in shared memory.
 template <int SPEC, int UX, int SY>
 __global__ void __launch_bounds__(UX* SY) nu_tail_kernel(NuDev d, int L, int log2N) {
@@ -201,11 +221,11 @@ __global__ void __launch_bounds__(UX* SY) nu_tail_kernel(NuDev d, int L, int log
   const int u = blockIdx.x * UX + tx;
   const int K = lv.K;
   float2 a0 = make_float2(0.f, 0.f), a1 = a0;
-  if (u < U && K > 1) {
+  if (u < U && K > 2) {
     const int cur = slot_of(j, K);
-    const int nparts = K - 1;
+    const int nparts = K - 2;
     const int chunk = (nparts + SY - 1) / SY;
-    const int i0 = 1 + ty * chunk, i1 = min(K, i0 + chunk);
+    const int i0 = 2 + ty * chunk, i1 = min(K, i0 + chunk);
     const float4* Fc = reinterpret_cast<const float4*>(lv.fdl + (size_t)c * K * N) + u;
     const bool dc = (u == 0);
     int fs = (cur + i0 - 1) % K;
@@ -376,6 +396,9 @@ cudaError_t tail_s(const NuDev& d, int L, cudaStream_t st) {
 }
 
 cudaError_t launch_nu_tail(const NuDev& d, int L, cudaStream_t st) {
+  // two partitions or fewer: no tail (the head takes partitions 0 and 1); the
+  // level's tail row keeps the zeros it was allocated with
+  if (d.lv[L].K <= 2) return cudaSuccess;
   switch (d.spec) {
     case 0: return tail_s<0>(d, L, st);
     case 1: return tail_s<1>(d, L, st);
