@@ -504,16 +504,13 @@ def run_ours(args):
     p99 = float(max_over_ranks(pg, float(np.percentile(lat_ms, 99)), local))
     conv.Release()
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.cpu_sample_s)
     capacity = roofline_serving = None
     if rank == 0 and world == 1 and not args.no_capacity:
         from tan_b200 import serving
 
-        cp = serving.capacity(ctx, "plain", 4, 48000, 256, blocks=100)
-        cb = serving.capacity(ctx, "batched", 4, 48000, 256, blocks=100)
-        c24 = serving.capacity(ctx, "batched", 4, 48000, 256, spectrum=eng.SPECTRUM_FP24, blocks=100)
+        cp = serving.capacity(ctx, "plain", 4, 48000, 256, blocks=150)
+        cb = serving.capacity(ctx, "batched", 4, 48000, 256, blocks=150)
+        c24 = serving.capacity(ctx, "batched", 4, 48000, 256, spectrum=eng.SPECTRUM_FP24, blocks=150)
         capacity = {"what": "max channels (sessions of 4 ch, IR 48000 = 1 s, block 256 @ 48 kHz) with p99 "
                             "block latency < 5.33 ms, host buffers, FP32",
                     "plain_fp32": cp["max_realtime_channels"], "batched_fp32": cb["max_realtime_channels"],
@@ -531,6 +528,11 @@ def run_ours(args):
                             "what": "batched FP32 engine at its real-time capacity (sessions of 4 ch, IR 48000, "
                                     "block 256), device I/O, CUDA events per block; working set >> L2",
                             **{k: v for k, v in rs.items() if k != "achieved_gbs"}}
+    # the CPU baseline loads every host core for seconds; it runs after the
+    # latency measurements above, whose host-side copies it would slow down
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_sample_s)
 
     if rank == 0:
         deadline_ms = 1000.0 * B / FS

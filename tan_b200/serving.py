@@ -235,7 +235,7 @@ def capacity(ctx, form="batched", C=4, L=65536, block=256, spectrum=eng.SPECTRUM
         lo, hi = hi, hi * 2
         if hi * C > (1 << 17):
             break
-    while hi - lo > max(1, lo // 16):
+    while hi - lo > max(1, lo // 32):
         mid = (lo + hi) // 2
         good, p99 = ok(mid)
         last[mid] = p99
