@@ -6,7 +6,6 @@ from __future__ import annotations
 
 import ctypes
 
-import numpy as np
 
 from . import convolution as cv
 from .convolution import lib
