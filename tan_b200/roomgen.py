@@ -6,7 +6,6 @@ from __future__ import annotations
 
 import ctypes
 
-
 from . import convolution as cv
 from .convolution import lib
 
