@@ -83,7 +83,7 @@ def test_time_varying_swaps_parity(tan_ctx):
     gpu.Release()
 
 
-@pytest.mark.parametrize("B", [32, 64, 256, 2048, 8192])
+@pytest.mark.parametrize("B", [32, 64, 256, 512, 2048, 4096, 8192])
 @pytest.mark.parametrize("Lfac", [0.5, 1.0, 3.3])
 def test_sizes_sweep(tan_ctx, B, Lfac):
     L = max(1, int(B * Lfac))
