@@ -173,9 +173,9 @@ __device__ __forceinline__ void dft8_fwd(float2* v) {
 // IR partition spectra for transforms of M = 8^s points: radix-8 Stockham
 // stages in registers, M / 8 threads, one shared-memory pass per stage
 // instead of two for radix 4 (8192 transforms of 512 points: 32 us against
-// 45 us). Shared memory is
-// padded by one slot per 8 so that the strided stage stores spread over the
-// banks. Same inputs, twiddle table and output as ir_spectrum_kernel.
+// 45 us). Shared memory is padded by one slot per 8 so that the strided stage
+// stores spread over the banks. Same inputs, twiddle table and output as
+// ir_spectrum_kernel.
 template <int LOG2M>
 __global__ void __launch_bounds__((1 << LOG2M) / 8)
     ir_spectrum_r8_kernel(DevState s, IrRows ir, const int* __restrict__ chans, const ChanCtl* __restrict__ ctl) {
