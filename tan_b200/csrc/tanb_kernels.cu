@@ -170,17 +170,17 @@ __device__ __forceinline__ void dft8_fwd(float2* v) {
   v[7] = c_sub(e3, w3);
 }
 
-// IR partition spectra for transforms of M = 8^s points: radix-8 Stockham
-// stages in registers, M / 8 threads, one shared-memory pass per stage
-// instead of two for radix 4 (8192 transforms of 512 points: 32 us against
-// 45 us). Shared memory is padded by one slot per 8 so that the strided stage
-// stores spread over the banks. Same inputs, twiddle table and output as
-// ir_spectrum_kernel.
+// IR partition spectra with radix-8 Stockham stages in registers: M / 8
+// threads, one shared-memory pass per stage instead of two for radix 4
+// (8192 transforms of 512 points: 32 us against 45 us). When log2 M is not a
+// multiple of 3, a radix-2 or radix-4 stage comes first; it reads the row
+// directly, where the upper half of the frame is zero. Shared memory is
+// padded by one slot per 8 so that the strided stage stores spread over the
+// banks. Same inputs, twiddle table and output as ir_spectrum_kernel.
 template <int LOG2M>
 __global__ void __launch_bounds__((1 << LOG2M) / 8)
     ir_spectrum_r8_kernel(DevState s, IrRows ir, const int* __restrict__ chans, const ChanCtl* __restrict__ ctl) {
-  constexpr int M = 1 << LOG2M, T = M / 8;
-  static_assert(LOG2M % 3 == 0, "radix-8 transform sizes are powers of 8");
+  constexpr int M = 1 << LOG2M, T = M / 8, R0 = LOG2M % 3;  // first stage radix 2^R0 (1: none)
   __shared__ float2 sm[M + M / 8];
   auto pad = [](int i) { return i + (i >> 3); };
   const int part = blockIdx.x;
@@ -190,24 +190,54 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
   const float* h = ir.ptrs ? ir.ptrs[row] : ir.base + (size_t)row * ir.stride;
   const long long t0 = (long long)part * M;
   const int j = threadIdx.x;
-  // stage with Ns = 1 straight from the row: z[n] = (h[t0 + 2n], h[t0 + 2n + 1])
-  // for n < M / 2, zero above (inputs j + r M / 8 with r >= 4)
-  float2 v[8];
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    v[r] = make_float2(0.f, 0.f);
-    if (r < 4) {
-      const long long t = t0 + 2 * (j + r * T);
-      if (t < ir.n) v[r].x = h[t];
-      if (t + 1 < ir.n) v[r].y = h[t + 1];
+  // z[n] = (h[t0 + 2n], h[t0 + 2n + 1]) for n < M / 2, zero above
+  auto load = [&](int n) {
+    float2 v = make_float2(0.f, 0.f);
+    if (n < M / 2) {
+      const long long t = t0 + 2 * n;
+      if (t < ir.n) v.x = h[t];
+      if (t + 1 < ir.n) v.y = h[t + 1];
     }
+    return v;
+  };
+  int Ns = 1;
+  float2 v[8];
+  if constexpr (R0 == 0) {
+    // radix-8 stage with Ns = 1: inputs j + r M / 8, zero for r >= 4
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = load(j + r * T);
+    dft8_fwd(v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sm[pad((j << 3) + q)] = v[q];
+    Ns = 8;
+  } else if constexpr (R0 == 1) {
+    // radix 2, Ns = 1: butterflies b = j + e T (M / 2 of them) pair z[b] with
+    // z[b + M / 2] = 0, so both outputs are z[b]
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int b = j + e * T;
+      const float2 a = load(b);
+      sm[pad(2 * b)] = a;
+      sm[pad(2 * b + 1)] = a;
+    }
+    Ns = 2;
+  } else {
+    // radix 4, Ns = 1: butterflies b = j + e T (M / 4 of them) on z[b],
+    // z[b + M / 4] and two zeros: (a + c, a - i c, a - c, a + i c)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int b = j + e * T;
+      const float2 a = load(b), cc = load(b + M / 4);
+      sm[pad(4 * b)] = c_add(a, cc);
+      sm[pad(4 * b + 1)] = make_float2(a.x + cc.y, a.y - cc.x);
+      sm[pad(4 * b + 2)] = c_sub(a, cc);
+      sm[pad(4 * b + 3)] = make_float2(a.x - cc.y, a.y + cc.x);
+    }
+    Ns = 4;
   }
-  dft8_fwd(v);
-#pragma unroll
-  for (int q = 0; q < 8; ++q) sm[pad((j << 3) + q)] = v[q];
   __syncthreads();
-#pragma unroll
-  for (int Ns = 8; Ns < M; Ns <<= 3) {
+#pragma unroll 1
+  for (; Ns < M; Ns <<= 3) {
     const int k = j & (Ns - 1);
     const int tstep = (2 * M) / (8 * Ns);
 #pragma unroll
@@ -708,7 +738,7 @@ cudaError_t launch_ir_t(const DevState& s, const IrRows& ir, const int* chans, i
                         cudaStream_t st) {
   using S = FftShape<LOG2M>;
   dim3 grid(s.P, nch);
-  if constexpr (LOG2M % 3 == 0 && LOG2M >= 6 && LOG2M <= 12)
+  if constexpr (LOG2M <= 12)  // the padded buffer of 8192 points exceeds static shared memory
     ir_spectrum_r8_kernel<LOG2M><<<grid, S::M / 8, 0, st>>>(s, ir, chans, ctl);
   else
     ir_spectrum_kernel<LOG2M><<<grid, S::T, S::M * sizeof(float2), st>>>(s, ir, chans, ctl);
