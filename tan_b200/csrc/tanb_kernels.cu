@@ -200,7 +200,7 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
     }
     return v;
   };
-  int Ns = 1;
+  constexpr int NS0 = R0 == 0 ? 8 : (R0 == 1 ? 2 : 4);  // span after the first stage
   float2 v[8];
   if constexpr (R0 == 0) {
     // radix-8 stage with Ns = 1: inputs j + r M / 8, zero for r >= 4
@@ -209,7 +209,6 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
     dft8_fwd(v);
 #pragma unroll
     for (int q = 0; q < 8; ++q) sm[pad((j << 3) + q)] = v[q];
-    Ns = 8;
   } else if constexpr (R0 == 1) {
     // radix 2, Ns = 1: butterflies b = j + e T (M / 2 of them) pair z[b] with
     // z[b + M / 2] = 0, so both outputs are z[b]
@@ -220,7 +219,6 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
       sm[pad(2 * b)] = a;
       sm[pad(2 * b + 1)] = a;
     }
-    Ns = 2;
   } else {
     // radix 4, Ns = 1: butterflies b = j + e T (M / 4 of them) on z[b],
     // z[b + M / 4] and two zeros: (a + c, a - i c, a - c, a + i c)
@@ -233,11 +231,9 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
       sm[pad(4 * b + 2)] = c_sub(a, cc);
       sm[pad(4 * b + 3)] = make_float2(a.x - cc.y, a.y + cc.x);
     }
-    Ns = 4;
   }
   __syncthreads();
-#pragma unroll 1
-  for (; Ns < M; Ns <<= 3) {
+  auto stage = [&](const int Ns) {
     const int k = j & (Ns - 1);
     const int tstep = (2 * M) / (8 * Ns);
 #pragma unroll
@@ -251,6 +247,15 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
 #pragma unroll
     for (int q = 0; q < 8; ++q) sm[pad(d + q * Ns)] = v[q];
     __syncthreads();
+  };
+  // Powers of 8 unroll the stages (compile-time spans and twiddle strides);
+  // the others keep one loop body, which ptxas fits without spilling.
+  if constexpr (R0 == 0) {
+#pragma unroll
+    for (int Ns = NS0; Ns < M; Ns <<= 3) stage(Ns);
+  } else {
+#pragma unroll 1
+    for (int Ns = NS0; Ns < M; Ns <<= 3) stage(Ns);
   }
   float2* H = s.H + h_index(s, c, slot, part);
   for (int k = j; k <= M / 2; k += T) {
