@@ -109,6 +109,13 @@ struct tanb_convolution {
   // per-block descriptors passed as kernel parameters (C <= kParamChannels)
   std::vector<tanb::ParamDesc> pdesc;
   std::vector<tanb::StageDesc> sdesc;
+  // Process's per-call bookkeeping, sized at Init so that a call allocates
+  // nothing: running / flushed channels of the current block and of each
+  // block of a chunk, and each block's delay-line slot
+  std::vector<uint8_t> scr_run, scr_flush;
+  std::vector<std::vector<uint8_t>> scr_run_b;
+  std::vector<std::vector<int>> scr_flush_b;
+  std::vector<int> scr_cur_b;
   tanb::CtlParam last_ctlp{};
   bool last_is_param = false;
 
@@ -560,18 +567,17 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     TANB_CUDA(ensure_mix(v, *pcm, &epi));
     *v->h_clip = 0;
   }
-  std::vector<uint8_t> run(C), flush(C);
-  std::vector<std::vector<uint8_t>> run_b(kMaxBlocksPerChunk, std::vector<uint8_t>(C));
-  std::vector<std::vector<int>> flush_b(kMaxBlocksPerChunk);
-  std::vector<int> cur_b(kMaxBlocksPerChunk);
+  std::vector<uint8_t>& run = v->scr_run;
+  std::vector<uint8_t>& flush = v->scr_flush;
+  std::vector<std::vector<uint8_t>>& run_b = v->scr_run_b;
+  std::vector<std::vector<int>>& flush_b = v->scr_flush_b;
+  std::vector<int>& cur_b = v->scr_cur_b;
 
   const bool param = C <= tanb::kParamChannels;
   // rows in the object's staging (host rows, the fused pipeline's int16 rows
   // and its scratch outputs): two base pointers describe every channel
   const bool staged = param && (pcm || (in_mem == Mem::Host && out_mem == Mem::Host));
   const bool host_out = out_mem == Mem::Host;  // outputs are read back from host staging
-  if (param && v->pdesc.size() < (size_t)kMaxBlocksPerChunk) v->pdesc.resize(kMaxBlocksPerChunk);
-  if (staged && v->sdesc.size() < (size_t)kMaxBlocksPerChunk) v->sdesc.resize(kMaxBlocksPerChunk);
   while (processed < nblocks && status == TANB_OK) {
     int nb = (int)std::min<size_t>(kMaxBlocksPerChunk, nblocks - processed);
     TANB_CUDA(cudaEventSynchronize(v->ev_stage));
@@ -1080,6 +1086,14 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
   v->tail_left.assign(C, 0);
   v->available.assign(C, 0);
   v->flushed.assign(C, 0);
+  v->pdesc.resize(C <= tanb::kParamChannels ? kMaxBlocksPerChunk : 0);
+  v->sdesc.resize(C <= tanb::kParamChannels ? kMaxBlocksPerChunk : 0);
+  v->scr_run.assign(C, 0);
+  v->scr_flush.assign(C, 0);
+  v->scr_run_b.assign(kMaxBlocksPerChunk, std::vector<uint8_t>(C, 0));
+  v->scr_flush_b.assign(kMaxBlocksPerChunk, std::vector<int>());
+  for (auto& f : v->scr_flush_b) f.reserve(C);
+  v->scr_cur_b.assign(kMaxBlocksPerChunk, 0);
   v->cur = 0;
   v->blocks = 0;
   v->initialized = true;
