@@ -53,7 +53,8 @@ def test_known_answer_delta_irs_from_reference_fixture():
 
 
 @pytest.mark.parametrize("C,B,L,swaps", [(2, 256, 2000, [0, 7]), (3, 128, 1024, [0, 3, 4, 9]),
-                                         (1, 512, 512, [0, 5]), (2, 64, 5000, [2, 11])])
+                                         (1, 512, 512, [0, 5]), (2, 64, 5000, [2, 11]),
+                                         (2, 256, 400, [0, 6])])  # two partitions
 def test_restatement_matches_fp64_with_swaps(C, B, L, swaps):
     g = H.rng(C * 1000 + B)
     nb = 14
