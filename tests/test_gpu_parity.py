@@ -84,7 +84,7 @@ def test_time_varying_swaps_parity(tan_ctx):
 
 
 @pytest.mark.parametrize("B", [32, 64, 256, 512, 2048, 4096, 8192])
-@pytest.mark.parametrize("Lfac", [0.5, 1.0, 3.3])
+@pytest.mark.parametrize("Lfac", [0.5, 1.0, 2.0, 3.3])  # 2.0: two partitions, no tail launch
 def test_sizes_sweep(tan_ctx, B, Lfac):
     L = max(1, int(B * Lfac))
     C = 3
