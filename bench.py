@@ -533,6 +533,10 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_sample_s)
+        # also at the reference library's default thread count, a quarter of
+        # the host's processors (FFTImpl.cpp:245-249, MathImpl.cpp:154-158)
+        cpu["reference_default_threads"] = cpu_baseline(min(5.0, args.cpu_sample_s),
+                                                         threads=max(1, (os.cpu_count() or 4) // 4))
 
     if rank == 0:
         deadline_ms = 1000.0 * B / FS
