@@ -145,3 +145,17 @@ def test_restatement_free_channel_restarts_from_silence():
     assert np.all(y[0, ~live] == 9.0)
     assert fp64.error_db(y[0, live], exp[0, live]) < -120
     assert fp64.error_db(y[1], exp[1]) < -120
+
+
+def test_restatement_at_the_bench_shape_matches_fp64():
+    """64 channels, B = 512, IR 65536 (128 partitions), a swap at block 33."""
+    C, B, L, nb = 64, 512, 65536, 40
+    g = H.rng(20261203 + 1)
+    x = H.noise(g, C, nb * B)
+    h0, h1 = H.irs(g, C, L, (0.2, 1.5)), H.irs(g, C, L, (0.2, 1.5))
+    conv = ref.RefConvolution(L, B, C, threads=4)
+    y, codes = H.run_stream(conv, x, B, {0: (h0, None), 33: (h1, None)}, per_call_blocks=1)
+    conv.close()
+    assert all(c == 0 for c in codes)
+    exp = fp64.stream_fp64(x, B, [(0, {c: h0[c] for c in range(C)}), (33, {c: h1[c] for c in range(C)})])
+    assert max(fp64.error_db(y[c], exp[c]) for c in range(C)) < -120
