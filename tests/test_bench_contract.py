@@ -35,3 +35,8 @@ def test_reference_arm_prints_one_contract_line():
 
 def test_reference_arm_other_ranks_print_nothing():
     assert not [ln for ln in _run({"RANK": "1", "WORLD_SIZE": "2"}).splitlines() if ln.startswith("{")]
+
+
+def test_reference_arm_rank_zero_reports_the_world_size():
+    lines = [ln for ln in _run({"RANK": "0", "WORLD_SIZE": "2"}).splitlines() if ln.startswith("{")]
+    assert len(lines) == 1 and json.loads(lines[0])["n_gpus"] == 2
