@@ -41,6 +41,7 @@ C, B, L, SWAP_EVERY, N_IR_SETS = 64, 512, 65536, 32, 8
 SEED = 20261203 + 1
 L2_FLUSH_BYTES = 256 << 20
 PROFILE_STEPS = 512  # steps of the per-kernel (roofline) pass
+REF_WARM_BLOCKS = 64  # untimed blocks before the reference arm's timed steps
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -56,11 +57,27 @@ def parse():
     return p.parse_args()
 
 
+def swap_index(k, warmup):
+    """IR set loaded before step k, or None: the first IR before step 0, then a
+    swap every SWAP_EVERY steps counted from the first timed step (warmup), so
+    that every timed window of SWAP_EVERY or more steps contains swaps."""
+    if k == 0:
+        return 0
+    if k >= warmup and (k - warmup) % SWAP_EVERY == 0:
+        return 1 + (k - warmup) // SWAP_EVERY
+    return None
+
+
+def swaps_timed(steps):
+    return (steps + SWAP_EVERY - 1) // SWAP_EVERY
+
+
 def config_dict(P):
     return {
         "workload": "time-varying FP32 convolution: 64 ch, block 512 @ 48 kHz, IR 65536 (128 partitions), "
                     "IR swap every 32 blocks with 1-block crossfade",
         "channels": C, "block": B, "ir_length": L, "partitions": P, "swap_every_blocks": SWAP_EVERY,
+        "swap_schedule": "IR swaps at timed steps 0, 32, 64, ... (the first IR before warm-up step 0)",
         "sample_rate": FS, "deadline_ms": 1000.0 * B / FS, "ir_sets_cycled": N_IR_SETS,
     }
 
@@ -82,10 +99,13 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    MIN_WINDOW_S = 1.0
+
     def __init__(self, device):
         self.device = device
         self.proc = None
         self.lines = []
+        self.t0 = None
 
     def __enter__(self):
         try:
@@ -101,7 +121,18 @@ class ClockSampler:
             self.lines.clear()
         except Exception:
             self.proc = None
+        self.t0 = time.time()
         return self
+
+    def keep_busy(self, step):
+        """Runs step() (more of the timed workload, untimed) until the sampling
+        window has lasted MIN_WINDOW_S: nvidia-smi samples every 50 ms, and a
+        timed region of a few ms alone would see none."""
+        n = 0
+        while time.time() - self.t0 < self.MIN_WINDOW_S:
+            step(n)
+            n += 1
+        return n
 
     def _read(self):
         for line in self.proc.stdout:
@@ -133,7 +164,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": "timed steps, then the same workload continued to >= 1 s"}
 
 
 def dist_setup(args):
@@ -214,19 +245,28 @@ def run_reference(args):
     x, irs = make_inputs(64)
     conv = ref.RefConvolution(L, B, C, threads=threads)
     y = np.zeros((C, B), np.float32)
+    xs_blocks = [np.ascontiguousarray(x[:, j * B:(j + 1) * B]) for j in range(64)]
+    # Warm-up: the OpenMP pool, first touch of every buffer and one untimed IR
+    # swap, so that the timed blocks are steady-state blocks (at least
+    # REF_WARM_BLOCKS of them, whatever --warmup says).
+    nwarm = max(args.warmup, REF_WARM_BLOCKS)
+    for k in range(nwarm):
+        if k in (0, nwarm // 2):
+            conv.update_response_td(irs[(k // 7) % N_IR_SETS])
+        conv.process(xs_blocks[k % 64], None, y)
     times = []
-    for k in range(args.warmup + args.steps):
-        xs = np.ascontiguousarray(x[:, (k % 64) * B:((k % 64) + 1) * B])
+    for t in range(args.steps):
+        k = args.warmup + t
+        si = swap_index(k, args.warmup)
         t0 = time.perf_counter()
-        if k % SWAP_EVERY == 0:
-            conv.update_response_td(irs[(k // SWAP_EVERY) % N_IR_SETS])
-        conv.process(xs, None, y)
-        t1 = time.perf_counter()
-        if k >= args.warmup:
-            times.append(t1 - t0)
+        if si is not None:
+            conv.update_response_td(irs[si % N_IR_SETS])
+        conv.process(xs_blocks[k % 64], None, y)
+        times.append(time.perf_counter() - t0)
     total = sum(times)
     value = C * B * args.steps / total / 1e9
     lat = np.array(times) * 1e3
+    swap_step = np.array([swap_index(args.warmup + t, args.warmup) is not None for t in range(args.steps)])
     P = conv.partitions
     line = {
         "metric": METRIC, "value": value, "unit": "GSamples/s", "impl": "reference", "n_gpus": world,
@@ -235,8 +275,13 @@ def run_reference(args):
         "config": config_dict(P),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "p999": float(np.percentile(lat, 99.9))},
+        "latency_ms_without_swap_blocks": {"p50": float(np.percentile(lat[~swap_step], 50)),
+                                           "p99": float(np.percentile(lat[~swap_step], 99))},
+        "swap_block_ms_mean": float(lat[swap_step].mean()),
+        "swaps_timed": swaps_timed(args.steps), "warmup_blocks": nwarm,
         "cpu_baseline": {"value": value, "unit": "GSamples/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} timed blocks (64 ch x 512) incl. IR swaps every 32 blocks; "
+                         "sample": f"{args.steps} timed blocks (64 ch x 512) incl. IR swaps every 32 blocks "
+                                   f"({swaps_timed(args.steps)} timed) after {nwarm} warm-up blocks; "
                                    "oracle C++ restatement of TAN's CPU uniform-partitioned path "
                                    "(the reference needs OpenCL headers and FFTW 3.3.5, absent here)"},
         "e2e": {"value": value, "unit": "GSamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -260,26 +305,47 @@ def read_traffic(name="tail_kernel_64ch_b512_ir65536.txt"):
 
 def size_floor(torch, stream, flush_l2, nbytes, dev, reps=50):
     """What one bandwidth-bound launch over `nbytes` reaches when timed like the
-    tail kernel: a library reduction (torch sum) reading nbytes from HBM, L2
-    flushed before each launch, CUDA events around it; median of `reps`."""
+    partition MAC (L2 flushed before each launch, CUDA events around it on the
+    same stream, median of `reps`): the library's own streaming read
+    (tanb_stream_read, 16-byte loads) at its best of a few grid shapes, and a
+    torch reduction over the same bytes beside it."""
+    from tan_b200 import convolution as cv
+
+    lib = cv.lib()
+    nbytes = nbytes // 16 * 16
     buf = torch.ones(nbytes // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    acc = torch.zeros(1, dtype=torch.float32, device=f"cuda:{dev}")
     out = torch.empty((), dtype=torch.float32, device=f"cuda:{dev}")
-    ms = []
-    with torch.cuda.stream(stream):
-        for r in range(reps + 3):
-            flush_l2()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            torch.sum(buf, 0, out=out)
-            b.record(stream)
-            b.synchronize()
-            if r >= 3:
-                ms.append(a.elapsed_time(b))
-    us = 1e3 * statistics.median(ms)
+
+    def timed(fn):
+        ms = []
+        with torch.cuda.stream(stream):
+            for r in range(reps + 3):
+                flush_l2()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                b.synchronize()
+                if r >= 3:
+                    ms.append(a.elapsed_time(b))
+        return 1e3 * statistics.median(ms)
+
+    def own(cps, thr):
+        rc = lib.tanb_stream_read(buf.data_ptr(), nbytes, acc.data_ptr(), cps, thr, stream.cuda_stream)
+        assert rc == 0, cv.last_error()
+
+    grids = {f"{cps} CTAs/SM x {thr}": timed(lambda: own(cps, thr))
+             for cps, thr in ((1, 1024), (2, 1024), (2, 512), (4, 512), (4, 256), (8, 256))}
+    best = min(grids, key=grids.get)
+    torch_us = timed(lambda: torch.sum(buf, 0, out=out))
     del buf
-    return {"bytes": nbytes, "us": us, "gbs": nbytes / (us * 1e-6) / 1e9,
-            "what": "torch sum over the same bytes, one launch, L2 flushed, CUDA events (median)"}
+    us = grids[best]
+    return {"bytes": nbytes, "us": us, "gbs": nbytes / (us * 1e-6) / 1e9, "grid": best,
+            "what": "tanb_stream_read (the library's 16-byte streaming read) over the same bytes, best grid, "
+                    "one launch, L2 flushed, CUDA events (median)",
+            "grids_us": grids, "torch_sum_us": torch_us, "torch_sum_gbs": nbytes / (torch_us * 1e-6) / 1e9}
 
 
 def hbm_peak():
@@ -336,9 +402,9 @@ def run_ours(args):
     dev_done = ctypes.c_size_t(0)
 
     def dev_step(k):
-        if k % SWAP_EVERY == 0:
-            rc = lib.tanb_convolution_update_response_td_device(conv._h, dev_ir[(k // SWAP_EVERY) % N_IR_SETS], L,
-                                                                None, 0)
+        si = swap_index(k, args.warmup)
+        if si is not None:
+            rc = lib.tanb_convolution_update_response_td_device(conv._h, dev_ir[si % N_IR_SETS], L, None, 0)
             assert rc == 0, cv.last_error()
         rc = lib.tanb_convolution_process_device(conv._h, dev_in[k % xblocks], dev_out[k % 2], B, None,
                                                  ctypes.byref(dev_done))
@@ -366,8 +432,12 @@ def run_ours(args):
             b.record(stream)
             evs.append((a, b))
         conv.Synchronize()
+        counts = conv.profile_read()
+        # the same workload continues, untimed, so that the clock samples
+        # cover at least a second of it
+        nbusy = clk.keep_busy(lambda n: (flush_l2(), dev_step(nblocks + n)))
+        conv.Synchronize()
     torch.cuda.synchronize()
-    counts = conv.profile_read()
     dev_ms = sum(a.elapsed_time(b) for a, b in evs)
     dev_ms = max_over_ranks(pg, dev_ms, local)
     if pg:
@@ -378,7 +448,7 @@ def run_ours(args):
     # kernel launch (the tail then runs alone, after its head)
     nprof = min(args.steps, PROFILE_STEPS)
     conv.profile(True)
-    for k in range(nblocks, nblocks + nprof):
+    for k in range(nblocks + nbusy, nblocks + nbusy + nprof):
         flush_l2()
         dev_step(k)
     conv.Synchronize()
@@ -409,8 +479,9 @@ def run_ours(args):
     T = x_dev.shape[1]
 
     def eng_step(k):
-        if k % SWAP_EVERY == 0:
-            assert sess.update_response_td_device(ir_dev[(k // SWAP_EVERY) % N_IR_SETS], block_until_ready=True) == 0
+        si = swap_index(k, args.warmup)
+        if si is not None:
+            assert sess.update_response_td_device(ir_dev[si % N_IR_SETS], block_until_ready=True) == 0
         j = k % xblocks
         assert e.process_device(x_dev.data_ptr() + j * B * 4, y_full.data_ptr() + j * B * 4, T) == 0
 
@@ -438,13 +509,15 @@ def run_ours(args):
             b.record(estream)
             eevs.append((a, b))
         e.synchronize()
+        ecounts = e.profile_read()
+        ebusy = eclk.keep_busy(lambda n: (eflush(), eng_step(nblocks + n)))
+        e.synchronize()
     torch.cuda.synchronize()
-    ecounts = e.profile_read()
     einfo = e.info()
     eng_ms = max_over_ranks(pg, sum(a.elapsed_time(b) for a, b in eevs), local)
     eng_value = world * C * B * args.steps / (eng_ms / 1e3) / 1e9
     e.profile(True)
-    for k in range(nblocks, nblocks + nprof):
+    for k in range(nblocks + ebusy, nblocks + ebusy + nprof):
         eflush()
         eng_step(k)
     e.synchronize()
@@ -475,9 +548,9 @@ def run_ours(args):
     done = ctypes.c_size_t(0)
 
     def host_step(k):
-        if k % SWAP_EVERY == 0:
-            rc = lib.tanb_convolution_update_response_td(conv._h, ir_rows[(k // SWAP_EVERY) % N_IR_SETS], L,
-                                                         None, 0)
+        si = swap_index(k, args.warmup)
+        if si is not None:
+            rc = lib.tanb_convolution_update_response_td(conv._h, ir_rows[si % N_IR_SETS], L, None, 0)
             assert rc == 0
         rc = lib.tanb_convolution_process(conv._h, in_rows[k % xblocks], out_rows, B, None, ctypes.byref(done))
         assert rc == 0 and done.value == B
@@ -549,6 +622,7 @@ def run_ours(args):
             "metric": METRIC, "value": best["value"], "unit": "GSamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": best["ms_per_step"], "higher_is_better": True,
             "path": best_name, "paths": {"drop-in": plain, "engine": engine_path},
+            "swaps_timed": swaps_timed(args.steps),
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_dict(P),
             "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": p99,

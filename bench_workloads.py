@@ -1,7 +1,7 @@
 """Measurements of the path on each benchmark configuration (seeded synthetic
 inputs with the configurations' shapes; no public dataset is involved).
 
-    python -m tan_b200.workloads dropin_small|engine_uneven|nonuniform_long|nu-tune|pipeline [--quick]
+    python bench_workloads.py dropin_small|engine_uneven|nonuniform_long|nu-tune|pipeline [--quick]
 
 dropin_small  drop-in TANConvolution, 2 ch, B=1024, IR 8192, 200 blocks, FP32
 engine_uneven  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096..262144,
@@ -21,9 +21,15 @@ import time
 
 import numpy as np
 
-from . import convolution as cv
-from . import engine as eng
-from . import nupols
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+from tan_b200 import autotune  # noqa: E402
+from tan_b200 import convolution as cv  # noqa: E402
+from tan_b200 import engine as eng  # noqa: E402
+from tan_b200 import nupols  # noqa: E402
 
 FS = 48000
 
@@ -130,50 +136,11 @@ def engine_uneven(ctx, quick=False):
     return out
 
 
-def tune_nu(ctx, C, L, B0, max_blocks=(1024, 2048, 4096, 8192), mids=(1, 2), spectrum=0, periods=2):
-    """Times candidate schedules over whole periods of the largest level and
-    returns them sorted by mean block time (device-resident input)."""
-    import torch
-
-    res = []
-    g = _rng(40)
-    for mb in max_blocks:
-        for mid in mids:
-            lv = nupols.schedule(L, B0, mb)
-            if mid == 1 and len(lv) > 2:
-                # single partitions in the middle levels, the first level keeps two
-                lv = [lv[0]] + [(b, 1) for b, _ in lv[1:-1]] + [lv[-1]]
-                off = sum(b * k for b, k in lv[:-1])
-                lv[-1] = (lv[-1][0], -(-(L - off) // lv[-1][0]))
-            try:
-                nu = nupols.NonUniform(ctx, C, L, lv, spectrum)
-            except cv.TANError:
-                continue
-            period = lv[-1][0] // B0
-            n = period * periods
-            x = torch.from_numpy(g.uniform(-1, 1, (C, B0 * n)).astype(np.float32)).cuda()
-            y = torch.zeros_like(x)
-            st = torch.cuda.ExternalStream(nu.stream())
-            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
-            for k in range(n):
-                ev[k][0].record(st)
-                nu.process_device(x.data_ptr() + k * B0 * 4, y.data_ptr() + k * B0 * 4, B0 * n)
-                ev[k][1].record(st)
-            nu.synchronize()
-            ms = [a.elapsed_time(b) for a, b in ev]
-            res.append({"levels": lv, "mean_ms": float(np.mean(ms[period:])), "max_ms": float(np.max(ms[period:])),
-                        "tail_bytes_per_block": nu.info()["tail_bytes_per_block"]})
-            nu.release()
-            del x, y
-    res.sort(key=lambda r: r["mean_ms"])
-    return res
-
-
 def nonuniform_long(ctx, quick=False):
     g = _rng(3)
     C, L, B0 = (64 if quick else 256), 1 << 20, 128
     deadline = 1000.0 * B0 / FS
-    cands = tune_nu(ctx, C, L, B0)
+    cands = autotune.tune_nu(ctx, C, L, B0)
     ok = [r for r in cands if r["max_ms"] < deadline] or cands
     best = ok[0]
     nb = 600 if quick else 2000
@@ -214,7 +181,7 @@ def pipeline(ctx, quick=False, S=32, B=256, L=48000):
     forms must be identical."""
     from oracle import ref
 
-    from . import converter as cvt
+    from tan_b200 import converter as cvt
 
     g = _rng(6)
     C = 2 * S
@@ -297,7 +264,7 @@ def main():
     a = ap.parse_args()
     ctx = cv.TANContext(0)
     if a.which == "nu-tune":
-        r = tune_nu(ctx, 64 if a.quick else 256, 1 << 20, 128)
+        r = autotune.tune_nu(ctx, 64 if a.quick else 256, 1 << 20, 128)
     else:
         r = {"dropin_small": dropin_small, "engine_uneven": engine_uneven, "nonuniform_long": nonuniform_long,
              "pipeline": pipeline}[a.which](ctx, a.quick)

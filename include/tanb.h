@@ -480,6 +480,14 @@ int32_t tanb_nu_info(tanb_nu* nu, int64_t out[6]);
 int32_t tanb_convolve_no_alloc(const float* in, const float* ir, float* out, uint32_t channels, size_t samples,
                                size_t ir_length, uint32_t block, void* stream);
 
+/* No reference counterpart; a measurement aid. Reads `bytes` of device memory
+ * at `src` once (16-byte streaming loads, grid of ctas_per_sm CTAs per SM of
+ * `threads` threads) and adds their sum to *out (device float), on `stream`.
+ * Timed around one launch, it is the floor a bandwidth-bound launch of that
+ * size reaches on this GPU; the bench compares the partition MAC with it. */
+int32_t tanb_stream_read(const void* src, size_t bytes, float* out, uint32_t ctas_per_sm, uint32_t threads,
+                         void* stream);
+
 /* No reference counterpart: text of the last error raised on this thread. */
 const char* tanb_last_error(void);
 

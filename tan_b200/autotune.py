@@ -17,6 +17,7 @@ import os
 import numpy as np
 
 from . import convolution as cv
+from . import nupols
 
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
 
@@ -126,6 +127,46 @@ def tuned(ctx, method: int, L: int, B: int, C: int) -> cv.TANConvolution:
     if e is not None:
         conv.tiling(int(e["index"]))
     return conv
+
+
+
+def tune_nu(ctx, C, L, B0, max_blocks=(1024, 2048, 4096, 8192), mids=(1, 2), spectrum=0, periods=2):
+    """Times candidate schedules over whole periods of the largest level and
+    returns them sorted by mean block time (device-resident input)."""
+    import torch
+
+    res = []
+    g = np.random.Generator(np.random.PCG64(20261203 + 40))
+    for mb in max_blocks:
+        for mid in mids:
+            lv = nupols.schedule(L, B0, mb)
+            if mid == 1 and len(lv) > 2:
+                # single partitions in the middle levels, the first level keeps two
+                lv = [lv[0]] + [(b, 1) for b, _ in lv[1:-1]] + [lv[-1]]
+                off = sum(b * k for b, k in lv[:-1])
+                lv[-1] = (lv[-1][0], -(-(L - off) // lv[-1][0]))
+            try:
+                nu = nupols.NonUniform(ctx, C, L, lv, spectrum)
+            except cv.TANError:
+                continue
+            period = lv[-1][0] // B0
+            n = period * periods
+            x = torch.from_numpy(g.uniform(-1, 1, (C, B0 * n)).astype(np.float32)).cuda()
+            y = torch.zeros_like(x)
+            st = torch.cuda.ExternalStream(nu.stream())
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+            for k in range(n):
+                ev[k][0].record(st)
+                nu.process_device(x.data_ptr() + k * B0 * 4, y.data_ptr() + k * B0 * 4, B0 * n)
+                ev[k][1].record(st)
+            nu.synchronize()
+            ms = [a.elapsed_time(b) for a, b in ev]
+            res.append({"levels": lv, "mean_ms": float(np.mean(ms[period:])), "max_ms": float(np.max(ms[period:])),
+                        "tail_bytes_per_block": nu.info()["tail_bytes_per_block"]})
+            nu.release()
+            del x, y
+    res.sort(key=lambda r: r["mean_ms"])
+    return res
 
 
 def main():

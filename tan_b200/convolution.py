@@ -144,6 +144,7 @@ SIGNATURES = {
     "tanb_nu_stream": (_vp, [_vp]),
     "tanb_nu_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_convolve_no_alloc": (_i32, [_vp, _vp, _vp, _u32, _sz, _sz, _u32, _vp]),
+    "tanb_stream_read": (_i32, [_vp, _sz, _vp, _u32, _u32, _vp]),
     "tanb_last_error": (ctypes.c_char_p, []),
 }
 

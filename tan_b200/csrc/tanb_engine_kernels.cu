@@ -32,6 +32,7 @@
 
 #include "tanb_engine.h"
 #include "tanb_fft.cuh"
+#include "tanb_internal.h"
 
 namespace tanb {
 namespace {
@@ -575,15 +576,15 @@ cudaError_t commit_t(const EngChan* chans, const EngItem* items, int item0, int 
 }  // namespace
 
 cudaError_t eng_prepare() {
-  static cudaError_t r = [] {
+  static OncePerDevice once;
+  return once.run([] {
     cudaError_t e;
     if ((e = attrs_all<7>()) != cudaSuccess) return e;
     if ((e = attrs_all<8>()) != cudaSuccess) return e;
     if ((e = attrs_all<9>()) != cudaSuccess) return e;
     if ((e = attrs_all<10>()) != cudaSuccess) return e;
     return attrs_all<11>();
-  }();
-  return r;
+  });
 }
 
 cudaError_t eng_launch_ir(int log2B, int spec, EngChan* chans, const EngUpd* upd, int nupd, int maxP,

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 // A TAN context: the CUDA device its objects run on.
 struct tanb_context {
   int device = 0;
@@ -14,6 +16,33 @@ namespace tanb {
 
 // Records the text returned by tanb_last_error() on this thread.
 void set_last_error(const char* msg);
+
+// A set-up step that must run once on every CUDA device a process uses (kernel
+// attributes such as the dynamic shared-memory limit are held per device):
+// run(f) calls f() the first time it is called with a given device current
+// and returns that result on every later call on the same device.
+class OncePerDevice {
+ public:
+  template <class F>
+  cudaError_t run(F&& f) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu_);
+    if (!done_[dev]) {
+      res_[dev] = f();
+      done_[dev] = true;
+    }
+    return res_[dev];
+  }
+
+ private:
+  static constexpr int kMaxDevices = 64;
+  std::mutex mu_;
+  bool done_[kMaxDevices] = {};
+  cudaError_t res_[kMaxDevices] = {};
+};
 
 // Per-channel control word for one audio block, uploaded with the block's input.
 //   run       channel is processed this block (reference: !m_availableChannels[c])
@@ -195,7 +224,7 @@ struct TdChan {
 // history (len samples, [C][len]) and compute n direct-FIR outputs.
 cudaError_t launch_td(float* hist, int len, const TdChan* ch, int C, int n, int fade_len, cudaStream_t st);
 
-// Sets the shared-memory attributes of every kernel (once per process).
+// Sets the shared-memory attributes of every kernel (once per device).
 cudaError_t prepare_kernels();
 
 // Fills the twiddle table W_N^j = exp(-2 pi i j / N) on the host, computed in

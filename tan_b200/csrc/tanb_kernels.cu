@@ -799,13 +799,14 @@ cudaError_t launch_bulk_t(const DevState& s, const BlockRef& d, int which, int c
                           bool pdl) {
   if (s.B % BR != 0) return cudaErrorInvalidValue;
   constexpr int smem = bulk_smem_bytes<BR, RS, NS>();
-  static cudaError_t attr = [] {
+  static OncePerDevice once;
+  const cudaError_t attr = once.run([] {
     cudaError_t e = cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS, DevDesc>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(tail_bulk_kernel<BR, RS, NS, CtlDesc>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem);
-  }();
+  });
   if (attr != cudaSuccess) return attr;
   dim3 grid(s.B / BR, s.C);
   if (const CtlParam* cp = d.ctl_param())
@@ -838,7 +839,8 @@ constexpr int kTailCount = sizeof(kTail) / sizeof(kTail[0]);
 }  // namespace
 
 cudaError_t prepare_kernels() {
-  static cudaError_t result = [] {
+  static OncePerDevice once;
+  return once.run([] {
     cudaError_t e;
     if ((e = set_attrs<5>()) != cudaSuccess) return e;
     if ((e = set_attrs<6>()) != cudaSuccess) return e;
@@ -849,8 +851,7 @@ cudaError_t prepare_kernels() {
     if ((e = set_attrs<11>()) != cudaSuccess) return e;
     if ((e = set_attrs<12>()) != cudaSuccess) return e;
     return set_attrs<13>();
-  }();
-  return result;
+  });
 }
 
 cudaError_t launch_ir_spectrum(const DevState& s, const IrRows& ir, const int* chans, int nch,

@@ -27,7 +27,8 @@
 
 namespace {
 
-constexpr size_t kScratchBytes = (size_t)32 << 20;
+constexpr size_t kScratchBytes = TANB_NO_ALLOC_SCRATCH_BYTES;
+static_assert(kScratchBytes == ((size_t)32 << 20), "the header documents a 32 MiB scratch array");
 constexpr int kMaxDevices = 64;
 
 // The scratch array. In host code `g_scratch` names a host-side stand-in, not
@@ -104,7 +105,17 @@ extern "C" int32_t tanb_convolve_no_alloc(const float* in, const float* ir, floa
     return TANB_INVALID_ARG;
   }
   const size_t B = block, C = channels;
-  const size_t P = (ir_length + B - 1) / B;
+  // Reject sizes whose layout terms could wrap before forming any product:
+  // every term below is at most 28 * C * P * B bytes or 24 * C * B bytes.
+  const size_t P = ir_length / B + (ir_length % B != 0);
+  if (C > kScratchBytes / B || P > kScratchBytes / (28 * B) || C * P > kScratchBytes / (28 * B)) {
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "tanb_convolve_no_alloc: %zu channels x %zu taps at block %zu exceed the scratch array of %zu bytes", C,
+             ir_length, B, kScratchBytes);
+    tanb::set_last_error(msg);
+    return TANB_INVALID_ARG;
+  }
   // scratch layout
   const size_t o_tw = 0;
   const size_t o_H = o_tw + up256(2 * B * sizeof(float2));

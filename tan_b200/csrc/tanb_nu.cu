@@ -322,9 +322,11 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
 template <int LOG2M, int SPEC>
 cudaError_t head_t(const NuDev& d, int L, float* out, int ld, cudaStream_t st) {
   using S = FftShape<LOG2M>;
-  static cudaError_t attr = cudaFuncSetAttribute(nu_head_kernel<LOG2M, SPEC>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 S::M * (int)sizeof(float2));
+  static OncePerDevice once;
+  const cudaError_t attr = once.run([] {
+    return cudaFuncSetAttribute(nu_head_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                S::M * (int)sizeof(float2));
+  });
   if (attr != cudaSuccess) return attr;
   nu_head_kernel<LOG2M, SPEC><<<d.C, S::T, S::M * sizeof(float2), st>>>(d, L, out, ld);
   return cudaGetLastError();
@@ -333,8 +335,11 @@ cudaError_t head_t(const NuDev& d, int L, float* out, int ld, cudaStream_t st) {
 template <int LOG2M, int SPEC>
 cudaError_t ir_t(const NuDev& d, int L, const float* ir, long long stride, long long n, cudaStream_t st) {
   using S = FftShape<LOG2M>;
-  static cudaError_t attr = cudaFuncSetAttribute(nu_ir_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 S::M * (int)sizeof(float2));
+  static OncePerDevice once;
+  const cudaError_t attr = once.run([] {
+    return cudaFuncSetAttribute(nu_ir_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                S::M * (int)sizeof(float2));
+  });
   if (attr != cudaSuccess) return attr;
   dim3 grid(d.lv[L].K, d.C);
   nu_ir_kernel<LOG2M, SPEC><<<grid, S::T, S::M * sizeof(float2), st>>>(d, L, ir, stride, n);

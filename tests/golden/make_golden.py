@@ -3,7 +3,7 @@ inputs (tan/tests/src/TALibTestConvolution/*.wav). Run here, where the
 reference is mounted; the outputs are committed and nothing reads the
 reference at test time.
 
-    python tests/golden/make_golden.py [reference_root]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 Samples are converted short -> float as the reference's WAV reader does
 (s / 32768, tan/common/wav.cpp:235).
@@ -16,8 +16,7 @@ import wave
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-SRC = os.path.join(REF, "tan/tests/src/TALibTestConvolution")
+SRC = None  # set by main() from the required REFERENCE_ROOT argument
 
 
 def read_wav(name):
@@ -29,6 +28,10 @@ def read_wav(name):
 
 
 def main():
+    global SRC
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+    SRC = os.path.join(sys.argv[1], "tan/tests/src/TALibTestConvolution")
     resp, fs = read_wav("testresponse.wav")
     taps = []
     for c in range(resp.shape[0]):

@@ -72,3 +72,17 @@ def test_null_handles_are_rejected():
     assert lib.tanb_convolution_init(None, 1, 1024, 256, 2) == cv.AMF_INVALID_POINTER
     assert lib.tanb_convolution_process(None, None, None, 0, None, None) == cv.AMF_INVALID_POINTER
     assert lib.tanb_create_convolution(None, None) == cv.AMF_INVALID_POINTER
+
+
+def test_no_alloc_entry_point_refuses_sizes_that_would_wrap():
+    """Sizes whose scratch layout would overflow size_t are refused before any
+    product is formed or any device call is made (so this runs without a GPU)."""
+    lib = cv.lib()
+    buf = (ctypes.c_float * 16)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    huge = (1 << 64) // 2
+    for channels, ir_length, block in [(32, huge, 32), (1, huge + 32, 32), (1 << 31, 1024, 512),
+                                       (64, 1 << 16, 512)]:
+        rc = lib.tanb_convolve_no_alloc(p, p, p, channels, 4096, ir_length, block, None)
+        assert rc == cv.AMF_INVALID_ARG, (channels, ir_length, block)
+        assert "scratch" in cv.last_error()

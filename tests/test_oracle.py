@@ -159,3 +159,20 @@ def test_restatement_at_the_bench_shape_matches_fp64():
     assert all(c == 0 for c in codes)
     exp = fp64.stream_fp64(x, B, [(0, {c: h0[c] for c in range(C)}), (33, {c: h1[c] for c in range(C)})])
     assert max(fp64.error_db(y[c], exp[c]) for c in range(C)) < -120
+
+
+def test_restatement_on_the_dense_ir_fixture_matches_fp64():
+    """The reference's dense IR fixture (testresponse2.wav, first 4096 taps) on
+    its pulse-train input at the reference test's block size 128."""
+    import os
+
+    h = np.load(os.path.join(H.GOLDEN, "testresponse2_head.npy")).astype(np.float32) / 32768.0
+    x = H.pulsetrain(2)
+    B, L = 128, h.shape[1]
+    conv = ref.RefConvolution(L, B, 2, threads=2)
+    y, codes = H.run_stream(conv, x, B, {0: (h, None)})
+    conv.close()
+    assert all(c == 0 for c in codes)
+    exp = fp64.stream_fp64(x, B, [(0, {0: h[0], 1: h[1]})])
+    for c in range(2):
+        assert fp64.error_db(y[c], exp[c]) < -120
