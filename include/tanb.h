@@ -272,6 +272,21 @@ int32_t tanb_engine_release(tanb_engine* engine);
  * The session starts with an all-zero IR. */
 int32_t tanb_engine_open_session(tanb_engine* engine, uint32_t channels, uint32_t ir_length, int32_t* session,
                                  uint32_t* first_slot);
+/* Admits a non-uniformly partitioned session (the reference's
+ * TAN_CONVOLUTION_METHOD_*_NONUNIFORM methods, ConvolutionImpl.cpp:224-246,
+ * 2416-2428): level 0 has the engine's block and level_parts[0] partitions;
+ * level l >= 1 has block level_block[l] (a power of two above level l-1's, at
+ * most 16384) and level_parts[l] partitions starting at tap
+ * o_l = sum_{m<l} level_block[m] * level_parts[m], which must be >= its block
+ * (no added latency); the levels must cover ir_length. Every level runs in the
+ * same graph launch per block as every other session: its tail spread over
+ * the blocks of its period, its head beside the block launch at the blocks
+ * where its block completes. IR updates crossfade over one block exactly as
+ * for a uniform session (the new IR's output of the level blocks already
+ * computed is recomputed when the update is committed). */
+int32_t tanb_engine_open_session_nu(tanb_engine* engine, uint32_t channels, uint32_t ir_length, uint32_t nlevels,
+                                    const uint32_t* level_block, const uint32_t* level_parts, int32_t* session,
+                                    uint32_t* first_slot);
 int32_t tanb_engine_close_session(tanb_engine* engine, int32_t session);
 
 /* UpdateResponseTD for one session (host IR rows, n <= ir_length). The IR is
@@ -432,7 +447,9 @@ void* tanb_room_generator_stream(tanb_room_generator* generator);
 typedef struct tanb_nu tanb_nu;
 
 /* Default schedule: two partitions per size from base_block doubling up to
- * max_block, the largest size covering the rest of the IR. Arrays hold >= 16. */
+ * max_block (<= 16384; tanb_nu_create takes blocks up to 8192, engine
+ * sessions up to 16384), the largest size covering the rest of the IR.
+ * Arrays hold >= 16. */
 int32_t tanb_nu_schedule(uint32_t ir_length, uint32_t base_block, uint32_t max_block, uint32_t* nlevels,
                          uint32_t* level_block, uint32_t* level_parts);
 

@@ -47,15 +47,24 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD_DIR, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(os.path.dirname(HERE), "include", "tanb.h"))
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-x", "cu", "-c", src, "-o", obj]
-            if verbose:
-                print(" ".join(cmd), file=sys.stderr)
-            subprocess.run(cmd, check=True)
+            cmds.append([nvcc, *ARCH, *NVCC_FLAGS, "-x", "cu", "-c", src, "-o", obj])
+    # one nvcc per source, in parallel
+    from concurrent.futures import ThreadPoolExecutor
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        return subprocess.run(cmd).returncode
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        codes = list(ex.map(run, cmds))
+    if any(codes):
+        raise RuntimeError("nvcc failed")
     if force or _stale(LIB, objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"]
         if verbose:

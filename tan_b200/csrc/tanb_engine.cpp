@@ -6,11 +6,18 @@
 // device-memory arena sized by the caller's budget; opening a session that does
 // not fit is refused with AMF_OUT_OF_MEMORY (admission by memory budget).
 //
-// Per audio block one CUDA graph runs a single kernel launch: the heads of every
-// channel slot (reading the pinned input buffer and writing the pinned output
-// buffer in place) side by side with persistent CTAs over the tail work items,
-// which compute the next block's partial sums. The graph is re-instantiated
-// only when the high-water marks of channel slots or work items change.
+// A session is uniformly partitioned (partitions of the block size) or
+// non-uniformly partitioned (a base level at the block size and levels of
+// growing block sizes further along the IR, tanb_engine_open_session_nu).
+//
+// Per audio block one CUDA graph runs: a single block launch with the heads of
+// every channel slot (reading the input rows and writing the output rows in
+// place) side by side with persistent CTAs over the tail work items (the next
+// block's partial sums, and one bin slice of every non-uniform level's tail),
+// and, at the blocks where a level size completes, the level heads of that size
+// in a kernel beside it (a parallel branch of the same graph). The graph of each
+// set of due level sizes is instantiated once and re-instantiated only when the
+// high-water marks of channel slots, work items or level records change.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,11 +31,15 @@
 
 #include "../../include/tanb.h"
 #include "tanb_engine.h"
+#include "tanb_engine_host.h"
 #include "tanb_host_pool.h"
 #include "tanb_internal.h"
 
 using tanb::EngChan;
 using tanb::EngItem;
+using tanb::EngLevel;
+using tanb::EngLvlUpd;
+using tanb::EngNu;
 using tanb::EngUpd;
 
 namespace {
@@ -54,6 +65,12 @@ int32_t efail(int32_t code, const char* fmt, ...) {
 constexpr size_t kAlign = 256;
 
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+size_t pow2_at_least(size_t x) {
+  size_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
 
 // First-fit range allocator with coalescing (offsets in arbitrary units).
 class RangeAlloc {
@@ -104,16 +121,31 @@ class RangeAlloc {
   size_t size_ = 0;
 };
 
+// Shape of one level above the base level of a non-uniform session.
+struct LevelSpec {
+  int log2N = 0, K = 0, Kr = 0, ngroup = 0, R = 0;
+  long long off = 0;
+  int nfl = 0;  // level blocks whose output an IR swap recomputes (at most)
+};
+
 struct Session {
   int id = -1;
-  int C = 0, L = 0, P = 0, nitem = 0;
+  int C = 0, L = 0, P = 0, nitem = 0;  // P, nitem: the (base) level at the engine block
+  int items_per_chan = 0;              // base items + level items per channel
   size_t slot0 = 0, item0 = 0;
   size_t arena_off = 0, arena_bytes = 0;
+  std::vector<LevelSpec> lv;           // levels above the base level (empty: uniform)
+  std::vector<size_t> lv_first;        // per level: its C consecutive records in the size class's table
+  int rin = 0;                         // input history length (non-uniform)
   // IR update staged on the update stream, waiting for its event before commit
   bool staged = false;
   cudaEvent_t staged_ev = nullptr;
+  std::vector<uint8_t> staged_mask;    // channels the staged update replaces
   int64_t blocks = 0;            // blocks processed since the session opened
   int64_t last_swap_block = -1;  // session block at which the last IR update took effect
+  // per channel: the device ranges a flush clears (delay lines, history,
+  // partial sums, level rings)
+  std::vector<std::vector<std::pair<char*, size_t>>> zero;
 };
 
 }  // namespace
@@ -123,7 +155,8 @@ struct tanb_engine {
   std::mutex mu;
   int B = 0, log2B = 0, spec = 0, Q = 32;
   size_t budget = 0, max_channels = 0, max_items = 0;
-  cudaStream_t stream = nullptr;      // audio path: head, tail, I/O copies
+  cudaStream_t stream = nullptr;      // audio path: blocks, commits
+  cudaStream_t lstream = nullptr;     // level heads beside the block launch
   cudaStream_t upd_stream = nullptr;  // IR uploads and transforms
   std::mutex upd_mu;                  // serialises IR updates (taken before mu)
   char* arena = nullptr;
@@ -132,22 +165,34 @@ struct tanb_engine {
   EngChan* h_chans = nullptr;
   EngItem* d_items = nullptr;
   EngItem* h_items = nullptr;
+  // level records: size class c (level block 2^(log2B + 1 + c)) at [c * max_channels, (c + 1) * max_channels)
+  int nclass = 0;
+  EngLevel* d_levels = nullptr;
+  EngLevel* h_levels = nullptr;
+  std::vector<RangeAlloc> lvl_alloc;
+  std::vector<size_t> lvl_hwm;
+  std::vector<float2*> d_tw_lv;       // twiddles of each size class (2N entries)
   float* h_in = nullptr;   // pinned; read in place by the heads
   float* h_out = nullptr;  // pinned; written in place by the heads
   long long* d_block = nullptr;     // blocks processed (device)
-  unsigned int* d_done = nullptr;   // CTAs finished in the running launch
+  unsigned int* d_done = nullptr;   // CTAs finished in the running block
+  long long k_host = 0;             // blocks enqueued (the device counter after they ran)
   float* h_ir = nullptr;
   float* d_ir = nullptr;
   size_t ir_cap = 0;
   EngUpd* h_upd = nullptr;
   EngUpd* d_upd = nullptr;
+  EngLvlUpd* h_lupd = nullptr;
+  EngLvlUpd* d_lupd = nullptr;
   float2* d_tw = nullptr;
   int tail_grid = 0;
   size_t nslots_hwm = 0, nitems_hwm = 0;
-  size_t graph_slots = (size_t)-1, graph_items = (size_t)-1;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
+  // graphs of the host-buffer block, one per set of due level size classes,
+  // valid for the high-water marks in graph_key
+  std::map<unsigned, cudaGraphExec_t> graphs;
+  std::vector<size_t> graph_key;
   cudaEvent_t ev_out = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_audio = nullptr;  // audio-stream point an IR upload waits for
   std::map<int, Session> sessions;
   int next_id = 1;
@@ -165,52 +210,71 @@ size_t spec_bytes(int spec) { return spec == tanb::kSpecFP32 ? 8 : spec == tanb:
 size_t fdl_bytes(int spec) { return spec == tanb::kSpecFP24 ? 6 : 8; }
 bool spec_scaled(int spec) { return spec == tanb::kSpecFP16 || spec == tanb::kSpecBF16; }
 
-size_t session_bytes(const tanb_engine* e, int C, int P, int nitem) {
+size_t chan_bytes(const tanb_engine* e, int P, int nitem, const std::vector<LevelSpec>& lv, int rin) {
   const size_t B = e->B;
   size_t per = align_up(2 * (size_t)P * B * spec_bytes(e->spec));        // H
   if (spec_scaled(e->spec)) per += align_up(2 * (size_t)P * 4);          // scales
   per += align_up((size_t)P * B * fdl_bytes(e->spec));                   // fdl
   per += align_up(B * 4);                                                // prev
   per += align_up(4 * (size_t)nitem * B * 8);                            // partials
-  return per * C;
+  if (!lv.empty()) {
+    per += align_up(sizeof(EngNu)) + align_up((size_t)rin * 4);
+    for (const LevelSpec& l : lv) {
+      const size_t N = (size_t)1 << l.log2N;
+      per += align_up(2 * (size_t)l.K * N * spec_bytes(e->spec));
+      if (spec_scaled(e->spec)) per += align_up(2 * (size_t)l.K * 4);
+      per += align_up((size_t)l.Kr * N * fdl_bytes(e->spec));
+      per += align_up(2 * (size_t)l.ngroup * N * 8);
+      per += align_up(2 * (size_t)l.R * 4);
+    }
+  }
+  return per;
 }
 
-void destroy_graph(tanb_engine* e) {
-  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
-  if (e->graph) cudaGraphDestroy(e->graph);
-  e->graph_exec = nullptr;
-  e->graph = nullptr;
-  e->graph_slots = e->graph_items = (size_t)-1;
+int level_class(const tanb_engine* e, int log2N) { return log2N - e->log2B - 1; }
+
+void destroy_graphs(tanb_engine* e) {
+  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+  e->graphs.clear();
+  e->graph_key.clear();
 }
 
 void free_engine(tanb_engine* e) {
   if (e->upd_stream) cudaStreamSynchronize(e->upd_stream);
   if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->lstream) cudaStreamSynchronize(e->lstream);
   for (auto& kv : e->sessions)
     if (kv.second.staged_ev) cudaEventDestroy(kv.second.staged_ev);
   e->sessions.clear();
-  destroy_graph(e);
+  destroy_graphs(e);
   cudaFree(e->arena);
   cudaFree(e->d_chans);
   cudaFree(e->d_items);
+  cudaFree(e->d_levels);
   cudaFree(e->d_block);
   cudaFree(e->d_ir);
   cudaFree(e->d_upd);
+  cudaFree(e->d_lupd);
   cudaFree(e->d_tw);
+  for (float2* t : e->d_tw_lv) cudaFree(t);
   cudaFreeHost(e->h_chans);
   cudaFreeHost(e->h_items);
+  cudaFreeHost(e->h_levels);
   cudaFreeHost(e->h_in);
   cudaFreeHost(e->h_out);
   cudaFreeHost(e->h_ir);
   cudaFreeHost(e->h_upd);
+  cudaFreeHost(e->h_lupd);
   if (e->ev_out) cudaEventDestroy(e->ev_out);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
   if (e->ev_audio) cudaEventDestroy(e->ev_audio);
   if (e->pa) cudaEventDestroy(e->pa);
   if (e->pb) cudaEventDestroy(e->pb);
   if (e->upd_stream) cudaStreamDestroy(e->upd_stream);
+  if (e->lstream) cudaStreamDestroy(e->lstream);
   if (e->stream) cudaStreamDestroy(e->stream);
 }
-
 
 cudaError_t upload_chans(tanb_engine* e, size_t first, size_t n) {
   if (!n) return cudaSuccess;
@@ -224,15 +288,24 @@ cudaError_t upload_items(tanb_engine* e, size_t first, size_t n) {
                          e->stream);
 }
 
+cudaError_t upload_levels(tanb_engine* e, size_t first, size_t n) {
+  if (!n) return cudaSuccess;
+  return cudaMemcpyAsync(e->d_levels + first, e->h_levels + first, n * sizeof(EngLevel), cudaMemcpyHostToDevice,
+                         e->stream);
+}
+
 void update_hwm(tanb_engine* e) {
   e->nslots_hwm = e->slot_alloc.high_water();
   e->nitems_hwm = e->item_alloc.high_water();
+  for (int c = 0; c < e->nclass; ++c) e->lvl_hwm[c] = e->lvl_alloc[c].high_water();
 }
 
 // Commits every staged IR update whose transform has finished: the channels'
-// pending flags go to the device table and the new IR's partial sums for the
-// coming block are computed from the current delay line, both on the audio
-// stream before this block's launch (whose heads then crossfade to the new IR).
+// pending flags go to the device table, the new IR's partial sums for the
+// coming block are computed from the current delay line and, for non-uniform
+// sessions, the levels' partial sums of the level blocks still to come and the
+// output of level blocks still to be played, all on the audio stream before
+// this block's launch (whose heads then crossfade to the new IR).
 // Caller holds mu.
 cudaError_t commit_updates(tanb_engine* e) {
   for (auto& kv : e->sessions) {
@@ -243,17 +316,36 @@ cudaError_t commit_updates(tanb_engine* e) {
     if (q != cudaSuccess) return q;
     s.staged = false;
     s.last_swap_block = s.blocks;  // the head of this block crossfades to the new IR
-    for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j].pending = 1;
-    // not a copy of the mirror: process_device returns before the device has
-    // run this, and the mirror advances right away
-    cudaError_t r = tanb::eng_launch_mark_pending(e->d_chans, (int)s.slot0, s.C, e->stream);
-    if (r != cudaSuccess) return r;
-    if (s.nitem) {
-      r = tanb::eng_launch_commit(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, s.C * s.nitem,
-                                  std::min(e->tail_grid, s.C * s.nitem), e->d_block, e->stream);
+    // runs of updated channels; not a copy of the mirror: process returns
+    // before the device has run this, and the mirror advances right away
+    for (int j = 0; j < s.C;) {
+      if (!s.staged_mask[j]) {
+        ++j;
+        continue;
+      }
+      int j1 = j;
+      while (j1 < s.C && s.staged_mask[j1]) e->h_chans[s.slot0 + j1++].pending = 1;
+      cudaError_t r = tanb::eng_launch_mark_pending(e->d_chans, (int)s.slot0 + j, j1 - j, e->stream);
       if (r != cudaSuccess) return r;
-      e->n_commit += 1;
+      j = j1;
     }
+    const int nit = s.C * s.items_per_chan;
+    const int grid = std::max(1, std::min(e->tail_grid, nit));
+    cudaError_t r = cudaSuccess;
+    if (s.nitem)
+      r = tanb::eng_launch_commit(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, nit, grid, e->d_block,
+                                  e->stream);
+    if (r == cudaSuccess && nit > s.C * s.nitem)
+      r = tanb::eng_launch_level_commit_items(e->log2B, e->spec, e->d_chans, e->d_levels, e->d_items, (int)s.item0,
+                                              nit, grid, e->d_block, e->stream);
+    for (size_t l = 0; l < s.lv.size() && r == cudaSuccess; ++l) {
+      const int c = level_class(e, s.lv[l].log2N);
+      r = tanb::eng_launch_level_commit_out(e->log2B, s.lv[l].log2N, e->spec, e->d_chans,
+                                            e->d_levels + (size_t)c * e->max_channels, (int)s.lv_first[l], s.C,
+                                            s.lv[l].nfl, e->d_tw_lv[c], e->d_block, e->stream);
+    }
+    if (r != cudaSuccess) return r;
+    e->n_commit += 1;
   }
   return cudaSuccess;
 }
@@ -264,35 +356,92 @@ int tail_ctas(const tanb_engine* e) {
   return (int)std::min<size_t>(e->tail_grid - e->tail_grid / 4, e->nitems_hwm);
 }
 
-// Enqueues one block: the single launch over all slots and work items (in and
-// out: device rows or the pinned host buffers).
-cudaError_t enqueue_block(tanb_engine* e, const float* in, float* out, size_t ld) {
-  return tanb::eng_launch_block(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, e->d_items, (int)e->nitems_hwm,
-                                tail_ctas(e), in, out, (int)ld, e->d_tw, tanb::EngSync{e->d_block, e->d_done},
-                                e->stream);
+// Level size classes due at block k (bit c: class c has records and its
+// block completes with base block k).
+unsigned due_mask(const tanb_engine* e, long long k) {
+  unsigned m = 0;
+  for (int c = 0; c < e->nclass; ++c) {
+    const long long p = 2LL << c;  // N / B
+    if (e->lvl_hwm[c] && ((k + 1) % p) == 0) m |= 1u << c;
+  }
+  return m;
 }
 
-cudaError_t ensure_graph(tanb_engine* e) {
-  if (e->graph_exec && e->graph_slots == e->nslots_hwm && e->graph_items == e->nitems_hwm) return cudaSuccess;
-  destroy_graph(e);
+// Enqueues one block: the block launch over all slots and work items, and the
+// heads of the due level classes on the level stream beside it (forked from
+// and joined back into the audio stream, so that a captured graph holds them
+// as parallel branches).
+cudaError_t enqueue_block(tanb_engine* e, const tanb::EngRows& rows, unsigned due) {
+  const int tc = tail_ctas(e);
+  unsigned total = tanb::eng_block_ctas((int)e->nslots_hwm, tc);
+  for (int c = 0; c < e->nclass; ++c)
+    if (due >> c & 1u) total += (unsigned)e->lvl_hwm[c];
+  const tanb::EngSync sync{e->d_block, e->d_done};
+  cudaError_t r;
+  if (due) {
+    if ((r = cudaEventRecord(e->ev_fork, e->stream)) != cudaSuccess) return r;
+    if ((r = cudaStreamWaitEvent(e->lstream, e->ev_fork, 0)) != cudaSuccess) return r;
+  }
+  r = tanb::eng_launch_block(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, e->d_items, (int)e->nitems_hwm, tc,
+                             e->d_levels, rows, e->d_tw, sync, total, e->stream);
+  if (r != cudaSuccess || !due) return r;
+  for (int c = 0; c < e->nclass; ++c) {
+    if (!(due >> c & 1u)) continue;
+    r = tanb::eng_launch_level_heads(e->log2B, e->log2B + 1 + c, e->spec, e->d_chans, (int)e->nslots_hwm,
+                                     e->d_levels + (size_t)c * e->max_channels, (int)e->lvl_hwm[c], rows,
+                                     e->d_tw_lv[c], sync, total, e->lstream);
+    if (r != cudaSuccess) return r;
+  }
+  if ((r = cudaEventRecord(e->ev_join, e->lstream)) != cudaSuccess) return r;
+  return cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+}
+
+std::vector<size_t> graph_key(const tanb_engine* e) {
+  std::vector<size_t> k{e->nslots_hwm, e->nitems_hwm};
+  k.insert(k.end(), e->lvl_hwm.begin(), e->lvl_hwm.end());
+  return k;
+}
+
+cudaError_t ensure_graph(tanb_engine* e, unsigned due, cudaGraphExec_t* out) {
+  const std::vector<size_t> key = graph_key(e);
+  if (key != e->graph_key) {
+    destroy_graphs(e);
+    e->graph_key = key;
+  }
+  auto it = e->graphs.find(due);
+  if (it != e->graphs.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
   cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
   if (r != cudaSuccess) return r;
-  cudaError_t r2 = enqueue_block(e, e->h_in, e->h_out, e->B);
+  tanb::EngRows rows;
+  rows.in_base = e->h_in;
+  rows.out_base = e->h_out;
+  rows.ld = e->B;
+  cudaError_t r2 = enqueue_block(e, rows, due);
   // inside stream capture a plain record only marks a capture dependency; the
   // external flag makes it an event-record node that fires on every launch
   if (r2 == cudaSuccess) r2 = cudaEventRecordWithFlags(e->ev_out, e->stream, cudaEventRecordExternal);
-  r = cudaStreamEndCapture(e->stream, &e->graph);
-  if (r2 != cudaSuccess) return r2;
+  r = cudaStreamEndCapture(e->stream, &g);
+  if (r2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return r2;
+  }
   if (r != cudaSuccess) return r;
-  r = cudaGraphInstantiate(&e->graph_exec, e->graph, 0);
+  r = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
   if (r != cudaSuccess) return r;
-  e->graph_slots = e->nslots_hwm;
-  e->graph_items = e->nitems_hwm;
+  e->graphs[due] = ge;
+  *out = ge;
   return cudaSuccess;
 }
 
-// Host mirror of what the head kernel does to the channel table.
+// Host mirror of what the block launch does to the channel table.
 void advance_mirror(tanb_engine* e) {
+  e->k_host += 1;
   for (auto& kv : e->sessions) {
     Session& s = kv.second;
     s.blocks += 1;
@@ -307,7 +456,346 @@ void advance_mirror(tanb_engine* e) {
   }
 }
 
+// Checks a non-uniform level schedule and derives its level shapes.
+int32_t make_levels(const tanb_engine* e, uint32_t ir_length, uint32_t nlevels, const uint32_t* block,
+                    const uint32_t* parts, std::vector<LevelSpec>* lv, int* P0, int* rin) {
+  if (nlevels == 0 || nlevels > (uint32_t)tanb::kMaxLevels + 1)
+    return efail(TANB_INVALID_ARG, "a non-uniform schedule has 1 to %d levels", tanb::kMaxLevels + 1);
+  if (block[0] != (uint32_t)e->B) return efail(TANB_INVALID_ARG, "level 0's block must be the engine block %d", e->B);
+  long long off = 0;
+  size_t nmax = e->B;
+  lv->clear();
+  for (uint32_t l = 0; l < nlevels; ++l) {
+    const uint32_t N = block[l];
+    if (parts[l] == 0) return efail(TANB_INVALID_ARG, "level %u has no partitions", l);
+    if (l > 0) {
+      if ((N & (N - 1)) || N <= block[l - 1] || N > (1u << tanb::kMaxLog2Level))
+        return efail(TANB_INVALID_ARG, "level %u: block %u must be a power of two above the previous level's and "
+                     "at most %u", l, N, 1u << tanb::kMaxLog2Level);
+      if (off < (long long)N)
+        return efail(TANB_INVALID_ARG, "level %u starts at tap %lld < its block %u (would add latency)", l, off, N);
+      LevelSpec s;
+      while ((1u << s.log2N) < N) ++s.log2N;
+      s.K = (int)parts[l];
+      s.off = off;
+      s.nfl = (int)((off + N - 1) / N);
+      s.Kr = s.K + s.nfl - 1;
+      s.ngroup = s.K > 2 ? (s.K - 2 + e->Q - 1) / e->Q : 0;
+      s.R = (int)pow2_at_least((size_t)off + N + 2 * (size_t)e->B);
+      lv->push_back(s);
+      nmax = std::max<size_t>(nmax, N);
+    } else {
+      *P0 = (int)parts[0];
+    }
+    off += (long long)N * parts[l];
+  }
+  if (off < (long long)ir_length) return efail(TANB_INVALID_ARG, "levels cover %lld < %u taps", off, ir_length);
+  *rin = (int)pow2_at_least(2 * nmax + e->B);
+  return TANB_OK;
+}
+
+int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint32_t nlevels,
+                     const uint32_t* level_block, const uint32_t* level_parts, int32_t* session,
+                     uint32_t* first_slot) {
+  if (!e || !session) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(e->mu);
+  if (channels == 0 || ir_length == 0) return efail(TANB_INVALID_ARG, "channels and IR length must be > 0");
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  Session s;
+  s.C = (int)channels;
+  s.L = (int)ir_length;
+  if (nlevels) {
+    const int32_t r = make_levels(e, ir_length, nlevels, level_block, level_parts, &s.lv, &s.P, &s.rin);
+    if (r != TANB_OK) return r;
+  } else {
+    s.P = (int)std::max<uint32_t>(1, (ir_length + e->B - 1) / e->B);
+  }
+  // work items cover partitions [2, P); the head does partitions 0 and 1
+  s.nitem = s.P > 2 ? (s.P - 2 + e->Q - 1) / e->Q : 0;
+  s.items_per_chan = s.nitem;
+  for (const LevelSpec& l : s.lv) s.items_per_chan += l.ngroup << (l.log2N - e->log2B);
+  const size_t per_chan = chan_bytes(e, s.P, s.nitem, s.lv, s.rin);
+  s.arena_bytes = per_chan * s.C;
+  if (!e->arena_alloc.alloc(s.arena_bytes / kAlign, &s.arena_off))
+    return efail(TANB_OUT_OF_MEMORY, "session of %u channels x %u taps needs %zu bytes; device budget exhausted",
+                 channels, ir_length, s.arena_bytes);
+  if (!e->slot_alloc.alloc(s.C, &s.slot0)) {
+    e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
+    return efail(TANB_OUT_OF_MEMORY, "no %u free channel slots", channels);
+  }
+  const size_t nit_total = (size_t)s.C * s.items_per_chan;
+  if (nit_total && !e->item_alloc.alloc(nit_total, &s.item0)) {
+    e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
+    e->slot_alloc.release(s.slot0, s.C);
+    return efail(TANB_OUT_OF_MEMORY, "work-item table full");
+  }
+  s.lv_first.assign(s.lv.size(), 0);
+  for (size_t l = 0; l < s.lv.size(); ++l) {
+    const int c = level_class(e, s.lv[l].log2N);
+    if (!e->lvl_alloc[c].alloc(s.C, &s.lv_first[l])) {
+      for (size_t m = 0; m < l; ++m) e->lvl_alloc[level_class(e, s.lv[m].log2N)].release(s.lv_first[m], s.C);
+      e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
+      e->slot_alloc.release(s.slot0, s.C);
+      if (nit_total) e->item_alloc.release(s.item0, nit_total);
+      return efail(TANB_OUT_OF_MEMORY, "level table full");
+    }
+  }
+  ENG_CUDA(cudaStreamSynchronize(e->stream));  // pinned mirrors are rewritten below
+  char* base = e->arena + s.arena_off * kAlign;
+  ENG_CUDA(cudaMemsetAsync(base, 0, s.arena_bytes, e->stream));
+  const size_t B = e->B;
+  std::vector<EngNu> nus(s.lv.empty() ? 0 : s.C);
+  std::vector<EngNu*> nu_dev(nus.size());
+  s.zero.assign(s.C, {});
+  for (int j = 0; j < s.C; ++j) {
+    auto& zero = s.zero[j];
+    EngChan ch{};
+    ch.H = base;
+    base += align_up(2 * (size_t)s.P * B * spec_bytes(e->spec));
+    if (spec_scaled(e->spec)) {
+      ch.scale = reinterpret_cast<float*>(base);
+      base += align_up(2 * (size_t)s.P * 4);
+    }
+    // delay line, history and partial sums are consecutive: one flush range
+    char* z0 = base;
+    ch.fdl = reinterpret_cast<float2*>(base);
+    base += align_up((size_t)s.P * B * fdl_bytes(e->spec));
+    ch.prev = reinterpret_cast<float*>(base);
+    base += align_up(B * 4);
+    ch.part = reinterpret_cast<float2*>(base);
+    base += align_up(4 * (size_t)s.nitem * B * 8);
+    zero.push_back({z0, (size_t)(base - z0)});
+    ch.P = s.P;
+    ch.nitem = s.nitem;
+    ch.cur = 0;
+    ch.active = 0;
+    ch.pending = 0;
+    ch.run = 1;
+    const int slot = (int)(s.slot0 + j);
+    size_t it = s.item0 + (size_t)j * s.items_per_chan;
+    for (int r = 0; r < s.nitem; ++r) {
+      const int i0 = 2 + r * e->Q;
+      e->h_items[it++] = EngItem{slot, i0, std::min(s.P, i0 + e->Q), r, -1, 0};
+    }
+    if (!s.lv.empty()) {
+      EngNu& nu = nus[j];
+      nu_dev[j] = reinterpret_cast<EngNu*>(base);
+      ch.nu = nu_dev[j];
+      base += align_up(sizeof(EngNu));
+      nu.in_ring = reinterpret_cast<float*>(base);
+      nu.rin = s.rin;
+      nu.nlv = (int)s.lv.size();
+      zero.push_back({base, (size_t)s.rin * 4});
+      base += align_up((size_t)s.rin * 4);
+      for (size_t l = 0; l < s.lv.size(); ++l) {
+        const LevelSpec& ls = s.lv[l];
+        const size_t N = (size_t)1 << ls.log2N;
+        const int c = level_class(e, ls.log2N);
+        const size_t rec = (size_t)c * e->max_channels + s.lv_first[l] + j;
+        EngLevel lv{};
+        lv.H = base;
+        base += align_up(2 * (size_t)ls.K * N * spec_bytes(e->spec));
+        if (spec_scaled(e->spec)) {
+          lv.scale = reinterpret_cast<float*>(base);
+          base += align_up(2 * (size_t)ls.K * 4);
+        }
+        char* z1 = base;
+        lv.fdl = reinterpret_cast<float2*>(base);
+        base += align_up((size_t)ls.Kr * N * fdl_bytes(e->spec));
+        lv.part = reinterpret_cast<float2*>(base);
+        base += align_up(2 * (size_t)ls.ngroup * N * 8);
+        lv.ring = reinterpret_cast<float*>(base);
+        base += align_up(2 * (size_t)ls.R * 4);
+        zero.push_back({z1, (size_t)(base - z1)});
+        lv.chan = slot;
+        lv.log2N = ls.log2N;
+        lv.K = ls.K;
+        lv.Kr = ls.Kr;
+        lv.ngroup = ls.ngroup;
+        lv.R = ls.R;
+        lv.off = ls.off;
+        e->h_levels[rec] = lv;
+        nu.ring[l] = lv.ring;
+        nu.R[l] = ls.R;
+        const int p = 1 << (ls.log2N - e->log2B);
+        for (int g = 0; g < ls.ngroup; ++g) {
+          const int i0 = 2 + g * e->Q;
+          for (int sl = 0; sl < p; ++sl)
+            e->h_items[it++] = EngItem{slot, i0, std::min(ls.K, i0 + e->Q), g, (int)(c * e->max_channels +
+                                       s.lv_first[l] + j), sl};
+        }
+      }
+    }
+    e->h_chans[slot] = ch;
+  }
+  if (base != e->arena + s.arena_off * kAlign + s.arena_bytes)
+    return efail(TANB_FAIL, "session layout does not match its size (internal error)");
+  for (size_t j = 0; j < nus.size(); ++j)
+    ENG_CUDA(cudaMemcpyAsync(nu_dev[j], &nus[j], sizeof(EngNu), cudaMemcpyHostToDevice, e->stream));
+  for (size_t l = 0; l < s.lv.size(); ++l)
+    ENG_CUDA(upload_levels(e, (size_t)level_class(e, s.lv[l].log2N) * e->max_channels + s.lv_first[l], s.C));
+  ENG_CUDA(upload_chans(e, s.slot0, s.C));
+  ENG_CUDA(upload_items(e, s.item0, nit_total));
+  // the copies read the pinned mirrors (and nus), which change after this
+  ENG_CUDA(cudaStreamSynchronize(e->stream));
+  ENG_CUDA(cudaEventCreateWithFlags(&s.staged_ev, cudaEventDisableTiming));
+  s.staged_mask.assign(s.C, 0);
+  s.id = e->next_id++;
+  e->sessions[s.id] = s;
+  update_hwm(e);
+  *session = s.id;
+  if (first_slot) *first_slot = (uint32_t)s.slot0;
+  return TANB_OK;
+}
+
+int32_t engine_update(tanb_engine* e, int32_t session, const float* const* ir, size_t n, bool device, uint32_t op,
+                      const uint8_t* mask) {
+  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  if (!ir) return efail(TANB_INVALID_ARG, "ppBuffer == NULL");
+  std::lock_guard<std::mutex> ulock(e->upd_mu);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  // the previous upload's copies read the pinned staging rewritten below
+  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
+  Session s;
+  std::vector<int> chans;  // session channels updated
+  {
+    // read the session and choose the idle IR slots under the main lock: the
+    // audio path flips slots only under this lock, so the choice is consistent
+    std::lock_guard<std::mutex> lock(e->mu);
+    auto it = e->sessions.find(session);
+    if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
+    s = it->second;
+    if (n > (size_t)s.L) return efail(TANB_INVALID_ARG, "IR length %zu exceeds the session's %d", n, s.L);
+    for (int j = 0; j < s.C; ++j) {
+      if (mask && !mask[j]) continue;
+      if (!ir[j] && n) return efail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", j);
+      chans.push_back(j);
+    }
+    if (chans.empty()) return TANB_OK;
+    for (size_t q = 0; q < chans.size(); ++q) {
+      const int j = chans[q];
+      e->h_upd[q] = EngUpd{(int)(s.slot0 + j), 1 - e->h_chans[s.slot0 + j].active, nullptr, (int64_t)n};
+    }
+    it->second.staged = false;  // a newer upload supersedes one not yet committed
+    // The mirror (and so the idle-slot choice) already reflects every block
+    // enqueued on the audio stream; blocks still running there may read the
+    // chosen slot (a crossfade from it), so the transform waits for them.
+    ENG_CUDA(cudaEventRecord(e->ev_audio, e->stream));
+    ENG_CUDA(cudaStreamWaitEvent(e->upd_stream, e->ev_audio, 0));
+  }
+  const int nch = (int)chans.size();
+  if (!device && n) {
+    const size_t need = n * (size_t)nch;
+    if (need > e->ir_cap) {
+      cudaFree(e->d_ir);
+      cudaFreeHost(e->h_ir);
+      e->d_ir = nullptr;
+      e->h_ir = nullptr;
+      e->ir_cap = 0;
+      ENG_CUDA(cudaMalloc(&e->d_ir, need * sizeof(float)));
+      ENG_CUDA(cudaMallocHost(&e->h_ir, need * sizeof(float)));
+      e->ir_cap = need;
+    }
+  }
+  if (device) {
+    // the transforms read the caller's rows in place
+    for (int q = 0; q < nch; ++q) e->h_upd[q].src = ir[chans[q]];
+  } else if (n) {
+    // compact staging (row stride n) copied on the host pool, one transfer
+    auto copy_row = [&](int q) { tanb::copy_for_device(e->h_ir + (size_t)q * n, ir[chans[q]], n * sizeof(float)); };
+    if ((size_t)nch * n * sizeof(float) >= (1u << 20))
+      tanb::host_parallel_for(nch, copy_row);
+    else
+      for (int q = 0; q < nch; ++q) copy_row(q);
+    ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, (size_t)nch * n * sizeof(float), cudaMemcpyHostToDevice,
+                             e->upd_stream));
+    for (int q = 0; q < nch; ++q) e->h_upd[q].src = e->d_ir + (size_t)q * n;
+  }
+  ENG_CUDA(cudaMemcpyAsync(e->d_upd, e->h_upd, nch * sizeof(EngUpd), cudaMemcpyHostToDevice, e->upd_stream));
+  ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_upd, nch, s.P, e->d_tw, e->upd_stream));
+  // the levels of a non-uniform session, one transform launch per level
+  for (size_t l = 0; l < s.lv.size(); ++l) {
+    const int c = level_class(e, s.lv[l].log2N);
+    EngLvlUpd* hl = e->h_lupd + l * e->max_channels;
+    for (int q = 0; q < nch; ++q)
+      hl[q] = EngLvlUpd{(int)(s.lv_first[l] + chans[q]), e->h_upd[q].slot, e->h_upd[q].src, (int64_t)n};
+    EngLvlUpd* dl = e->d_lupd + l * e->max_channels;
+    ENG_CUDA(cudaMemcpyAsync(dl, hl, nch * sizeof(EngLvlUpd), cudaMemcpyHostToDevice, e->upd_stream));
+    ENG_CUDA(tanb::eng_launch_level_ir(s.lv[l].log2N, e->spec, e->d_levels + (size_t)c * e->max_channels, dl, nch,
+                                       s.lv[l].K, e->d_tw_lv[c], e->upd_stream));
+  }
+  ENG_CUDA(cudaEventRecord(s.staged_ev, e->upd_stream));
+  // BLOCK_UNTIL_READY: the new IR is ready for the next block when this returns
+  if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) ENG_CUDA(cudaEventSynchronize(s.staged_ev));
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    auto it = e->sessions.find(session);
+    if (it != e->sessions.end()) {
+      it->second.staged = true;
+      std::fill(it->second.staged_mask.begin(), it->second.staged_mask.end(), 0);
+      for (int j : chans) it->second.staged_mask[j] = 1;
+    }
+    e->n_ir += 1;
+  }
+  return TANB_OK;
+}
+
+// One block: commit staged updates, then the block (a graph for the host
+// buffers, direct launches for other rows). Caller holds mu.
+int32_t run_block(tanb_engine* e, const tanb::EngRows* rows) {
+  ENG_CUDA(commit_updates(e));
+  const unsigned due = due_mask(e, e->k_host);
+  if (!rows) {
+    cudaGraphExec_t ge = nullptr;
+    ENG_CUDA(ensure_graph(e, due, &ge));
+    ENG_CUDA(cudaGraphLaunch(ge, e->stream));
+  } else {
+    if (e->profiling) ENG_CUDA(cudaEventRecord(e->pa, e->stream));
+    ENG_CUDA(enqueue_block(e, *rows, due));
+    if (e->profiling) {
+      ENG_CUDA(cudaEventRecord(e->pb, e->stream));
+      ENG_CUDA(cudaEventSynchronize(e->pb));
+      float a = 0;
+      cudaEventElapsedTime(&a, e->pa, e->pb);
+      e->ms_block += a;
+      e->n_timed += 1;
+    }
+  }
+  e->n_block += 1;
+  advance_mirror(e);
+  return TANB_OK;
+}
+
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Internal interface for the drop-in object's non-uniform methods
+// (tanb_engine_host.h).
+namespace tanb {
+
+int32_t engine_update_channels(tanb_engine* e, int32_t session, const float* const* ir, size_t n, bool device,
+                               uint32_t op, const uint8_t* mask) {
+  return engine_update(e, session, ir, n, device, op, mask);
+}
+
+int32_t engine_flush_channel(tanb_engine* e, int32_t session, int channel) {
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->sessions.find(session);
+  if (it == e->sessions.end() || channel < 0 || channel >= it->second.C)
+    return efail(TANB_INVALID_ARG, "no channel %d in session %d", channel, session);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  for (const auto& z : it->second.zero[channel]) ENG_CUDA(cudaMemsetAsync(z.first, 0, z.second, e->stream));
+  return TANB_OK;
+}
+
+int32_t engine_process_rows(tanb_engine* e, const EngRows& rows) {
+  std::lock_guard<std::mutex> lock(e->mu);
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
+  return run_block(e, &rows);
+}
+
+}  // namespace tanb
 
 extern "C" {
 
@@ -328,27 +816,43 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   e->Q = (int)partitions_per_item;
   e->budget = budget_bytes;
   e->max_channels = max_channels;
-  e->max_items = (size_t)max_channels * 64;
+  // work items: 64 per channel slot, or as many as the budget can feed (an
+  // item streams at least Q partitions x B bins x 8 bytes of IR spectrum)
+  e->max_items = std::min<size_t>(std::max<size_t>((size_t)max_channels * 64,
+                                                   budget_bytes / ((size_t)e->Q * e->B * 8)),
+                                  (size_t)1 << 26);
+  e->nclass = tanb::kMaxLog2Level - e->log2B;
   cudaError_t r = cudaSetDevice(ctx->device);
   if (r == cudaSuccess) r = tanb::eng_prepare();
   if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->lstream, cudaStreamNonBlocking);
   if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->upd_stream, cudaStreamNonBlocking);
   const size_t io = e->max_channels * e->B;
+  const size_t nlev = (size_t)e->nclass * e->max_channels;
   if (r == cudaSuccess) r = cudaMalloc(&e->arena, std::max<size_t>(budget_bytes, kAlign));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_chans, e->max_channels * sizeof(EngChan));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_items, e->max_items * sizeof(EngItem));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_levels, std::max<size_t>(1, nlev) * sizeof(EngLevel));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_block, 2 * sizeof(long long));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_upd, e->max_channels * sizeof(EngUpd));
+  if (r == cudaSuccess) r = cudaMalloc(&e->d_lupd, tanb::kMaxLevels * e->max_channels * sizeof(EngLvlUpd));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_tw, 2 * e->B * sizeof(float2));
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_chans, e->max_channels * sizeof(EngChan));
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_items, e->max_items * sizeof(EngItem));
+  if (r == cudaSuccess) r = cudaMallocHost(&e->h_levels, std::max<size_t>(1, nlev) * sizeof(EngLevel));
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_in, io * sizeof(float));
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_out, io * sizeof(float));
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_upd, e->max_channels * sizeof(EngUpd));
+  if (r == cudaSuccess) r = cudaMallocHost(&e->h_lupd, tanb::kMaxLevels * e->max_channels * sizeof(EngLvlUpd));
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_audio, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreate(&e->pa);
   if (r == cudaSuccess) r = cudaEventCreate(&e->pb);
+  e->d_tw_lv.assign(e->nclass, nullptr);
+  for (int c = 0; c < e->nclass && r == cudaSuccess; ++c)
+    r = cudaMalloc(&e->d_tw_lv[c], (size_t)(4 << (e->log2B + c)) * sizeof(float2));  // 2N entries
   if (r != cudaSuccess) {
     free_engine(e);
     delete e;
@@ -357,17 +861,30 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
                  cudaGetErrorString(r));
   }
   std::memset(e->h_chans, 0, e->max_channels * sizeof(EngChan));
-  for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0};
+  for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0, -1, 0};
+  for (size_t i = 0; i < nlev; ++i) {
+    e->h_levels[i] = EngLevel{};
+    e->h_levels[i].chan = -1;
+  }
   std::memset(e->h_in, 0, io * sizeof(float));
   std::memset(e->h_out, 0, io * sizeof(float));
   e->arena_alloc.reset(budget_bytes / kAlign);
   e->slot_alloc.reset(e->max_channels);
   e->item_alloc.reset(e->max_items);
+  e->lvl_alloc.assign(e->nclass, RangeAlloc());
+  for (auto& a : e->lvl_alloc) a.reset(e->max_channels);
+  e->lvl_hwm.assign(e->nclass, 0);
   std::vector<float2> tw(2 * e->B);
   tanb::make_twiddles(2 * e->B, tw.data());
-  r = cudaMemcpyAsync(e->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, e->stream);
+  r = cudaMemcpy(e->d_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
+  for (int c = 0; c < e->nclass && r == cudaSuccess; ++c) {
+    std::vector<float2> twl((size_t)4 << (e->log2B + c));
+    tanb::make_twiddles((int)twl.size(), twl.data());
+    r = cudaMemcpy(e->d_tw_lv[c], twl.data(), twl.size() * sizeof(float2), cudaMemcpyHostToDevice);
+  }
   if (r == cudaSuccess) r = cudaMemsetAsync(e->d_chans, 0, e->max_channels * sizeof(EngChan), e->stream);
   if (r == cudaSuccess) r = upload_items(e, 0, e->max_items);
+  if (r == cudaSuccess) r = upload_levels(e, 0, nlev);
   if (e->d_block) e->d_done = reinterpret_cast<unsigned int*>(e->d_block + 1);
   if (r == cudaSuccess) r = cudaMemsetAsync(e->d_block, 0, 2 * sizeof(long long), e->stream);
   if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
@@ -399,71 +916,14 @@ int32_t tanb_engine_release(tanb_engine* e) {
 
 int32_t tanb_engine_open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, int32_t* session,
                                  uint32_t* first_slot) {
-  if (!e || !session) return efail(TANB_INVALID_POINTER, "null argument");
-  std::lock_guard<std::mutex> lock(e->mu);
-  if (channels == 0 || ir_length == 0) return efail(TANB_INVALID_ARG, "channels and IR length must be > 0");
-  ENG_CUDA(cudaSetDevice(e->ctx->device));
-  Session s;
-  s.C = (int)channels;
-  s.L = (int)ir_length;
-  s.P = (int)std::max<uint32_t>(1, (ir_length + e->B - 1) / e->B);
-  // work items cover partitions [2, P); the head does partitions 0 and 1
-  s.nitem = s.P > 2 ? (s.P - 2 + e->Q - 1) / e->Q : 0;
-  s.arena_bytes = session_bytes(e, s.C, s.P, s.nitem);
-  if (!e->arena_alloc.alloc(s.arena_bytes / kAlign, &s.arena_off))
-    return efail(TANB_OUT_OF_MEMORY, "session of %u channels x %u taps needs %zu bytes; device budget exhausted",
-                 channels, ir_length, s.arena_bytes);
-  if (!e->slot_alloc.alloc(s.C, &s.slot0)) {
-    e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
-    return efail(TANB_OUT_OF_MEMORY, "no %u free channel slots", channels);
-  }
-  const size_t nit_total = (size_t)s.C * s.nitem;
-  if (nit_total && !e->item_alloc.alloc(nit_total, &s.item0)) {
-    e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
-    e->slot_alloc.release(s.slot0, s.C);
-    return efail(TANB_OUT_OF_MEMORY, "work-item table full");
-  }
-  ENG_CUDA(cudaStreamSynchronize(e->stream));  // pinned mirrors are rewritten below
-  char* base = e->arena + s.arena_off * kAlign;
-  ENG_CUDA(cudaMemsetAsync(base, 0, s.arena_bytes, e->stream));
-  const size_t B = e->B;
-  for (int j = 0; j < s.C; ++j) {
-    EngChan ch{};
-    ch.H = base;
-    base += align_up(2 * (size_t)s.P * B * spec_bytes(e->spec));
-    if (spec_scaled(e->spec)) {
-      ch.scale = reinterpret_cast<float*>(base);
-      base += align_up(2 * (size_t)s.P * 4);
-    }
-    ch.fdl = reinterpret_cast<float2*>(base);
-    base += align_up((size_t)s.P * B * fdl_bytes(e->spec));
-    ch.prev = reinterpret_cast<float*>(base);
-    base += align_up(B * 4);
-    ch.part = reinterpret_cast<float2*>(base);
-    base += align_up(4 * (size_t)s.nitem * B * 8);
-    ch.P = s.P;
-    ch.nitem = s.nitem;
-    ch.cur = 0;
-    ch.active = 0;
-    ch.pending = 0;
-    ch.run = 1;
-    e->h_chans[s.slot0 + j] = ch;
-    for (int r = 0; r < s.nitem; ++r) {
-      const int i0 = 2 + r * e->Q;
-      e->h_items[s.item0 + (size_t)j * s.nitem + r] = EngItem{(int)(s.slot0 + j), i0, std::min(s.P, i0 + e->Q), r};
-    }
-  }
-  ENG_CUDA(upload_chans(e, s.slot0, s.C));
-  ENG_CUDA(upload_items(e, s.item0, nit_total));
-  // the copies read the pinned mirrors, which the next block advances
-  ENG_CUDA(cudaStreamSynchronize(e->stream));
-  ENG_CUDA(cudaEventCreateWithFlags(&s.staged_ev, cudaEventDisableTiming));
-  s.id = e->next_id++;
-  e->sessions[s.id] = s;
-  update_hwm(e);
-  *session = s.id;
-  if (first_slot) *first_slot = (uint32_t)s.slot0;
-  return TANB_OK;
+  return open_session(e, channels, ir_length, 0, nullptr, nullptr, session, first_slot);
+}
+
+int32_t tanb_engine_open_session_nu(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint32_t nlevels,
+                                    const uint32_t* level_block, const uint32_t* level_parts, int32_t* session,
+                                    uint32_t* first_slot) {
+  if (!level_block || !level_parts || nlevels == 0) return efail(TANB_INVALID_POINTER, "null level schedule");
+  return open_session(e, channels, ir_length, nlevels, level_block, level_parts, session, first_slot);
 }
 
 int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
@@ -478,95 +938,36 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   const Session s = it->second;
   if (s.staged_ev) cudaEventDestroy(s.staged_ev);
   for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j] = EngChan{};
-  const size_t nit_total = (size_t)s.C * s.nitem;
-  for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0};
+  const size_t nit_total = (size_t)s.C * s.items_per_chan;
+  for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0, -1, 0};
+  for (size_t l = 0; l < s.lv.size(); ++l) {
+    const size_t first = (size_t)level_class(e, s.lv[l].log2N) * e->max_channels + s.lv_first[l];
+    for (int j = 0; j < s.C; ++j) {
+      e->h_levels[first + j] = EngLevel{};
+      e->h_levels[first + j].chan = -1;
+    }
+    ENG_CUDA(upload_levels(e, first, s.C));
+  }
   ENG_CUDA(upload_chans(e, s.slot0, s.C));
   ENG_CUDA(upload_items(e, s.item0, nit_total));
   ENG_CUDA(cudaStreamSynchronize(e->stream));  // the copies read the pinned mirrors
   e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
   e->slot_alloc.release(s.slot0, s.C);
-  e->item_alloc.release(s.item0, nit_total);
+  if (nit_total) e->item_alloc.release(s.item0, nit_total);
+  for (size_t l = 0; l < s.lv.size(); ++l) e->lvl_alloc[level_class(e, s.lv[l].log2N)].release(s.lv_first[l], s.C);
   e->sessions.erase(it);
   update_hwm(e);
   return TANB_OK;
 }
 
-static int32_t engine_update(tanb_engine* e, int32_t session, const float* const* ir, size_t n, bool device,
-                             uint32_t op) {
-  if (!e) return efail(TANB_INVALID_POINTER, "null engine");
-  if (!ir) return efail(TANB_INVALID_ARG, "ppBuffer == NULL");
-  std::lock_guard<std::mutex> ulock(e->upd_mu);
-  ENG_CUDA(cudaSetDevice(e->ctx->device));
-  // the previous upload's copies read the pinned staging rewritten below
-  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
-  Session s;
-  {
-    // read the session and choose the idle IR slots under the main lock: the
-    // audio path flips slots only under this lock, so the choice is consistent
-    std::lock_guard<std::mutex> lock(e->mu);
-    auto it = e->sessions.find(session);
-    if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
-    s = it->second;
-    if (n > (size_t)s.L) return efail(TANB_INVALID_ARG, "IR length %zu exceeds the session's %d", n, s.L);
-    for (int j = 0; j < s.C; ++j) {
-      if (!ir[j] && n) return efail(TANB_INVALID_ARG, "ppBuffer[%d] == NULL", j);
-      e->h_upd[j] = EngUpd{(int)(s.slot0 + j), 1 - e->h_chans[s.slot0 + j].active, nullptr, (int64_t)n};
-    }
-    it->second.staged = false;  // a newer upload supersedes one not yet committed
-    // The mirror (and so the idle-slot choice) already reflects every block
-    // enqueued on the audio stream; blocks still running there may read the
-    // chosen slot (a crossfade from it), so the transform waits for them.
-    ENG_CUDA(cudaEventRecord(e->ev_audio, e->stream));
-    ENG_CUDA(cudaStreamWaitEvent(e->upd_stream, e->ev_audio, 0));
-  }
-  const size_t PB = (size_t)s.P * e->B;
-  const size_t need = PB * s.C;
-  if (need > e->ir_cap) {
-    cudaFree(e->d_ir);
-    cudaFreeHost(e->h_ir);
-    e->d_ir = nullptr;
-    e->h_ir = nullptr;
-    e->ir_cap = 0;
-    ENG_CUDA(cudaMalloc(&e->d_ir, need * sizeof(float)));
-    ENG_CUDA(cudaMallocHost(&e->h_ir, need * sizeof(float)));
-    e->ir_cap = need;
-  }
-  if (device) {
-    // the transform reads the caller's rows in place
-    for (int j = 0; j < s.C; ++j) e->h_upd[j].src = ir[j];
-  } else if (n) {
-    // compact staging (row stride n) copied on the host pool, one transfer
-    auto copy_row = [&](int j) { tanb::copy_for_device(e->h_ir + (size_t)j * n, ir[j], n * sizeof(float)); };
-    if ((size_t)s.C * n * sizeof(float) >= (1u << 20))
-      tanb::host_parallel_for(s.C, copy_row);
-    else
-      for (int j = 0; j < s.C; ++j) copy_row(j);
-    ENG_CUDA(cudaMemcpyAsync(e->d_ir, e->h_ir, (size_t)s.C * n * sizeof(float), cudaMemcpyHostToDevice,
-                             e->upd_stream));
-    for (int j = 0; j < s.C; ++j) e->h_upd[j].src = e->d_ir + (size_t)j * n;
-  }
-  ENG_CUDA(cudaMemcpyAsync(e->d_upd, e->h_upd, s.C * sizeof(EngUpd), cudaMemcpyHostToDevice, e->upd_stream));
-  ENG_CUDA(tanb::eng_launch_ir(e->log2B, e->spec, e->d_chans, e->d_upd, s.C, s.P, e->d_tw, e->upd_stream));
-  ENG_CUDA(cudaEventRecord(s.staged_ev, e->upd_stream));
-  // BLOCK_UNTIL_READY: the new IR is ready for the next block when this returns
-  if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) ENG_CUDA(cudaEventSynchronize(s.staged_ev));
-  {
-    std::lock_guard<std::mutex> lock(e->mu);
-    auto it = e->sessions.find(session);
-    if (it != e->sessions.end()) it->second.staged = true;
-    e->n_ir += 1;
-  }
-  return TANB_OK;
-}
-
 int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const float* const* ir, size_t n,
                                        uint32_t operationFlags) {
-  return engine_update(e, session, ir, n, false, operationFlags);
+  return engine_update(e, session, ir, n, false, operationFlags, nullptr);
 }
 
 int32_t tanb_engine_update_response_td_device(tanb_engine* e, int32_t session, const float* const* ir,
                                               size_t n, uint32_t operationFlags) {
-  return engine_update(e, session, ir, n, true, operationFlags);
+  return engine_update(e, session, ir, n, true, operationFlags, nullptr);
 }
 
 int32_t tanb_engine_io(tanb_engine* e, float** in, float** out) {
@@ -603,12 +1004,9 @@ int32_t tanb_engine_process(tanb_engine* e) {
   std::lock_guard<std::mutex> lock(e->mu);
   ENG_CUDA(cudaSetDevice(e->ctx->device));
   if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
-  ENG_CUDA(commit_updates(e));
-  ENG_CUDA(ensure_graph(e));
-  ENG_CUDA(cudaGraphLaunch(e->graph_exec, e->stream));
+  const int32_t r = run_block(e, nullptr);
+  if (r != TANB_OK) return r;
   ENG_CUDA(cudaEventSynchronize(e->ev_out));
-  e->n_block += 1;
-  advance_mirror(e);
   return TANB_OK;
 }
 
@@ -618,21 +1016,11 @@ int32_t tanb_engine_process_device(tanb_engine* e, const float* in, float* out, 
   if (!out) return efail(TANB_INVALID_ARG, "null output");
   ENG_CUDA(cudaSetDevice(e->ctx->device));
   if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
-  if (ld == 0) ld = e->B;
-  ENG_CUDA(commit_updates(e));
-  if (e->profiling) ENG_CUDA(cudaEventRecord(e->pa, e->stream));
-  ENG_CUDA(enqueue_block(e, in, out, ld));
-  if (e->profiling) {
-    ENG_CUDA(cudaEventRecord(e->pb, e->stream));
-    ENG_CUDA(cudaEventSynchronize(e->pb));
-    float a = 0;
-    cudaEventElapsedTime(&a, e->pa, e->pb);
-    e->ms_block += a;
-    e->n_timed += 1;
-  }
-  e->n_block += 1;
-  advance_mirror(e);
-  return TANB_OK;
+  tanb::EngRows rows;
+  rows.in_base = in;
+  rows.out_base = out;
+  rows.ld = ld ? (int)ld : e->B;
+  return run_block(e, &rows);
 }
 
 int32_t tanb_engine_synchronize(tanb_engine* e) {
@@ -660,8 +1048,22 @@ int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
     // rows; the head reads input, history, the partial rows, partitions 0 and
     // 1 of the spectrum and X_{k-1}, and writes output, history and X_k
     const int64_t tail = (s.P > 2 ? (int64_t)(s.P - 2) * B * (sb + xb) : 0) + (int64_t)s.nitem * B * 8;
-    const int64_t head = 4 * B * 4 + (int64_t)s.nitem * B * 8 + (s.P > 1 ? 2 * B * sb + B * xb : B * sb) + B * xb;
-    block_bytes += (int64_t)s.C * (tail + head);
+    int64_t head = 4 * B * 4 + (int64_t)s.nitem * B * 8 + (s.P > 1 ? 2 * B * sb + B * xb : B * sb) + B * xb;
+    // non-uniform levels, per base block on average over their periods: the
+    // level items stream partitions [2, K) and write the partial rows; the
+    // level head reads its frame, the partial rows, partitions 0 and 1 and
+    // X_{j-1}, writes X_j and its N outputs; the base head writes the input
+    // history and reads one block of every level's ring
+    int64_t levels = 0;
+    if (!s.lv.empty()) head += B * 4 + (int64_t)s.lv.size() * B * 4;
+    for (const LevelSpec& l : s.lv) {
+      const int64_t N = 1LL << l.log2N, p = N / B;
+      const int64_t items = (l.K > 2 ? (int64_t)(l.K - 2) * N * (sb + xb) : 0) + (int64_t)l.ngroup * N * 8;
+      const int64_t lhead = 2 * N * 4 + (int64_t)l.ngroup * N * 8 + (l.K > 1 ? 2 * N * sb + N * xb : N * sb) +
+                            N * xb + N * 4;
+      levels += (items + lhead) / p;
+    }
+    block_bytes += (int64_t)s.C * (tail + head + levels);
   }
   out[0] = (int64_t)e->sessions.size();
   out[1] = chans;

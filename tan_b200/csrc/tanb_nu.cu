@@ -562,8 +562,8 @@ int32_t tanb_nu_schedule(uint32_t ir_length, uint32_t base_block, uint32_t max_b
                          uint32_t* level_block, uint32_t* level_parts) {
   if (!nlevels || !level_block || !level_parts) return nfail(TANB_INVALID_POINTER, "null argument");
   if (base_block < 32 || (base_block & (base_block - 1)) || max_block < base_block ||
-      (max_block & (max_block - 1)) || max_block > 8192 || ir_length == 0)
-    return nfail(TANB_INVALID_ARG, "blocks must be powers of two, 32 <= base <= max <= 8192");
+      (max_block & (max_block - 1)) || max_block > 16384 || ir_length == 0)
+    return nfail(TANB_INVALID_ARG, "blocks must be powers of two, 32 <= base <= max <= 16384");
   // two partitions per size while doubling, the largest size takes the rest
   uint32_t n = 0;
   long long off = 0;

@@ -92,6 +92,20 @@ class Engine:
             return rc, None
         return rc, Session(self, sid.value, first.value, channels, ir_length)
 
+    def open_session_nu(self, channels: int, ir_length: int, levels):
+        """Non-uniformly partitioned session; levels = [(block, partitions), ...]
+        with levels[0][0] == the engine block. Returns (AMF_RESULT, Session or None)."""
+        nl = len(levels)
+        blocks = (ctypes.c_uint32 * nl)(*[b for b, _ in levels])
+        parts = (ctypes.c_uint32 * nl)(*[k for _, k in levels])
+        sid = ctypes.c_int32(0)
+        first = ctypes.c_uint32(0)
+        rc = lib().tanb_engine_open_session_nu(self._h, channels, ir_length, nl, blocks, parts, ctypes.byref(sid),
+                                               ctypes.byref(first))
+        if rc != AMF_OK:
+            return rc, None
+        return rc, Session(self, sid.value, first.value, channels, ir_length)
+
     def write_input(self, first_slot: int, x: np.ndarray) -> int:
         """Copies the first `block` samples of each row of x (float32, C-contiguous
         rows) into the input buffer at slots first_slot, first_slot + 1, ..."""

@@ -10,7 +10,7 @@ from tan_b200.convolution import TANError
 
 
 @pytest.mark.parametrize("L,B0,Nmax", [(1 << 20, 128, 8192), (48000, 256, 4096), (100, 128, 1024),
-                                       (65536, 512, 512), (300000, 32, 8192)])
+                                       (65536, 512, 512), (300000, 32, 8192), (1 << 20, 128, 16384)])
 def test_schedule_shape_and_coverage(L, B0, Nmax):
     levels = nupols.schedule(L, B0, Nmax)
     assert 1 <= len(levels) <= 16
@@ -28,7 +28,7 @@ def test_schedule_shape_and_coverage(L, B0, Nmax):
         off += b * k
 
 
-@pytest.mark.parametrize("args", [(1000, 100, 1024), (1000, 256, 128), (1000, 16, 1024), (1000, 128, 16384),
+@pytest.mark.parametrize("args", [(1000, 100, 1024), (1000, 256, 128), (1000, 16, 1024), (1000, 128, 32768),
                                   (0, 128, 1024)])
 def test_schedule_rejects_invalid_arguments(args):
     with pytest.raises(TANError):
