@@ -100,12 +100,29 @@ int32_t tanb_convolution_release(tanb_convolution* conv);
 
 /* TANConvolution::Init / InitCpu / InitGpu (TrueAudioNext.h:134-146,
  * ConvolutionImpl.cpp:179-281, 1113-1259). `method` is a TANB_METHOD_* value,
- * optionally or-ed with TANB_METHOD_USE_PROCESS_FINALIZE. Every partitioned
- * and head/tail method runs the uniformly-partitioned engine; bufferSize must
- * be a power of two in [32, 8192] (the reference's GPU rule, :1136-1146). */
+ * optionally or-ed with TANB_METHOD_USE_PROCESS_FINALIZE. The uniform
+ * partitioned and head/tail methods run the uniformly-partitioned path; the
+ * non-uniform methods (TANB_METHOD_FFT_PARTITIONED_NONUNIFORM,
+ * _FHT_NONUNIFORM_PARTITIONED, _FFT_NONUNIFORM_PARTITIONED) run levels of
+ * growing block size along the IR (see tanb_convolution_init_nu); bufferSize
+ * must be a power of two in [32, 8192] (the reference's GPU rule, :1136-1146). */
 int32_t tanb_convolution_init(tanb_convolution* conv, uint32_t method,
                               uint32_t responseLengthInSamples,
                               uint32_t bufferSizeInSamples, uint32_t channels);
+
+/* No reference counterpart: Init of a non-uniform method
+ * (TANB_METHOD_FFT_PARTITIONED_NONUNIFORM, _FHT_NONUNIFORM_PARTITIONED or
+ * _FFT_NONUNIFORM_PARTITIONED) with an explicit level schedule, as
+ * tanb_engine_open_session_nu takes it (level_block[0] = bufferSize), for a
+ * schedule chosen by the autotuner. tanb_convolution_init picks a default
+ * schedule for those methods: two partitions per size doubling from the block
+ * to about L / 32 (at most 16384), the largest size taking the rest. The
+ * non-uniform methods run blocks in [128, 2048] (else AMF_NOT_SUPPORTED); an IR
+ * update takes effect on the next block, even for a channel that is free at
+ * the time (the uniform methods apply it at the channel's next running block). */
+int32_t tanb_convolution_init_nu(tanb_convolution* conv, uint32_t method, uint32_t responseLengthInSamples,
+                                 uint32_t bufferSizeInSamples, uint32_t channels, uint32_t nlevels,
+                                 const uint32_t* level_block, const uint32_t* level_parts);
 
 /* TANConvolution::Terminate (TrueAudioNext.h:148, ConvolutionImpl.cpp:307-352). */
 int32_t tanb_convolution_terminate(tanb_convolution* conv);

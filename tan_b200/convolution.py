@@ -72,6 +72,7 @@ SIGNATURES = {
     "tanb_create_convolution": (_i32, [_vp, ctypes.POINTER(_vp)]),
     "tanb_convolution_release": (_i32, [_vp]),
     "tanb_convolution_init": (_i32, [_vp, _u32, _u32, _u32, _u32]),
+    "tanb_convolution_init_nu": (_i32, [_vp, _u32, _u32, _u32, _u32, _u32, _u32p, _u32p]),
     "tanb_convolution_terminate": (_i32, [_vp]),
     "tanb_convolution_update_response_td": (_i32, [_vp, _pp, _sz, _u32p, _u32]),
     "tanb_convolution_update_response_td_device": (_i32, [_vp, _pp, _sz, _u32p, _u32]),
@@ -258,6 +259,19 @@ class TANConvolution:
 
     InitGpu = Init
     InitCpu = Init
+
+    def InitNonUniform(self, method: int, responseLengthInSamples: int, bufferSizeInSamples: int, channels: int,
+                       levels) -> int:
+        """Init of a non-uniform method with an explicit level schedule
+        [(block, partitions), ...], levels[0][0] == bufferSizeInSamples."""
+        nl = len(levels)
+        blocks = (ctypes.c_uint32 * nl)(*[b for b, _ in levels])
+        parts = (ctypes.c_uint32 * nl)(*[k for _, k in levels])
+        rc = lib().tanb_convolution_init_nu(self._h, method, responseLengthInSamples, bufferSizeInSamples, channels,
+                                            nl, blocks, parts)
+        if rc == AMF_OK:
+            self.channels, self.block = channels, bufferSizeInSamples
+        return rc
 
     def Terminate(self) -> int:
         return lib().tanb_convolution_terminate(self._h)

@@ -30,6 +30,7 @@
 #endif
 
 #include "../../include/tanb.h"
+#include "tanb_engine_host.h"
 #include "tanb_host_pool.h"
 #include "tanb_internal.h"
 
@@ -143,6 +144,18 @@ struct tanb_convolution {
   int* h_clip = nullptr;            // host-mapped clip flag
   std::vector<uint32_t> mix_groups; // group map the table holds
 
+  // Non-uniform methods: a private batched engine holding one non-uniformly
+  // partitioned session of C channels (slots [0, C)); the channel-flag
+  // bookkeeping stays here. Row tables for device rows: pinned [8 blocks][2][C]
+  // (inputs, outputs) and their device copy.
+  tanb_engine* nu_eng = nullptr;
+  int32_t nu_sess = -1;
+  float* nu_in = nullptr;    // the engine's pinned input rows [C][B]
+  float* nu_out = nullptr;   // the engine's pinned output rows [C][B]
+  const float** h_nu_tab = nullptr;
+  const float** d_nu_tab = nullptr;
+  std::vector<uint32_t> nu_blocks, nu_parts;
+
   // TIME_DOMAIN method state (history of `length` samples per channel)
   bool td = false;
   float* td_hist = nullptr;    // [C][length]
@@ -223,6 +236,13 @@ void drain_timed(tanb_convolution* v) {
 }
 
 void free_all(tanb_convolution* v) {
+  if (v->nu_eng) tanb_engine_release(v->nu_eng);
+  v->nu_eng = nullptr;
+  v->nu_sess = -1;
+  v->nu_in = v->nu_out = nullptr;
+  cudaFreeHost(v->h_nu_tab);
+  cudaFree(v->d_nu_tab);
+  v->h_nu_tab = v->d_nu_tab = nullptr;
   if (v->stream) cudaStreamSynchronize(v->stream);
   drain_timed(v);
   for (cudaEvent_t e : v->ev_pool) cudaEventDestroy(e);
@@ -330,6 +350,9 @@ int32_t td_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem 
                    size_t n, const uint32_t* flags, size_t* done);
 int channel_flags(tanb_convolution* v, const uint32_t* flags, std::vector<uint8_t>& run,
                   std::vector<uint8_t>& flush);
+int32_t nu_update(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags);
+int32_t nu_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
+                   size_t n, const uint32_t* flags, size_t* done);
 
 // Per-update descriptors, one upload: [ChanCtl x C][int channel list x C]
 // [8-byte aligned: IR row pointers x C].
@@ -345,6 +368,7 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   if (n > (size_t)v->L) return fail(TANB_INVALID_ARG, "IR length %zu exceeds Init length %d", n, v->L);
   TANB_CUDA(cudaSetDevice(v->ctx->device));
   if (v->td) return td_update(v, mem, ir, n, flags, op);
+  if (v->nu_eng) return nu_update(v, mem, ir, n, flags);
   if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
 
   const int C = v->C;
@@ -556,6 +580,10 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   if (!out) return fail(TANB_INVALID_ARG, "ppBufferOutput == NULL");
   TANB_CUDA(cudaSetDevice(v->ctx->device));
   if (v->td) return td_process(v, in_mem, in, out_mem, out, n, flags, done);
+  if (v->nu_eng) {
+    if (pcm) return fail(TANB_NOT_SUPPORTED, "the fused PCM pipeline runs the uniformly partitioned methods");
+    return nu_process(v, in_mem, in, out_mem, out, n, flags, done);
+  }
   if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
 
   const int B = v->B, C = v->C, P = v->P;
@@ -736,6 +764,173 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     if (v->finalize_mode && processed < nblocks && status == TANB_OK) {
       if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
     }
+  }
+  if (done) *done = processed * B;
+  return status;
+}
+
+// ---------------------------------------------------------------------------
+// Non-uniform methods (TANB_METHOD_FFT_PARTITIONED_NONUNIFORM and the FHT / FFT
+// NONUNIFORM_PARTITIONED GPU names; the reference's CPU form is
+// ConvolutionImpl.cpp:224-246, 2416-2428), on a private engine session.
+// ---------------------------------------------------------------------------
+
+constexpr int kNuBlocksPerChunk = kMaxBlocksPerChunk;
+
+// The default level schedule for an IR of L taps at block B: two partitions per
+// size, doubling from B up to about L / 16 (at most 16384), the largest size
+// taking the rest (tanb_nu_schedule).
+int32_t nu_default_schedule(uint32_t L, uint32_t B, std::vector<uint32_t>* blocks, std::vector<uint32_t>* parts) {
+  uint32_t mx = B;
+  while (mx < 16384 && (uint64_t)mx * 32 <= L) mx <<= 1;
+  uint32_t nl = 0;
+  blocks->assign(16, 0);
+  parts->assign(16, 0);
+  const int32_t r = tanb_nu_schedule(L, B, mx, &nl, blocks->data(), parts->data());
+  blocks->resize(nl);
+  parts->resize(nl);
+  return r;
+}
+
+int32_t nu_init(tanb_convolution* v, uint32_t L, uint32_t B, uint32_t C, uint32_t nlevels, const uint32_t* blocks,
+                const uint32_t* parts) {
+  if (B < 128 || B > 2048)
+    return fail(TANB_NOT_SUPPORTED, "the non-uniform methods run blocks in [128, 2048] (block %u)", B);
+  if (nlevels) {
+    v->nu_blocks.assign(blocks, blocks + nlevels);
+    v->nu_parts.assign(parts, parts + nlevels);
+  } else if (nu_default_schedule(L, B, &v->nu_blocks, &v->nu_parts) != TANB_OK) {
+    return TANB_INVALID_ARG;
+  }
+  const uint32_t nl = (uint32_t)v->nu_blocks.size();
+  const size_t bytes = tanb::engine_nu_session_bytes((int)B, TANB_SPECTRUM_FP32, (int)C, L, nl, v->nu_blocks.data(),
+                                                     v->nu_parts.data());
+  if (!bytes) return fail(TANB_INVALID_ARG, "invalid non-uniform level schedule");
+  int32_t r = tanb_engine_create(v->ctx, B, TANB_SPECTRUM_FP32, bytes, C, 0, &v->nu_eng);
+  if (r != TANB_OK) return r;
+  uint32_t first = 0;
+  r = tanb_engine_open_session_nu(v->nu_eng, C, L, nl, v->nu_blocks.data(), v->nu_parts.data(), &v->nu_sess, &first);
+  if (r == TANB_OK) r = tanb_engine_io(v->nu_eng, &v->nu_in, &v->nu_out);
+  if (r != TANB_OK) {
+    const std::string msg = tanb_last_error();
+    free_all(v);
+    return fail(r, "%s", msg.c_str());
+  }
+  const size_t tab = (size_t)kNuBlocksPerChunk * 2 * C * sizeof(float*);
+  cudaError_t e = cudaMallocHost(&v->h_nu_tab, tab);
+  if (e == cudaSuccess) e = cudaMalloc(&v->d_nu_tab, tab);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&v->ev_stage, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(v->ev_stage, (cudaStream_t)tanb_engine_stream(v->nu_eng));
+  if (e != cudaSuccess) {
+    free_all(v);
+    return fail(e == cudaErrorMemoryAllocation ? TANB_OUT_OF_MEMORY : TANB_FAIL, "non-uniform setup: %s",
+                cudaGetErrorString(e));
+  }
+  int64_t info[8];
+  tanb_engine_info(v->nu_eng, info);
+  v->dev_bytes = (size_t)info[4];
+  return TANB_OK;
+}
+
+// UpdateResponseTD: channels flagged STOP_INPUT keep their IR, FLUSH_STREAM
+// channels are flushed; the transform completes before this returns, so the
+// new IR takes effect (with the one-block crossfade) on the next block.
+int32_t nu_update(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags) {
+  const int C = v->C;
+  std::vector<uint8_t> mask(C, 1);
+  for (int c = 0; c < C; ++c) {
+    if (flags && (flags[c] & kFlush)) {
+      const int32_t r = tanb::engine_flush_channel(v->nu_eng, v->nu_sess, c);
+      if (r != TANB_OK) return r;
+    }
+    if (flags && (flags[c] & kStopInput)) mask[c] = 0;
+  }
+  return tanb::engine_update_channels(v->nu_eng, v->nu_sess, ir, n, mem == Mem::Device,
+                                      TANB_OPERATION_FLAG_BLOCK_UNTIL_READY, mask.data());
+}
+
+int32_t nu_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
+                   size_t n, const uint32_t* flags, size_t* done) {
+  const int B = v->B, C = v->C;
+  const size_t nblocks = n / (size_t)B;
+  cudaStream_t st = (cudaStream_t)tanb_engine_stream(v->nu_eng);
+  // Host rows go through the engine's pinned rows, one block at a time (its
+  // graph when both sides are host rows); device rows through row tables,
+  // written for a chunk of blocks and uploaded once before the chunk's blocks.
+  const bool host_io = in_mem == Mem::Host || out_mem == Mem::Host;
+  const bool tables = in_mem == Mem::Device || out_mem == Mem::Device;
+  size_t processed = 0;
+  int32_t status = TANB_OK;
+  while (processed < nblocks && status == TANB_OK) {
+    const int nb = host_io ? 1 : (int)std::min<size_t>(kNuBlocksPerChunk, nblocks - processed);
+    TANB_CUDA(cudaEventSynchronize(v->ev_stage));  // the previous chunk's tables have been uploaded
+    // pass 1: channel flags of every block of the chunk and its row tables
+    int filled = 0;
+    for (int b = 0; b < nb; ++b) {
+      std::vector<uint8_t>& run = v->scr_run_b[b];
+      if (channel_flags(v, flags, run, v->scr_flush) == 0) {
+        status = fail(TANB_WRONG_STATE, "no running channels");
+        break;
+      }
+      v->scr_flush_b[b].clear();
+      for (int c = 0; c < C; ++c)
+        if (v->scr_flush[c]) v->scr_flush_b[b].push_back(c);
+      const size_t blk = processed + b;
+      const float** tin = v->h_nu_tab + (size_t)(2 * b) * C;
+      const float** tout = tin + C;
+      for (int c = 0; c < C; ++c) {
+        if (in_mem == Mem::Device) tin[c] = (run[c] && in[c]) ? in[c] + blk * B : nullptr;
+        if (out_mem == Mem::Device) tout[c] = (run[c] && out[c]) ? out[c] + blk * B : nullptr;
+      }
+      ++filled;
+    }
+    if (filled && tables)
+      TANB_CUDA(cudaMemcpyAsync(v->d_nu_tab, v->h_nu_tab, (size_t)2 * filled * C * sizeof(float*),
+                                cudaMemcpyHostToDevice, st));
+    // pass 2: flushes (ordered on the engine's stream before the block), input
+    // rows, the block, output rows
+    for (int b = 0; b < filled; ++b) {
+      const size_t blk = processed + b;
+      const std::vector<uint8_t>& run = v->scr_run_b[b];
+      for (int c : v->scr_flush_b[b]) {
+        const int32_t r = tanb::engine_flush_channel(v->nu_eng, v->nu_sess, c);
+        if (r != TANB_OK) return r;
+      }
+      tanb::EngRows rows;
+      rows.ld = B;
+      if (in_mem == Mem::Host) {
+        // free channels and missing rows read silence
+        for (int c = 0; c < C; ++c) {
+          float* row = v->nu_in + (size_t)c * B;
+          if (run[c] && in[c])
+            tanb::copy_rows_for_device(row, in[c] + blk * B, B * sizeof(float));
+          else
+            std::memset(row, 0, B * sizeof(float));
+        }
+        tanb::copy_for_device_fence();
+        rows.in_base = v->nu_in;
+      } else {
+        rows.in_tab = v->d_nu_tab + (size_t)(2 * b) * C;
+      }
+      if (out_mem == Mem::Host)
+        rows.out_base = v->nu_out;
+      else
+        rows.out_tab = reinterpret_cast<float* const*>(const_cast<float**>(v->d_nu_tab + (size_t)(2 * b + 1) * C));
+      int32_t r;
+      if (in_mem == Mem::Host && out_mem == Mem::Host) {
+        r = tanb_engine_process(v->nu_eng);  // the engine's graph over its pinned rows; waits for the output
+      } else {
+        r = tanb::engine_process_rows(v->nu_eng, rows);
+        if (r == TANB_OK && host_io) TANB_CUDA(cudaStreamSynchronize(st));  // pinned rows reused next block
+      }
+      if (r != TANB_OK) return r;
+      if (out_mem == Mem::Host)
+        for (int c = 0; c < C; ++c)
+          if (run[c] && out[c]) std::memcpy(out[c] + blk * B, v->nu_out + (size_t)c * B, B * sizeof(float));
+    }
+    if (tables) TANB_CUDA(cudaEventRecord(v->ev_stage, st));
+    processed += filled;
+    v->blocks += filled;
   }
   if (done) *done = processed * B;
   return status;
@@ -972,7 +1167,12 @@ int32_t tanb_convolution_release(tanb_convolution* v) {
   return TANB_OK;
 }
 
-int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, uint32_t B, uint32_t C) {
+}  // extern "C"
+
+namespace {
+
+int32_t init_impl(tanb_convolution* v, uint32_t method, uint32_t L, uint32_t B, uint32_t C, uint32_t nlevels,
+                  const uint32_t* level_block, const uint32_t* level_parts) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
   std::lock_guard<std::mutex> lock(v->mu);
   if (v->terminated) return fail(TANB_WRONG_STATE, "Cannot initialize after termination");
@@ -1001,6 +1201,34 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
 
   cudaError_t e = cudaSetDevice(v->ctx->device);
   if (e != cudaSuccess) return fail(TANB_NO_DEVICE, "cudaSetDevice: %s", cudaGetErrorString(e));
+  auto host_state = [&] {
+    v->active.assign(C, 0);
+    v->pending.assign(C, 0);
+    v->slot_new.assign(C, 1);
+    v->tail_left.assign(C, 0);
+    v->available.assign(C, 0);
+    v->flushed.assign(C, 0);
+    v->scr_run.assign(C, 0);
+    v->scr_flush.assign(C, 0);
+    v->scr_run_b.assign(kMaxBlocksPerChunk, std::vector<uint8_t>(C, 0));
+    v->scr_flush_b.assign(kMaxBlocksPerChunk, std::vector<int>());
+    for (auto& f : v->scr_flush_b) f.reserve(C);
+    v->scr_cur_b.assign(kMaxBlocksPerChunk, 0);
+    v->cur = 0;
+    v->blocks = 0;
+  };
+  const bool nonuniform = base == TANB_METHOD_FFT_PARTITIONED_NONUNIFORM ||
+                          base == TANB_METHOD_FHT_NONUNIFORM_PARTITIONED ||
+                          base == TANB_METHOD_FFT_NONUNIFORM_PARTITIONED;
+  if (nonuniform) {
+    const int32_t r = nu_init(v, L, B, C, nlevels, level_block, level_parts);
+    if (r != TANB_OK) return r;
+    v->finalize_mode = false;  // the head and every level run in one graph launch per block
+    host_state();
+    v->initialized = true;
+    return TANB_OK;
+  }
+  if (nlevels) return fail(TANB_INVALID_ARG, "a level schedule needs a non-uniform method");
   if ((e = tanb::prepare_kernels()) != cudaSuccess) return fail(TANB_FAIL, "kernel setup: %s", cudaGetErrorString(e));
   if ((e = cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking)) != cudaSuccess)
     return fail(TANB_FAIL, "stream: %s", cudaGetErrorString(e));
@@ -1080,24 +1308,25 @@ int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, 
     return fail(TANB_FAIL, "mapped host words: %s", cudaGetErrorString(e));
   }
   v->tiling = default_tiling(B, v->P);
-  v->active.assign(C, 0);
-  v->pending.assign(C, 0);
-  v->slot_new.assign(C, 1);
-  v->tail_left.assign(C, 0);
-  v->available.assign(C, 0);
-  v->flushed.assign(C, 0);
+  host_state();
   v->pdesc.resize(C <= tanb::kParamChannels ? kMaxBlocksPerChunk : 0);
   v->sdesc.resize(C <= tanb::kParamChannels ? kMaxBlocksPerChunk : 0);
-  v->scr_run.assign(C, 0);
-  v->scr_flush.assign(C, 0);
-  v->scr_run_b.assign(kMaxBlocksPerChunk, std::vector<uint8_t>(C, 0));
-  v->scr_flush_b.assign(kMaxBlocksPerChunk, std::vector<int>());
-  for (auto& f : v->scr_flush_b) f.reserve(C);
-  v->scr_cur_b.assign(kMaxBlocksPerChunk, 0);
-  v->cur = 0;
-  v->blocks = 0;
   v->initialized = true;
   return TANB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t tanb_convolution_init(tanb_convolution* v, uint32_t method, uint32_t L, uint32_t B, uint32_t C) {
+  return init_impl(v, method, L, B, C, 0, nullptr, nullptr);
+}
+
+int32_t tanb_convolution_init_nu(tanb_convolution* v, uint32_t method, uint32_t L, uint32_t B, uint32_t C,
+                                 uint32_t nlevels, const uint32_t* level_block, const uint32_t* level_parts) {
+  if (!level_block || !level_parts || nlevels == 0) return fail(TANB_INVALID_POINTER, "null level schedule");
+  return init_impl(v, method, L, B, C, nlevels, level_block, level_parts);
 }
 
 int32_t tanb_convolution_update_response_td(tanb_convolution* v, const float* const* ir, size_t n,
@@ -1150,7 +1379,8 @@ int32_t tanb_convolution_process_mix_pcm16(tanb_convolution* v, const int16_t* c
   {
     std::lock_guard<std::mutex> lock(v->mu);
     if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "Process before Init");
-    if (v->td) return fail(TANB_NOT_SUPPORTED, "the fused PCM pipeline runs the partitioned methods");
+    if (v->td || v->nu_eng)
+      return fail(TANB_NOT_SUPPORTED, "the fused PCM pipeline runs the uniformly partitioned methods");
     C = v->C;
   }
   if (ngroups == 0 || ngroups > (uint32_t)C) return fail(TANB_INVALID_ARG, "ngroups must be in [1, channels]");
@@ -1212,12 +1442,16 @@ int32_t tanb_convolution_synchronize(tanb_convolution* v) {
   std::lock_guard<std::mutex> lock(v->mu);
   if (!v->initialized) return TANB_OK;
   TANB_CUDA(cudaSetDevice(v->ctx->device));
+  if (v->nu_eng) return tanb_engine_synchronize(v->nu_eng);
   TANB_CUDA(cudaStreamSynchronize(v->stream));
   if (v->h_err && *v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
   return TANB_OK;
 }
 
-void* tanb_convolution_stream(tanb_convolution* v) { return v ? (void*)v->stream : nullptr; }
+void* tanb_convolution_stream(tanb_convolution* v) {
+  if (v && v->nu_eng) return tanb_engine_stream(v->nu_eng);
+  return v ? (void*)v->stream : nullptr;
+}
 
 int32_t tanb_convolution_tiling(tanb_convolution* v, int32_t index, int32_t out[3]) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
@@ -1257,7 +1491,7 @@ int32_t tanb_convolution_profile_read(tanb_convolution* v, int64_t counts[6], do
 
 int32_t tanb_convolution_info(tanb_convolution* v, int64_t out[4]) {
   if (!v || !out) return fail(TANB_INVALID_POINTER, "null argument");
-  out[0] = v->P;
+  out[0] = v->nu_eng ? (int64_t)v->nu_parts[0] : v->P;  // non-uniform: the base level's partitions
   out[1] = v->B;
   out[2] = v->C;
   out[3] = (int64_t)v->dev_bytes;

@@ -109,6 +109,11 @@ class RangeAlloc {
       }
     }
   }
+  // extends the range to [0, size) (size >= the current size)
+  void grow(size_t size) {
+    if (size > size_) release(size_, size - size_);
+    size_ = std::max(size_, size);
+  }
   // one past the highest allocated unit
   size_t high_water() const {
     if (free_.empty()) return size_;
@@ -397,7 +402,7 @@ cudaError_t enqueue_block(tanb_engine* e, const tanb::EngRows& rows, unsigned du
 }
 
 std::vector<size_t> graph_key(const tanb_engine* e) {
-  std::vector<size_t> k{e->nslots_hwm, e->nitems_hwm};
+  std::vector<size_t> k{e->nslots_hwm, e->nitems_hwm, e->max_items};
   k.insert(k.end(), e->lvl_hwm.begin(), e->lvl_hwm.end());
   return k;
 }
@@ -494,6 +499,39 @@ int32_t make_levels(const tanb_engine* e, uint32_t ir_length, uint32_t nlevels, 
   return TANB_OK;
 }
 
+// Grows the work-item table to hold at least `need` more items (a new device
+// table and pinned mirror with the old contents; the graphs, which hold the
+// table's address, are rebuilt on their next use). Caller holds mu and has
+// drained the audio stream.
+cudaError_t grow_items(tanb_engine* e, size_t need) {
+  const size_t cap = std::max(2 * e->max_items, e->max_items + need);
+  EngItem* d = nullptr;
+  EngItem* h = nullptr;
+  cudaError_t r = cudaMalloc(&d, cap * sizeof(EngItem));
+  if (r == cudaSuccess) r = cudaMallocHost(&h, cap * sizeof(EngItem));
+  if (r != cudaSuccess) {
+    cudaFree(d);
+    cudaFreeHost(h);
+    return r;
+  }
+  std::memcpy(h, e->h_items, e->max_items * sizeof(EngItem));
+  for (size_t i = e->max_items; i < cap; ++i) h[i] = EngItem{-1, 0, 0, 0, -1, 0};
+  r = cudaMemcpyAsync(d, h, cap * sizeof(EngItem), cudaMemcpyHostToDevice, e->stream);
+  if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
+  if (r != cudaSuccess) {
+    cudaFree(d);
+    cudaFreeHost(h);
+    return r;
+  }
+  cudaFree(e->d_items);
+  cudaFreeHost(e->h_items);
+  e->d_items = d;
+  e->h_items = h;
+  e->max_items = cap;
+  e->item_alloc.grow(cap);
+  return cudaSuccess;
+}
+
 int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint32_t nlevels,
                      const uint32_t* level_block, const uint32_t* level_parts, int32_t* session,
                      uint32_t* first_slot) {
@@ -525,9 +563,13 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
   }
   const size_t nit_total = (size_t)s.C * s.items_per_chan;
   if (nit_total && !e->item_alloc.alloc(nit_total, &s.item0)) {
-    e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
-    e->slot_alloc.release(s.slot0, s.C);
-    return efail(TANB_OUT_OF_MEMORY, "work-item table full");
+    cudaError_t r = cudaStreamSynchronize(e->stream);
+    if (r == cudaSuccess) r = grow_items(e, nit_total);
+    if (r != cudaSuccess || !e->item_alloc.alloc(nit_total, &s.item0)) {
+      e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
+      e->slot_alloc.release(s.slot0, s.C);
+      return efail(TANB_OUT_OF_MEMORY, "work-item table full");
+    }
   }
   s.lv_first.assign(s.lv.size(), 0);
   for (size_t l = 0; l < s.lv.size(); ++l) {
@@ -788,6 +830,19 @@ int32_t engine_flush_channel(tanb_engine* e, int32_t session, int channel) {
   return TANB_OK;
 }
 
+size_t engine_nu_session_bytes(int block, int spectrum, int channels, uint32_t ir_length, uint32_t nlevels,
+                               const uint32_t* level_block, const uint32_t* level_parts) {
+  tanb_engine probe;  // shape only: no device state
+  probe.B = block;
+  while ((1 << probe.log2B) < block) ++probe.log2B;
+  probe.spec = spectrum;
+  std::vector<LevelSpec> lv;
+  int P = 0, rin = 0;
+  if (make_levels(&probe, ir_length, nlevels, level_block, level_parts, &lv, &P, &rin) != TANB_OK) return 0;
+  const int nitem = P > 2 ? (P - 2 + probe.Q - 1) / probe.Q : 0;
+  return chan_bytes(&probe, P, nitem, lv, rin) * (size_t)channels;
+}
+
 int32_t engine_process_rows(tanb_engine* e, const EngRows& rows) {
   std::lock_guard<std::mutex> lock(e->mu);
   ENG_CUDA(cudaSetDevice(e->ctx->device));
@@ -816,11 +871,9 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   e->Q = (int)partitions_per_item;
   e->budget = budget_bytes;
   e->max_channels = max_channels;
-  // work items: 64 per channel slot, or as many as the budget can feed (an
-  // item streams at least Q partitions x B bins x 8 bytes of IR spectrum)
-  e->max_items = std::min<size_t>(std::max<size_t>((size_t)max_channels * 64,
-                                                   budget_bytes / ((size_t)e->Q * e->B * 8)),
-                                  (size_t)1 << 26);
+  // work items: 64 per channel slot to start with; the table grows when a
+  // session needs more (non-uniform levels take one item per bin slice)
+  e->max_items = (size_t)max_channels * 64;
   e->nclass = tanb::kMaxLog2Level - e->log2B;
   cudaError_t r = cudaSetDevice(ctx->device);
   if (r == cudaSuccess) r = tanb::eng_prepare();

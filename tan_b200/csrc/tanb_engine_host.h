@@ -17,6 +17,10 @@ int32_t engine_update_channels(tanb_engine* e, int32_t session, const float* con
 // Clears channel `channel` of the session: delay lines, history, partial sums,
 // level rings (the IR spectra stay), on the audio stream.
 int32_t engine_flush_channel(tanb_engine* e, int32_t session, int channel);
+// Arena bytes a non-uniform session of this shape takes in an engine of
+// `block` and `spectrum` (0 when the schedule is invalid).
+size_t engine_nu_session_bytes(int block, int spectrum, int channels, uint32_t ir_length, uint32_t nlevels,
+                               const uint32_t* level_block, const uint32_t* level_parts);
 // One block with the given rows (direct launches on the audio stream).
 int32_t engine_process_rows(tanb_engine* e, const EngRows& rows);
 
