@@ -258,6 +258,15 @@ int32_t tanb_convolution_profile(tanb_convolution* conv, int32_t enable);
  * summed device milliseconds. Waits for the timed launches to finish. */
 int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6], double ms[3]);
 
+/* No reference counterpart; a test hook for failure handling. Sets how many
+ * times the tail kernel's cp.async.bulk pipelines poll a stage's barrier
+ * before giving up (default and maximum 2^20; negative: the default). On a
+ * timeout the kernel records the error, waits with the full bound for its
+ * copies in flight and exits; Process or Synchronize then return AMF_FAIL.
+ * A bound of 0 makes the first wait give up at once, so that the failure
+ * path runs without any fault. */
+int32_t tanb_convolution_set_wait_limit(tanb_convolution* conv, int32_t polls);
+
 /* ---------------------------------------------------------------------------
  * Batched engine. No single reference counterpart: it is the serving form of
  * the same path -- many TANConvolution-equivalent sessions (C channels, IR

@@ -88,6 +88,7 @@ SIGNATURES = {
     "tanb_convolution_info": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_convolution_tiling": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_int32)]),
     "tanb_convolution_profile": (_i32, [_vp, _i32]),
+    "tanb_convolution_set_wait_limit": (_i32, [_vp, _i32]),
     "tanb_convolution_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_engine_create": (_i32, [_vp, _u32, _u32, ctypes.c_uint64, _u32, _u32, ctypes.POINTER(_vp)]),
     "tanb_engine_release": (_i32, [_vp]),

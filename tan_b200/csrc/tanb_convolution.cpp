@@ -1466,6 +1466,14 @@ int32_t tanb_convolution_tiling(tanb_convolution* v, int32_t index, int32_t out[
   return TANB_OK;
 }
 
+int32_t tanb_convolution_set_wait_limit(tanb_convolution* v, int32_t polls) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  std::lock_guard<std::mutex> lock(v->mu);
+  if (polls < 0) polls = tanb::kBulkWaitLimit;
+  v->ds.wait_limit = std::min(polls, tanb::kBulkWaitLimit);
+  return TANB_OK;
+}
+
 int32_t tanb_convolution_profile(tanb_convolution* v, int32_t enable) {
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
   std::lock_guard<std::mutex> lock(v->mu);

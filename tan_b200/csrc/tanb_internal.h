@@ -56,6 +56,12 @@ struct ChanCtl {
   int32_t slot_new;
 };
 
+// Error codes a kernel writes to DevState::err.
+enum : int { kErrNone = 0, kErrBulkWaitTimeout = 1 };
+
+// Polls of an mbarrier before a bounded wait gives up (about a second).
+constexpr int kBulkWaitLimit = 1 << 20;
+
 // Device-resident state of one convolution object.
 // Spectra are "packed" half spectra of a 2B-point real FFT: B complex bins,
 // bin 0 holding (X[0].re, X[B].re) -- both are real.
@@ -71,10 +77,13 @@ struct DevState {
   const float2* tw;  // W_N^j, N = 2B, j in [0, N)
   int* err;       // device-visible error word (host-mapped); nonzero after a
                   // bounded wait in a kernel gave up (kErr* codes)
+  int wait_limit = kBulkWaitLimit;  // polls of a bounded wait for a pipeline
+                                    // stage before it gives up (a test hook
+                                    // lowers it; draining in-flight copies
+                                    // always uses kBulkWaitLimit)
 };
 
-// Error codes a kernel writes to DevState::err.
-enum : int { kErrNone = 0, kErrBulkWaitTimeout = 1 };
+
 
 __host__ __device__ inline size_t h_index(const DevState& s, int c, int slot, int part) {
   return (((size_t)c * 2 + slot) * s.P + part) * s.B;

@@ -610,7 +610,6 @@ __global__ void __launch_bounds__(UX* SY)
 // holding them in registers. Waits are bounded: on timeout the kernel records
 // kErrBulkWaitTimeout, waits (bounded) for its copies in flight and returns.
 // No multicast; every load reads this GPU's own memory.
-constexpr int kBulkWaitLimit = 1 << 20;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -624,8 +623,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < kBulkWaitLimit; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit) {
+  for (int it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -693,7 +692,7 @@ __global__ void __launch_bounds__(BR / 2)
   for (; q < nchunks; ++q) {
     const int st = q % NS;
     const uint32_t parity = (uint32_t)(q / NS) & 1u;
-    const bool landed = mbar_wait(smem_addr(&bars[st]), parity);
+    const bool landed = mbar_wait(smem_addr(&bars[st]), parity, s.wait_limit);
     if (__syncthreads_or(!landed)) {  // CTA-uniform decision
       ok = false;
       break;
@@ -711,7 +710,8 @@ __global__ void __launch_bounds__(BR / 2)
     // record the failure, then let copies already issued land before exiting
     if (tid == 0) {
       atomicExch(s.err, kErrBulkWaitTimeout);
-      for (int r = q; r < nchunks && r < q + NS; ++r) mbar_wait(smem_addr(&bars[r % NS]), (uint32_t)(r / NS) & 1u);
+      for (int r = q; r < nchunks && r < q + NS; ++r)
+        mbar_wait(smem_addr(&bars[r % NS]), (uint32_t)(r / NS) & 1u, kBulkWaitLimit);
     }
     __syncthreads();
     return;

@@ -57,7 +57,7 @@ def percentiles(lat_ms):
 
 def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256, spectrum=eng.SPECTRUM_FP32,
           budget=150 << 30, max_channels=1 << 16, ch_range=(1, 8), len_range=(8192, 524288), seed=20261203 + 4,
-          prefill=True):
+          prefill=True, trace=0):
     """Runs the serving loop; returns a dict of latency and occupancy statistics.
 
     The audio thread admits and retires sessions and runs one engine block per
@@ -66,7 +66,13 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
     transform finished) and closes retired sessions, as the reference's update
     thread does for TANConvolution. The audio input buffer is filled once (the
     caller's audio I/O would write it in place); the block latency is the host
-    wall time of admission + engine block."""
+    wall time of admission + engine block.
+
+    trace=N records the first N sessions admitted in the loop (not prefilled):
+    they live to the end, their IR swaps are made on the audio thread with
+    BLOCK_UNTIL_READY (so each lands on a known block), and their input rows,
+    swap IRs and output rows are returned under "traces", so that a caller can
+    check each against the same session run alone."""
     import queue
     import threading
 
@@ -104,8 +110,10 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
     lat, chans = [], []
     t = 0.0
     next_arrival = g.exponential(1.0 / rate)
+    traces = {}  # id -> {"session", "x", "events": {block: ir}, "y": [blocks]}
+    k_now = 0
 
-    def new_session(now):
+    def new_session(now, traced=False):
         nonlocal refused, admitted
         C = int(g.integers(ch_range[0], ch_range[1] + 1))
         L = int(np.exp(g.uniform(np.log(len_range[0]), np.log(len_range[1]))))
@@ -114,6 +122,13 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
             refused += 1
             return
         admitted += 1
+        if traced:
+            ir = pool.get(g, C, L)
+            assert s.update_response_td(ir, block_until_ready=True) == cv.AMF_OK
+            traces[s.id] = {"channels": C, "ir_length": L, "x": e.inp[s.slots].copy(), "events": {0: ir},
+                            "start": k_now, "y": []}
+            live[s.id] = [s, float("inf"), now + g.exponential(1.0 / swap_rate)]
+            return
         work.put(("ir", s))
         live[s.id] = [s, now + g.exponential(lifetime), now + g.exponential(1.0 / swap_rate)]
 
@@ -123,19 +138,28 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
         while not work.empty():
             time.sleep(0.01)
     for k in range(nblocks):
+        k_now = k
         t0 = time.perf_counter()
         while next_arrival <= t:
-            new_session(t)
+            new_session(t, traced=len(traces) < trace)
             next_arrival += g.exponential(1.0 / rate)
         for sid in [sid for sid, v in live.items() if v[1] <= t]:
             work.put(("close", live.pop(sid)[0]))
-        for v in live.values():
+        for sid, v in live.items():
             if v[2] <= t:
-                work.put(("ir", v[0]))
+                if sid in traces:
+                    tr = traces[sid]
+                    ir = pool.get(g, tr["channels"], tr["ir_length"])
+                    assert v[0].update_response_td(ir, block_until_ready=True) == cv.AMF_OK
+                    tr["events"][k - tr["start"]] = ir
+                else:
+                    work.put(("ir", v[0]))
                 v[2] = t + g.exponential(1.0 / swap_rate)
         rc = e.process()
         assert rc == cv.AMF_OK, cv.last_error()
         lat.append(1000.0 * (time.perf_counter() - t0))
+        for sid, tr in traces.items():
+            tr["y"].append(e.out[live[sid][0].slots].copy())
         chans.append(e.info()["channels"])
         t += dt
     work.put(None)
@@ -144,11 +168,14 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
     info = e.info()
     e.release()
     lat = np.asarray(lat)
-    return {"blocks": nblocks, "deadline_ms": deadline_ms, "latency_ms": percentiles(lat),
-            "deadline_misses": int((lat > deadline_ms).sum()), "concurrent_channels_mean": float(np.mean(chans)),
-            "concurrent_channels_max": int(np.max(chans)), "admitted": admitted, "refused": refused,
-            "control_errors": errors[:5], "arena_bytes_end": info["arena_bytes"],
-            "spectrum": ["fp32", "fp16", "bf16", "fp24"][spectrum]}
+    out = {"blocks": nblocks, "deadline_ms": deadline_ms, "latency_ms": percentiles(lat),
+           "deadline_misses": int((lat > deadline_ms).sum()), "concurrent_channels_mean": float(np.mean(chans)),
+           "concurrent_channels_max": int(np.max(chans)), "admitted": admitted, "refused": refused,
+           "control_errors": errors[:5], "arena_bytes_end": info["arena_bytes"],
+           "spectrum": ["fp32", "fp16", "bf16", "fp24"][spectrum]}
+    if trace:
+        out["traces"] = [dict(tr, y=np.concatenate(tr["y"], axis=1)) for tr in traces.values()]
+    return out
 
 
 def _block_latencies_batched(ctx, nsess, C, L, block, spectrum, blocks, g, pool):
