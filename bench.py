@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--cpu-sample-s", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-capacity", action="store_true")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the sub-records of the other configurations (uneven batch, non-uniform, serving)")
     return p.parse_args()
 
 
@@ -582,6 +584,7 @@ def run_ours(args):
         from tan_b200 import serving
 
         cp = serving.capacity(ctx, "plain", 4, 48000, 256, blocks=150)
+        c1 = serving.capacity(ctx, "plain_one", 4, 48000, 256, blocks=100, start=512)
         cb = serving.capacity(ctx, "batched", 4, 48000, 256, blocks=150)
         c24 = serving.capacity(ctx, "batched", 4, 48000, 256, spectrum=eng.SPECTRUM_FP24, blocks=150)
         capacity = {"what": "max channels (sessions of 4 ch, IR 48000 = 1 s, block 256 @ 48 kHz) with p99 "
@@ -591,7 +594,10 @@ def run_ours(args):
                     "batched_fp24": c24["max_realtime_channels"],
                     "fp24_what": "IR spectra and delay line stored in 24 bits (error vs FP64 about -100 dB, "
                                  "tests/test_gpu_engine.py), FP32 accumulation",
-                    "ratio_fp24": c24["max_realtime_channels"] / max(1, cp["max_realtime_channels"])}
+                    "ratio_fp24": c24["max_realtime_channels"] / max(1, cp["max_realtime_channels"]),
+                    "plain_one_object_fp32": c1["max_realtime_channels"],
+                    "plain_one_object_what": "one drop-in TANConvolution holding every channel (host rows)",
+                    "ratio_vs_one_object": cb["max_realtime_channels"] / max(1, c1["max_realtime_channels"])}
         # the MAC where its working set is far above L2: the batched engine's
         # block launch at the capacity found above
         rs = serving.mac_roofline(ctx, cb["max_realtime_channels"], 4, 48000, 256)
@@ -601,6 +607,15 @@ def run_ours(args):
                             "what": "batched FP32 engine at its real-time capacity (sessions of 4 ch, IR 48000, "
                                     "block 256), device I/O, CUDA events per block; working set >> L2",
                             **{k: v for k, v in rs.items() if k != "achieved_gbs"}}
+    # the other configurations: the uneven batch (cfg3, error vs FP64 for every
+    # channel), the non-uniform 2^20-tap IRs (cfg4, on the engine, with its
+    # autotuned schedule) and the serving loop (cfg5, FP32 and FP24)
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        import bench_workloads as bw
+
+        configs = {"cfg3": bw.engine_uneven(ctx), "cfg4": bw.nonuniform_long(ctx),
+                   "cfg5": bw.serving_cfg5(ctx, seconds=10.0)}
     # the CPU baseline loads every host core for seconds; it runs after the
     # latency measurements above, whose host-side copies it would slow down
     cpu = None
@@ -656,6 +671,8 @@ def run_ours(args):
             line["max_realtime_channels"] = capacity
         if roofline_serving:
             line["roofline_serving"] = roofline_serving
+        if configs:
+            line["configs"] = configs
         print(json.dumps(line), flush=True)
     ctx.Release()
     if pg:

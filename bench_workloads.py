@@ -5,9 +5,10 @@ inputs with the configurations' shapes; no public dataset is involved).
 
 dropin_small  drop-in TANConvolution, 2 ch, B=1024, IR 8192, 200 blocks, FP32
 engine_uneven  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096..262144,
-      input at -6 dBFS, FP32 / FP24 / FP16 / BF16 spectra; error vs FP64 per channel
-nonuniform_long  non-uniform partitions, 256 ch, IR 2^20, base block 128, schedule from the
-      autotuner, FP32 / FP16; error vs FP64 on sampled channels
+      input at -6 dBFS, FP32 / FP24 / FP16 / BF16 spectra; error vs FP64 for every channel
+nonuniform_long  non-uniform partitions, 256 ch, IR 2^20, base block 128, levels up to 16384,
+      schedule from the autotuner, one engine session, FP32 / FP16; error vs FP64 on every channel
+serving  the serving loop (Poisson sessions, budget admission, swaps), FP32 / FP24
 pipeline  the sample pipeline (int16 stereo sources, per-ear convolution, mix,
       int16 out): fused call vs separate GPU calls vs the CPU restatement
 Each prints one JSON object: throughput (GSamples/s), per-block latency
@@ -62,6 +63,31 @@ def _pct(a):
     return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "max": float(a.max())}
 
 
+def _db_one(args):
+    """Error of one channel's output y against the FP64 convolution of x with
+    h, in dB; block 0 is the crossfade from the initial zero IR."""
+    x, h, y, B = args
+    ref = _conv64(x, h)
+    ref[:B] *= np.arange(B) / B
+    return _db(y, ref)
+
+
+def db_all_channels(x, irs, y, B):
+    """Per-channel error vs FP64 for every channel, on a pool of worker
+    processes (started with spawn, so that no GPU context is forked)."""
+    import multiprocessing as mp
+
+    jobs = [(x[c], irs[c], y[c], B) for c in range(len(irs))]
+    with mp.get_context("spawn").Pool(max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        return pool.map(_db_one, jobs, chunksize=max(1, len(jobs) // (4 * (os.cpu_count() or 1))))
+
+
+def _db_summary(errs):
+    e = np.asarray(errs)
+    return {"channels": int(e.size), "min": float(e.min()), "median": float(np.median(e)), "max": float(e.max()),
+            "per_channel": [round(float(v), 2) for v in e]}
+
+
 def dropin_small(ctx, quick=False):
     g = _rng(0)
     C, B, L, nb = 2, 1024, 8192, 200
@@ -91,85 +117,134 @@ def dropin_small(ctx, quick=False):
             "error_db_vs_fp64": err}
 
 
-def engine_uneven(ctx, quick=False):
+def engine_uneven(ctx, quick=False, specs=("fp32", "fp24", "fp16", "bf16")):
+    """cfg3: 1024 single-channel sessions with IR lengths log-uniform in
+    [4096, 262144] in one engine (B = 256), input at -6 dBFS, every spectrum
+    form; error vs FP64 for EVERY channel over 1040 blocks (the longest IR has
+    1024 partitions, so every partition of every channel multiplies signal)."""
     g = _rng(2)
     C, B = (256 if quick else 1024), 256
-    nb = 48
+    nb = 300 if quick else 1040
     lens = np.exp(g.uniform(np.log(4096), np.log(262144), C)).astype(int)
     x = (g.uniform(-1, 1, (C, nb * B)) * 10 ** (-6 / 20)).astype(np.float32)
     irs = [_ir(g, int(L), float(g.uniform(0.2, 3.0))) for L in lens]
-    sample = g.choice(C, 32, replace=False)
-    refs = {int(c): _conv64(x[c], irs[c]) for c in sample}
-    out = {"config": "engine_uneven", "channels": C, "block": B, "ir_lengths": [int(lens.min()), int(np.median(lens)),
-                                                                       int(lens.max())], "blocks": nb}
-    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp24", eng.SPECTRUM_FP24), ("fp16", eng.SPECTRUM_FP16),
-                       ("bf16", eng.SPECTRUM_BF16)):
-        e = eng.Engine(ctx, B, spec, budget_bytes=60 << 30, max_channels=C)
+    out = {"config": "engine_uneven (cfg3)", "channels": C, "block": B,
+           "ir_lengths": [int(lens.min()), int(np.median(lens)), int(lens.max())], "blocks": nb,
+           "input": "uniform[-1, 1] at -6 dBFS", "data": "synthetic (seeded)"}
+    for name in specs:
+        spec = {"fp32": eng.SPECTRUM_FP32, "fp24": eng.SPECTRUM_FP24, "fp16": eng.SPECTRUM_FP16,
+                "bf16": eng.SPECTRUM_BF16}[name]
+        budget = sum(eng.session_bytes(B, 1, int(L), None, spec) for L in lens) + (64 << 20)
+        e = eng.Engine(ctx, B, spec, budget_bytes=budget, max_channels=C)
         sess = []
         for c in range(C):
             rc, s = e.open_session(1, int(lens[c]))
-            assert rc == 0, cv.last_error()
+            assert rc == 0 and s.first_slot == c, cv.last_error()
             sess.append(s)
         for c in range(C):
             assert sess[c].update_response_td(irs[c][None, :], block_until_ready=True) == 0
         y = np.zeros_like(x)
         lat = []
         for k in range(nb):
-            for c in range(C):
-                e.inp[sess[c].first_slot] = x[c, k * B:(k + 1) * B]
+            e.inp[:C] = x[:, k * B:(k + 1) * B]
             t0 = time.perf_counter()
             assert e.process() == 0
             lat.append(1e3 * (time.perf_counter() - t0))
-            for c in range(C):
-                y[c, k * B:(k + 1) * B] = e.out[sess[c].first_slot]
+            y[:, k * B:(k + 1) * B] = e.out[:C]
         info = e.info()
         e.release()
-        errs = []
-        for c in sample:
-            ref = refs[int(c)].copy()
-            ref[:B] *= np.arange(B) / B
-            errs.append(_db(y[c], ref))
-        out[name] = {"error_db_vs_fp64": {"min": min(errs), "median": float(np.median(errs)), "max": max(errs),
-                                          "channels_sampled": len(errs)},
-                     "latency_ms": _pct(lat[4:]), "block_bytes": info["block_bytes"],
-                     "device_bytes": info["arena_bytes"]}
+        out[name] = {"error_db_vs_fp64": _db_summary(db_all_channels(x, irs, y, B)),
+                     "latency_ms": _pct(lat[4:]), "deadline_ms": 1000.0 * B / FS,
+                     "block_bytes": info["block_bytes"], "device_bytes": info["arena_bytes"]}
     return out
 
 
 def nonuniform_long(ctx, quick=False):
+    """cfg4: 256 channels, IR 2^20 (RT60 8 s), base block 128, level sizes
+    doubling 128 -> 16384, schedule and work-item size chosen by the
+    autotuner, as one non-uniform session of the batched engine (one graph
+    launch per block), FP32 and FP16 spectra: per-block device time (CUDA
+    events, device rows) and host latency (pinned rows), and the error vs FP64
+    for every channel. The standalone object of the previous design
+    (tanb_nu_*, one small graph of level kernels per block, blocks up to 8192)
+    is timed beside it on its own tuned schedule."""
+    import torch
+
     g = _rng(3)
     C, L, B0 = (64 if quick else 256), 1 << 20, 128
     deadline = 1000.0 * B0 / FS
-    cands = autotune.tune_nu(ctx, C, L, B0)
+    cands = autotune.tune_nu_engine(ctx, C, L, B0)
     ok = [r for r in cands if r["max_ms"] < deadline] or cands
     best = ok[0]
     nb = 600 if quick else 2000
     x = g.uniform(-1, 1, (C, nb * B0)).astype(np.float32)
     irs = np.stack([_ir(g, L, 8.0) for _ in range(C)])
-    sample = [0, C // 2, C - 1]
-    refs = {c: _conv64(x[c], irs[c]) for c in sample}
-    out = {"config": "nonuniform_long", "channels": C, "ir": L, "base_block": B0, "blocks": nb, "deadline_ms": deadline,
-           "autotuner": [{"levels": r["levels"], "mean_ms": r["mean_ms"], "max_ms": r["max_ms"]} for r in cands],
-           "schedule": best["levels"]}
-    for name, spec in (("fp32", 0), ("fp16", 1)):
-        nu = nupols.NonUniform(ctx, C, L, best["levels"], spec)
-        assert nu.set_response(irs) == 0
+    out = {"config": "nonuniform_long (cfg4)", "channels": C, "ir": L, "base_block": B0, "blocks": nb,
+           "deadline_ms": deadline, "data": "synthetic (seeded)",
+           "autotuner": [{k: r[k] for k in ("levels", "partitions_per_item", "mean_ms", "p99_ms", "max_ms")}
+                         for r in cands],
+           "schedule": best["levels"], "partitions_per_item": best["partitions_per_item"]}
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros_like(xd)
+    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp16", eng.SPECTRUM_FP16)):
+        e = eng.Engine(ctx, B0, spec, budget_bytes=eng.session_bytes(B0, C, L, best["levels"], spec,
+                                                                     best["partitions_per_item"]),
+                       max_channels=C, partitions_per_item=best["partitions_per_item"])
+        rc, s = e.open_session_nu(C, L, best["levels"])
+        assert rc == 0, cv.last_error()
+        assert s.update_response_td(irs, block_until_ready=True) == 0
         y = np.zeros_like(x)
         lat = []
         for k in range(nb):
-            nu.inp[:] = x[:, k * B0:(k + 1) * B0]
+            e.inp[:C] = x[:, k * B0:(k + 1) * B0]
             t0 = time.perf_counter()
-            assert nu.process() == 0
+            assert e.process() == 0
             lat.append(1e3 * (time.perf_counter() - t0))
-            y[:, k * B0:(k + 1) * B0] = nu.out
-        info = nu.info()
-        nu.release()
-        out[name] = {"error_db_vs_fp64": [_db(y[c], refs[c]) for c in sample], "latency_ms": _pct(lat),
-                     "gsamples_per_s_host": C * B0 * nb / (sum(lat) / 1e3) / 1e9,
-                     "deadline_misses": int((np.asarray(lat) > deadline).sum()),
-                     "device_bytes": info["device_bytes"], "avg_tail_bytes_per_block": info["tail_bytes_per_block"]}
+            y[:, k * B0:(k + 1) * B0] = e.out[:C]
+        # device time per block: the same stream again with device rows
+        assert s.update_response_td(irs, block_until_ready=True) == 0
+        st = torch.cuda.ExternalStream(e.stream())
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nb)]
+        for k in range(nb):
+            ev[k][0].record(st)
+            assert e.process_device(xd.data_ptr() + k * B0 * 4, yd.data_ptr() + k * B0 * 4, nb * B0) == 0
+            ev[k][1].record(st)
+        e.synchronize()
+        dev_ms = np.array([a.elapsed_time(b) for a, b in ev])[best["levels"][-1][0] // B0:]
+        info = e.info()
+        e.release()
+        out[name] = {"error_db_vs_fp64": _db_summary(db_all_channels(x, irs, y, B0)),
+                     "host_latency_ms": _pct(lat), "device_ms": {"mean": float(dev_ms.mean()),
+                                                                 "p99": float(np.percentile(dev_ms, 99)),
+                                                                 "max": float(dev_ms.max())},
+                     "deadline_misses_host": int((np.asarray(lat) > deadline).sum()),
+                     "gsamples_per_s_device": C * B0 / (dev_ms.mean() / 1e3) / 1e9,
+                     "device_bytes": info["arena_bytes"], "avg_block_bytes": info["block_bytes"]}
+    del xd, yd
+    # the standalone object on its own tuned schedule (blocks up to 8192)
+    sc = autotune.tune_nu(ctx, C, L, B0)
+    if sc:
+        out["standalone_tanb_nu"] = {"schedule": sc[0]["levels"], "device_mean_ms": sc[0]["mean_ms"],
+                                     "device_max_ms": sc[0]["max_ms"],
+                                     "what": "tanb_nu_* object: per block one graph of the due levels' kernels"}
     # the same IR as uniform partitions (block 128) would stream this many bytes per block
     out["uniform_tail_bytes_per_block"] = C * ((L // B0) - 1) * B0 * 16
+    return out
+
+
+def serving_cfg5(ctx, seconds=10.0, quick=False):
+    """cfg5: the serving loop at 48 kHz, block 256 (5.33 ms deadline), Poisson
+    arrivals 20/s, exponential lifetimes (mean 30 s), 1-8 channels, IR lengths
+    log-uniform 8192..524288, IR swaps at 0.5/s per session, 150 GB budget,
+    starting in steady state; FP32 and FP24 forms."""
+    from tan_b200 import serving
+
+    out = {"config": "serving (cfg5)", "seconds": seconds, "data": "synthetic (seeded)"}
+    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp24", eng.SPECTRUM_FP24)):
+        r = serving.serve(ctx, seconds=(2.0 if quick else seconds), spectrum=spec)
+        out[name] = {k: r[k] for k in ("blocks", "deadline_ms", "latency_ms", "deadline_misses",
+                                       "concurrent_channels_mean", "concurrent_channels_max", "admitted",
+                                       "refused", "control_errors")}
     return out
 
 
@@ -259,15 +334,16 @@ def pipeline(ctx, quick=False, S=32, B=256, L=48000):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("which", choices=["dropin_small", "engine_uneven", "nonuniform_long", "nu-tune", "pipeline"])
+    ap.add_argument("which", choices=["dropin_small", "engine_uneven", "nonuniform_long", "nu-tune", "pipeline",
+                                      "serving"])
     ap.add_argument("--quick", action="store_true")
     a = ap.parse_args()
     ctx = cv.TANContext(0)
     if a.which == "nu-tune":
-        r = autotune.tune_nu(ctx, 64 if a.quick else 256, 1 << 20, 128)
+        r = autotune.tune_nu_engine(ctx, 64 if a.quick else 256, 1 << 20, 128)
     else:
         r = {"dropin_small": dropin_small, "engine_uneven": engine_uneven, "nonuniform_long": nonuniform_long,
-             "pipeline": pipeline}[a.which](ctx, a.quick)
+             "pipeline": pipeline, "serving": lambda c, q: serving_cfg5(c, quick=q)}[a.which](ctx, a.quick)
     print(json.dumps(r))
 
 

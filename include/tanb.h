@@ -315,6 +315,15 @@ int32_t tanb_engine_open_session_nu(tanb_engine* engine, uint32_t channels, uint
                                     uint32_t* first_slot);
 int32_t tanb_engine_close_session(tanb_engine* engine, int32_t session);
 
+/* Device bytes a session of this shape takes from the budget of an engine
+ * created with `block`, `spectrum` and `partitions_per_item` (0: 32):
+ * nlevels = 0 for a uniformly partitioned session, else the level schedule of
+ * tanb_engine_open_session_nu. Host arithmetic only (no device needed), so a
+ * router can place sessions on GPUs by the engines' own admission rule. */
+int32_t tanb_engine_session_bytes(uint32_t block, uint32_t spectrum, uint32_t partitions_per_item, uint32_t channels,
+                                  uint32_t ir_length, uint32_t nlevels, const uint32_t* level_block,
+                                  const uint32_t* level_parts, uint64_t* bytes);
+
 /* UpdateResponseTD for one session (host IR rows, n <= ir_length). The IR is
  * copied before this returns and transformed on the engine's update stream,
  * off the audio path; it takes effect, with a one-block crossfade, on the

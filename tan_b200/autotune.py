@@ -18,6 +18,7 @@ import numpy as np
 
 from . import convolution as cv
 from . import nupols
+from .convolution import AMF_OK
 
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
 
@@ -165,6 +166,70 @@ def tune_nu(ctx, C, L, B0, max_blocks=(1024, 2048, 4096, 8192), mids=(1, 2), spe
                         "tail_bytes_per_block": nu.info()["tail_bytes_per_block"]})
             nu.release()
             del x, y
+    res.sort(key=lambda r: r["mean_ms"])
+    return res
+
+
+def nu_candidates(L, B0, max_blocks=(1024, 2048, 4096, 8192, 16384), mids=(1, 2)):
+    """Level schedules the non-uniform search tries: the default doubling ladder
+    (two partitions per size) up to each maximum block, and the same ladder
+    with one partition in the middle levels."""
+    out = []
+    for mb in max_blocks:
+        if mb < B0:
+            continue
+        for mid in mids:
+            lv = nupols.schedule(L, B0, mb)
+            if mid == 1 and len(lv) > 2:
+                lv = [lv[0]] + [(b, 1) for b, _ in lv[1:-1]] + [lv[-1]]
+                off = sum(b * k for b, k in lv[:-1])
+                if any(sum(b * k for b, k in lv[:i]) < lv[i][0] for i in range(1, len(lv))):
+                    continue  # a level would start before its block
+                lv[-1] = (lv[-1][0], -(-(L - off) // lv[-1][0]))
+            if lv not in out:
+                out.append(lv)
+    return out
+
+
+def tune_nu_engine(ctx, C, L, B0, max_blocks=(1024, 2048, 4096, 8192, 16384), mids=(1, 2), spectrum=0,
+                   items=(16, 32), periods=2):
+    """Times every candidate schedule (nu_candidates) with every work-item size
+    as one non-uniform engine session of C channels: CUDA events around each
+    block launch (device rows), over `periods` periods of the largest level
+    after one period of warm-up. Returns the results sorted by mean block time."""
+    import torch
+
+    from . import engine as eng
+
+    res = []
+    g = np.random.Generator(np.random.PCG64(20261203 + 41))
+    h = (g.standard_normal((C, L)) * 1e-3).astype(np.float32)
+    for lv in nu_candidates(L, B0, max_blocks, mids):
+        period = lv[-1][0] // B0
+        n = period * (periods + 1)
+        x = torch.from_numpy(g.uniform(-1, 1, (C, B0 * n)).astype(np.float32)).cuda()
+        y = torch.zeros_like(x)
+        for q in items:
+            e = eng.Engine(ctx, B0, spectrum, budget_bytes=eng.session_bytes(B0, C, L, lv, spectrum, q),
+                           max_channels=C, partitions_per_item=q)
+            rc, s = e.open_session_nu(C, L, lv)
+            if rc != AMF_OK:
+                e.release()
+                continue
+            assert s.update_response_td(h, block_until_ready=True) == AMF_OK
+            st = torch.cuda.ExternalStream(e.stream())
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+            for k in range(n):
+                ev[k][0].record(st)
+                assert e.process_device(x.data_ptr() + k * B0 * 4, y.data_ptr() + k * B0 * 4, B0 * n) == AMF_OK
+                ev[k][1].record(st)
+            e.synchronize()
+            ms = [a.elapsed_time(b) for a, b in ev][period:]
+            res.append({"levels": lv, "partitions_per_item": q, "mean_ms": float(np.mean(ms)),
+                        "p99_ms": float(np.percentile(ms, 99)), "max_ms": float(np.max(ms)),
+                        "block_bytes": e.info()["block_bytes"]})
+            e.release()
+        del x, y
     res.sort(key=lambda r: r["mean_ms"])
     return res
 

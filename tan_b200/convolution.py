@@ -96,6 +96,8 @@ SIGNATURES = {
     "tanb_engine_open_session_nu": (_i32, [_vp, _u32, _u32, _u32, _u32p, _u32p, ctypes.POINTER(ctypes.c_int32),
                                             _u32p]),
     "tanb_engine_close_session": (_i32, [_vp, _i32]),
+    "tanb_engine_session_bytes": (_i32, [_u32, _u32, _u32, _u32, _u32, _u32, _u32p, _u32p,
+                                         ctypes.POINTER(ctypes.c_uint64)]),
     "tanb_engine_update_response_td": (_i32, [_vp, _i32, _pp, _sz, _u32]),
     "tanb_engine_update_response_td_device": (_i32, [_vp, _i32, _pp, _sz, _u32]),
     "tanb_engine_io": (_i32, [_vp, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),

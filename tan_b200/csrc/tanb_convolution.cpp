@@ -44,7 +44,13 @@ thread_local std::string g_last_error;
 
 }  // namespace
 
-void tanb::set_last_error(const char* msg) { g_last_error = msg; }
+// Every reported failure also clears the CUDA runtime's per-thread last error:
+// a failed runtime call leaves it set, and the next launch check
+// (cudaGetLastError after a launch) would otherwise report that stale error.
+void tanb::set_last_error(const char* msg) {
+  g_last_error = msg;
+  cudaGetLastError();
+}
 
 namespace {
 
@@ -54,7 +60,7 @@ int32_t fail(int32_t code, const char* fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
-  g_last_error = buf;
+  tanb::set_last_error(buf);
   return code;
 }
 
@@ -1354,7 +1360,7 @@ int32_t tanb_convolution_process(tanb_convolution* v, const float* const* in, fl
 int32_t tanb_convolution_process_host_to_device(tanb_convolution* v, const float* const* in, float* const* out,
                                                 size_t n, const uint32_t* flags, size_t* done) {
   int32_t r = process_common(v, Mem::Host, in, Mem::Device, out, n, flags, done);
-  if (r == TANB_OK && v->initialized) {
+  if (r == TANB_OK && v->initialized && !v->nu_eng) {
     cudaError_t e = cudaEventSynchronize(v->ev_out);
     if (e != cudaSuccess) return fail(TANB_FAIL, "sync: %s", cudaGetErrorString(e));
   }

@@ -832,15 +832,11 @@ int32_t engine_flush_channel(tanb_engine* e, int32_t session, int channel) {
 
 size_t engine_nu_session_bytes(int block, int spectrum, int channels, uint32_t ir_length, uint32_t nlevels,
                                const uint32_t* level_block, const uint32_t* level_parts) {
-  tanb_engine probe;  // shape only: no device state
-  probe.B = block;
-  while ((1 << probe.log2B) < block) ++probe.log2B;
-  probe.spec = spectrum;
-  std::vector<LevelSpec> lv;
-  int P = 0, rin = 0;
-  if (make_levels(&probe, ir_length, nlevels, level_block, level_parts, &lv, &P, &rin) != TANB_OK) return 0;
-  const int nitem = P > 2 ? (P - 2 + probe.Q - 1) / probe.Q : 0;
-  return chan_bytes(&probe, P, nitem, lv, rin) * (size_t)channels;
+  uint64_t bytes = 0;
+  if (tanb_engine_session_bytes((uint32_t)block, (uint32_t)spectrum, 0, (uint32_t)channels, ir_length, nlevels,
+                                level_block, level_parts, &bytes) != TANB_OK)
+    return 0;
+  return (size_t)bytes;
 }
 
 int32_t engine_process_rows(tanb_engine* e, const EngRows& rows) {
@@ -964,6 +960,33 @@ int32_t tanb_engine_release(tanb_engine* e) {
     free_engine(e);
   }
   delete e;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_session_bytes(uint32_t block, uint32_t spectrum, uint32_t partitions_per_item, uint32_t channels,
+                                  uint32_t ir_length, uint32_t nlevels, const uint32_t* level_block,
+                                  const uint32_t* level_parts, uint64_t* bytes) {
+  if (!bytes) return efail(TANB_INVALID_POINTER, "null argument");
+  *bytes = 0;
+  if (block < 128 || block > 2048 || (block & (block - 1)) || spectrum > tanb::kSpecFP24 || channels == 0 ||
+      ir_length == 0)
+    return efail(TANB_INVALID_ARG, "invalid engine block, spectrum, channels or IR length");
+  if (nlevels && (!level_block || !level_parts)) return efail(TANB_INVALID_POINTER, "null level schedule");
+  tanb_engine probe;  // shape only: no device state
+  probe.B = (int)block;
+  while ((1 << probe.log2B) < probe.B) ++probe.log2B;
+  probe.spec = (int)spectrum;
+  probe.Q = partitions_per_item ? (int)partitions_per_item : 32;
+  std::vector<LevelSpec> lv;
+  int P = 0, rin = 0;
+  if (nlevels) {
+    const int32_t r = make_levels(&probe, ir_length, nlevels, level_block, level_parts, &lv, &P, &rin);
+    if (r != TANB_OK) return r;
+  } else {
+    P = (int)std::max<uint32_t>(1, (ir_length + block - 1) / block);
+  }
+  const int nitem = P > 2 ? (P - 2 + probe.Q - 1) / probe.Q : 0;
+  *bytes = (uint64_t)chan_bytes(&probe, P, nitem, lv, rin) * channels;
   return TANB_OK;
 }
 

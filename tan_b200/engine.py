@@ -19,6 +19,22 @@ SPECTRUM_BF16 = 2
 SPECTRUM_FP24 = 3  # IR spectra and delay line in 24 bits (engine only)
 
 
+def session_bytes(block: int, channels: int, ir_length: int, levels=None, spectrum: int = SPECTRUM_FP32,
+                  partitions_per_item: int = 0) -> int:
+    """Device bytes a session takes from an engine's budget (host arithmetic,
+    tanb_engine_session_bytes): uniform when levels is None, else the
+    non-uniform schedule [(block, partitions), ...]."""
+    nl = len(levels) if levels else 0
+    blocks = (ctypes.c_uint32 * max(1, nl))(*[b for b, _ in (levels or [])])
+    parts = (ctypes.c_uint32 * max(1, nl))(*[k for _, k in (levels or [])])
+    out = ctypes.c_uint64(0)
+    rc = lib().tanb_engine_session_bytes(block, spectrum, partitions_per_item, channels, ir_length, nl,
+                                         blocks if nl else None, parts if nl else None, ctypes.byref(out))
+    if rc != AMF_OK:
+        raise TANError(rc, "tanb_engine_session_bytes")
+    return out.value
+
+
 class Session:
     def __init__(self, engine: "Engine", sid: int, first_slot: int, channels: int, ir_length: int):
         self.engine, self.id, self.first_slot = engine, sid, first_slot

@@ -155,8 +155,9 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
                 else:
                     work.put(("ir", v[0]))
                 v[2] = t + g.exponential(1.0 / swap_rate)
-        rc = e.process()
-        assert rc == cv.AMF_OK, cv.last_error()
+        if live:  # an idle engine has no block to run
+            rc = e.process()
+            assert rc == cv.AMF_OK, cv.last_error()
         lat.append(1000.0 * (time.perf_counter() - t0))
         for sid, tr in traces.items():
             tr["y"].append(e.out[live[sid][0].slots].copy())
@@ -234,10 +235,46 @@ def _block_latencies_plain(ctx, nsess, C, L, block, blocks, g, pool):
     return np.asarray(lat)
 
 
+def _block_latencies_plain_one(ctx, nsess, C, L, block, blocks, g, pool):
+    """One drop-in object holding every channel (nsess * C), host rows."""
+    from . import autotune
+
+    n = nsess * C
+    try:
+        conv = autotune.tuned(ctx, cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, block, n)
+    except cv.TANError:
+        return None
+    import ctypes
+
+    lib = cv.lib()
+    # one IR row for every channel (the transform and the streamed bytes are
+    # the same as with distinct rows; the host keeps one row instead of n)
+    h = pool.get(g, 1, L)
+    rows = (ctypes.c_void_p * n)(*([h[0].ctypes.data] * n))
+    assert lib.tanb_convolution_update_response_td(conv._h, rows, L, None, 0) == cv.AMF_OK
+    x = g.uniform(-1, 1, (n, block)).astype(np.float32)
+    y = np.zeros_like(x)
+    rin = (ctypes.c_void_p * n)(*[x[c].ctypes.data for c in range(n)])
+    rout = (ctypes.c_void_p * n)(*[y[c].ctypes.data for c in range(n)])
+    done = ctypes.c_size_t(0)
+    lat = []
+    for k in range(blocks + 5):
+        t0 = time.perf_counter()
+        rc = lib.tanb_convolution_process(conv._h, rin, rout, block, None, ctypes.byref(done))
+        assert rc == cv.AMF_OK
+        if k >= 5:
+            lat.append(1000.0 * (time.perf_counter() - t0))
+    conv.Release()
+    return np.asarray(lat)
+
+
 def capacity(ctx, form="batched", C=4, L=65536, block=256, spectrum=eng.SPECTRUM_FP32, blocks=200,
              seed=20261203 + 5, start=4):
     """Largest channel count (sessions of C channels, IR length L) whose p99 block
-    latency is under the deadline; doubling then bisection on the session count."""
+    latency is under the deadline; doubling then bisection on the session count.
+    form: "batched" (the engine), "plain" (one TANConvolution per session,
+    processed in turn) or "plain_one" (one TANConvolution holding every
+    channel)."""
     g = np.random.Generator(np.random.PCG64(seed))
     pool = IRPool(g, n=4, length=L)
     deadline = 1000.0 * block / FS
@@ -245,6 +282,8 @@ def capacity(ctx, form="batched", C=4, L=65536, block=256, spectrum=eng.SPECTRUM
     def ok(n):
         if form == "batched":
             lat = _block_latencies_batched(ctx, n, C, L, block, spectrum, blocks, g, pool)
+        elif form == "plain_one":
+            lat = _block_latencies_plain_one(ctx, n, C, L, block, blocks, g, pool)
         else:
             lat = _block_latencies_plain(ctx, n, C, L, block, blocks, g, pool)
         if lat is None:
@@ -320,7 +359,7 @@ def main():
     ap.add_argument("--spectrum", choices=["fp32", "fp16", "bf16", "fp24"], default="fp32")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--capacity", action="store_true")
-    ap.add_argument("--form", choices=["batched", "plain"], default="batched")
+    ap.add_argument("--form", choices=["batched", "plain", "plain_one"], default="batched")
     ap.add_argument("--ir-length", type=int, default=65536)
     ap.add_argument("--channels", type=int, default=4)
     ap.add_argument("--mac-roofline", type=int, default=0, metavar="CHANNELS",

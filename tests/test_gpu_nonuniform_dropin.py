@@ -152,6 +152,6 @@ def test_nonuniform_init_rules(tan_ctx):
                                     [np.zeros(256, np.int16)], 1, 1.0, 256)
     assert rc == cv.AMF_NOT_SUPPORTED
     rc, done = conv.Process(x, x.copy(), 256)
-    assert rc == cv.AMF_OK and done == 256
+    assert rc == cv.AMF_OK and done == 256, cv.last_error()
     assert conv.ProcessFinalize() == cv.AMF_OK
     conv.Release()
