@@ -64,28 +64,31 @@ def _pct(a):
 
 
 def _db_one(args):
-    """Error of one channel's output y against the FP64 convolution of x with
-    h, in dB; block 0 is the crossfade from the initial zero IR."""
-    x, h, y, B = args
+    """Errors of one channel's outputs ys (one per run) against the FP64
+    convolution of x with h, in dB; block 0 is the crossfade from the initial
+    zero IR. A non-finite output scores +999."""
+    x, h, ys, B = args
     ref = _conv64(x, h)
     ref[:B] *= np.arange(B) / B
-    return _db(y, ref)
+    return [_db(y, ref) if np.isfinite(y).all() else 999.0 for y in ys]
 
 
-def db_all_channels(x, irs, y, B):
-    """Per-channel error vs FP64 for every channel, on a pool of worker
-    processes (started with spawn, so that no GPU context is forked)."""
+def db_all_channels(x, irs, ys, B):
+    """Per-channel error vs FP64 of every channel of every run in ys (a list
+    of (channels, samples) outputs), on a pool of worker processes (started
+    with spawn, so that no GPU context is forked). Returns one list per run."""
     import multiprocessing as mp
 
-    jobs = [(x[c], irs[c], y[c], B) for c in range(len(irs))]
+    jobs = [(x[c], irs[c], [y[c] for y in ys], B) for c in range(len(irs))]
     with mp.get_context("spawn").Pool(max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
-        return pool.map(_db_one, jobs, chunksize=max(1, len(jobs) // (4 * (os.cpu_count() or 1))))
+        per = pool.map(_db_one, jobs, chunksize=max(1, len(jobs) // (4 * (os.cpu_count() or 1))))
+    return [[p[r] for p in per] for r in range(len(ys))]
 
 
 def _db_summary(errs):
     e = np.asarray(errs)
     return {"channels": int(e.size), "min": float(e.min()), "median": float(np.median(e)), "max": float(e.max()),
-            "per_channel": [round(float(v), 2) for v in e]}
+            "nonfinite_channels": int((e >= 999.0).sum()), "per_channel": [round(float(v), 2) for v in e]}
 
 
 def dropin_small(ctx, quick=False):
@@ -131,6 +134,7 @@ def engine_uneven(ctx, quick=False, specs=("fp32", "fp24", "fp16", "bf16")):
     out = {"config": "engine_uneven (cfg3)", "channels": C, "block": B,
            "ir_lengths": [int(lens.min()), int(np.median(lens)), int(lens.max())], "blocks": nb,
            "input": "uniform[-1, 1] at -6 dBFS", "data": "synthetic (seeded)"}
+    ys = []
     for name in specs:
         spec = {"fp32": eng.SPECTRUM_FP32, "fp24": eng.SPECTRUM_FP24, "fp16": eng.SPECTRUM_FP16,
                 "bf16": eng.SPECTRUM_BF16}[name]
@@ -153,9 +157,11 @@ def engine_uneven(ctx, quick=False, specs=("fp32", "fp24", "fp16", "bf16")):
             y[:, k * B:(k + 1) * B] = e.out[:C]
         info = e.info()
         e.release()
-        out[name] = {"error_db_vs_fp64": _db_summary(db_all_channels(x, irs, y, B)),
-                     "latency_ms": _pct(lat[4:]), "deadline_ms": 1000.0 * B / FS,
+        ys.append(y)
+        out[name] = {"latency_ms": _pct(lat[4:]), "deadline_ms": 1000.0 * B / FS,
                      "block_bytes": info["block_bytes"], "device_bytes": info["arena_bytes"]}
+    for name, errs in zip(specs, db_all_channels(x, irs, ys, B)):
+        out[name]["error_db_vs_fp64"] = _db_summary(errs)
     return out
 
 
@@ -186,6 +192,7 @@ def nonuniform_long(ctx, quick=False):
            "schedule": best["levels"], "partitions_per_item": best["partitions_per_item"]}
     xd = torch.from_numpy(x).cuda()
     yd = torch.zeros_like(xd)
+    ys = []
     for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp16", eng.SPECTRUM_FP16)):
         e = eng.Engine(ctx, B0, spec, budget_bytes=eng.session_bytes(B0, C, L, best["levels"], spec,
                                                                      best["partitions_per_item"]),
@@ -213,14 +220,16 @@ def nonuniform_long(ctx, quick=False):
         dev_ms = np.array([a.elapsed_time(b) for a, b in ev])[best["levels"][-1][0] // B0:]
         info = e.info()
         e.release()
-        out[name] = {"error_db_vs_fp64": _db_summary(db_all_channels(x, irs, y, B0)),
-                     "host_latency_ms": _pct(lat), "device_ms": {"mean": float(dev_ms.mean()),
+        ys.append(y)
+        out[name] = {"host_latency_ms": _pct(lat), "device_ms": {"mean": float(dev_ms.mean()),
                                                                  "p99": float(np.percentile(dev_ms, 99)),
                                                                  "max": float(dev_ms.max())},
                      "deadline_misses_host": int((np.asarray(lat) > deadline).sum()),
                      "gsamples_per_s_device": C * B0 / (dev_ms.mean() / 1e3) / 1e9,
                      "device_bytes": info["arena_bytes"], "avg_block_bytes": info["block_bytes"]}
     del xd, yd
+    for name, errs in zip(("fp32", "fp16"), db_all_channels(x, irs, ys, B0)):
+        out[name]["error_db_vs_fp64"] = _db_summary(errs)
     # the standalone object on its own tuned schedule (blocks up to 8192)
     sc = autotune.tune_nu(ctx, C, L, B0)
     if sc:

@@ -226,6 +226,9 @@ __device__ __forceinline__ void ir_partition(void* H, float* scale_tab, int P, i
       frexpf(mx, &e);  // mx = f * 2^e, f in [0.5, 1)
       e -= 15;
     }
+    // a partition of denormal samples: keep the scale a normal number (2^-149
+    // would round to zero and its inverse overflow)
+    e = e < -126 ? -126 : e;
     scale = ldexpf(1.0f, e);
     if (threadIdx.x == 0) scale_tab[(size_t)slot * P + part] = scale;
   }

@@ -310,6 +310,9 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
       frexpf(mx, &e);
       e -= 15;
     }
+    // a partition of denormal samples: keep the scale a normal number (2^-149
+    // would round to zero and its inverse overflow)
+    e = e < -126 ? -126 : e;
     scale = ldexpf(1.f, e);
     if (threadIdx.x == 0) lv.scale[(size_t)c * lv.K + part] = scale;
   }

@@ -255,3 +255,24 @@ def test_engine_write_input_rows(tan_ctx):
     assert np.array_equal(e.inp[0:3], small)
     assert e.write_input(2047, small) == cv.AMF_INVALID_ARG
     e.release()
+
+
+@pytest.mark.parametrize("spectrum", [eng.SPECTRUM_FP16, eng.SPECTRUM_BF16])
+def test_engine_scaled_spectra_with_denormal_partitions_stay_finite(tan_ctx, spectrum):
+    """IRs whose late partitions hold only denormal samples (a fast decay over
+    a long IR): the per-partition power-of-two scale stays a normal number, so
+    no partition turns into inf or NaN, and the output keeps its precision."""
+    g = H.rng(20261203 + 51)
+    B, nb, C, L = 256, 40, 2, 8192
+    h = H.irs(g, C, L)
+    h[:, 3 * B:5 * B] = (g.standard_normal((C, 2 * B)) * 1e-41).astype(np.float32)  # denormal partitions 3, 4
+    h[:, 6 * B:] = 0.0
+    x = H.noise(g, C, nb * B)
+    sessions = [{"C": C, "L": L, "x": x, "events": {0: h}, "start": 0}]
+    engine = eng.Engine(tan_ctx, B, spectrum, budget_bytes=64 << 20, max_channels=4)
+    y = run_engine(engine, sessions, nb)[0]
+    engine.release()
+    assert np.isfinite(y).all()
+    exp = fp64.stream_fp64(x, B, [(0, {c: h[c] for c in range(C)})])
+    for c in range(C):
+        assert fp64.error_db(y[c], exp[c]) < (-60 if spectrum == eng.SPECTRUM_FP16 else -40)

@@ -108,3 +108,19 @@ def test_nu_signal_longer_than_every_level_offset(tan_ctx, C, levels, nb):
     for c in (range(C) if C <= 8 else (0, C // 2, C - 1)):
         assert fp64.error_db(y[c], fp64.conv_fp64(x[c], h[c])) < -120, c
     nu.release()
+
+
+def test_nonuniform_fp16_with_denormal_partitions_stays_finite(tan_ctx):
+    """The standalone non-uniform object with FP16 spectra on an IR whose
+    later level partitions hold only denormal samples: finite output."""
+    g = H.rng(20261203 + 52)
+    C, L, B0, nb = 2, 8192, 128, 80
+    levels = nupols.schedule(L, B0, 1024)
+    h = H.irs(g, C, L)
+    h[:, 3000:] = (g.standard_normal((C, L - 3000)) * 1e-41).astype(np.float32)
+    x = H.noise(g, C, nb * B0)
+    nu = nupols.NonUniform(tan_ctx, C, L, levels, 1)
+    assert nu.set_response(h) == 0
+    y = nu.run(x)
+    nu.release()
+    assert np.isfinite(y).all()
