@@ -129,6 +129,7 @@ class RangeAlloc {
 // Shape of one level above the base level of a non-uniform session.
 struct LevelSpec {
   int log2N = 0, K = 0, Kr = 0, ngroup = 0, R = 0;
+  int q = 0;    // partitions per work item (group)
   long long off = 0;
   int nfl = 0;  // level blocks whose output an IR swap recomputes (at most)
 };
@@ -340,9 +341,15 @@ cudaError_t commit_updates(tanb_engine* e) {
     if (s.nitem)
       r = tanb::eng_launch_commit(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, nit, grid, e->d_block,
                                   e->stream);
-    if (r == cudaSuccess && nit > s.C * s.nitem)
+    if (r == cudaSuccess && nit > s.C * s.nitem) {
+      int slices = 1;  // bin slices of the largest level with work items
+      for (const LevelSpec& l : s.lv)
+        if (l.ngroup) slices = std::max(slices, 1 << (l.log2N - e->log2B));
+      const long long pairs = (long long)nit * slices;
       r = tanb::eng_launch_level_commit_items(e->log2B, e->spec, e->d_chans, e->d_levels, e->d_items, (int)s.item0,
-                                              nit, grid, e->d_block, e->stream);
+                                              nit, slices, (int)std::min<long long>(e->tail_grid, pairs), e->d_block,
+                                              e->stream);
+    }
     for (size_t l = 0; l < s.lv.size() && r == cudaSuccess; ++l) {
       const int c = level_class(e, s.lv[l].log2N);
       r = tanb::eng_launch_level_commit_out(e->log2B, s.lv[l].log2N, e->spec, e->d_chans,
@@ -485,7 +492,12 @@ int32_t make_levels(const tanb_engine* e, uint32_t ir_length, uint32_t nlevels, 
       s.off = off;
       s.nfl = (int)((off + N - 1) / N);
       s.Kr = s.K + s.nfl - 1;
-      s.ngroup = s.K > 2 ? (s.K - 2 + e->Q - 1) / e->Q : 0;
+      // Work items of a level take one bin slice per base block, so a level
+      // has only ngroup of them at a time: groups of at most Q partitions,
+      // and at least 8 groups when the level has 16 or more partitions, so
+      // that a level with few channels still spreads over many warps.
+      s.q = std::max(2, std::min(e->Q, (s.K - 2 + 7) / 8));
+      s.ngroup = s.K > 2 ? (s.K - 2 + s.q - 1) / s.q : 0;
       s.R = (int)pow2_at_least((size_t)off + N + 2 * (size_t)e->B);
       lv->push_back(s);
       nmax = std::max<size_t>(nmax, N);
@@ -515,7 +527,7 @@ cudaError_t grow_items(tanb_engine* e, size_t need) {
     return r;
   }
   std::memcpy(h, e->h_items, e->max_items * sizeof(EngItem));
-  for (size_t i = e->max_items; i < cap; ++i) h[i] = EngItem{-1, 0, 0, 0, -1, 0};
+  for (size_t i = e->max_items; i < cap; ++i) h[i] = EngItem{-1, 0, 0, 0, -1};
   r = cudaMemcpyAsync(d, h, cap * sizeof(EngItem), cudaMemcpyHostToDevice, e->stream);
   if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
   if (r != cudaSuccess) {
@@ -551,7 +563,7 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
   // work items cover partitions [2, P); the head does partitions 0 and 1
   s.nitem = s.P > 2 ? (s.P - 2 + e->Q - 1) / e->Q : 0;
   s.items_per_chan = s.nitem;
-  for (const LevelSpec& l : s.lv) s.items_per_chan += l.ngroup << (l.log2N - e->log2B);
+  for (const LevelSpec& l : s.lv) s.items_per_chan += l.ngroup;
   const size_t per_chan = chan_bytes(e, s.P, s.nitem, s.lv, s.rin);
   s.arena_bytes = per_chan * s.C;
   if (!e->arena_alloc.alloc(s.arena_bytes / kAlign, &s.arena_off))
@@ -617,7 +629,7 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
     size_t it = s.item0 + (size_t)j * s.items_per_chan;
     for (int r = 0; r < s.nitem; ++r) {
       const int i0 = 2 + r * e->Q;
-      e->h_items[it++] = EngItem{slot, i0, std::min(s.P, i0 + e->Q), r, -1, 0};
+      e->h_items[it++] = EngItem{slot, i0, std::min(s.P, i0 + e->Q), r, -1};
     }
     if (!s.lv.empty()) {
       EngNu& nu = nus[j];
@@ -659,12 +671,10 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
         e->h_levels[rec] = lv;
         nu.ring[l] = lv.ring;
         nu.R[l] = ls.R;
-        const int p = 1 << (ls.log2N - e->log2B);
         for (int g = 0; g < ls.ngroup; ++g) {
-          const int i0 = 2 + g * e->Q;
-          for (int sl = 0; sl < p; ++sl)
-            e->h_items[it++] = EngItem{slot, i0, std::min(ls.K, i0 + e->Q), g, (int)(c * e->max_channels +
-                                       s.lv_first[l] + j), sl};
+          const int i0 = 2 + g * ls.q;
+          e->h_items[it++] = EngItem{slot, i0, std::min(ls.K, i0 + ls.q), g, (int)(c * e->max_channels +
+                                     s.lv_first[l] + j)};
         }
       }
     }
@@ -910,7 +920,7 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
                  cudaGetErrorString(r));
   }
   std::memset(e->h_chans, 0, e->max_channels * sizeof(EngChan));
-  for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0, -1, 0};
+  for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0, -1};
   for (size_t i = 0; i < nlev; ++i) {
     e->h_levels[i] = EngLevel{};
     e->h_levels[i].chan = -1;
@@ -1015,7 +1025,7 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   if (s.staged_ev) cudaEventDestroy(s.staged_ev);
   for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j] = EngChan{};
   const size_t nit_total = (size_t)s.C * s.items_per_chan;
-  for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0, -1, 0};
+  for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0, -1};
   for (size_t l = 0; l < s.lv.size(); ++l) {
     const size_t first = (size_t)level_class(e, s.lv[l].log2N) * e->max_channels + s.lv_first[l];
     for (int j = 0; j < s.C; ++j) {

@@ -72,15 +72,15 @@ struct EngChan {
 // A tail work item. Base level (lvl < 0): partitions [i0, i1) (i0 >= 2;
 // partitions 0 and 1 belong to the head) of channel `chan`, partial sum row
 // `row`, every block. Level item (lvl >= 0, index into the level table):
-// partitions [i0, i1) of that level, bins [slice B, (slice + 1) B) of its
-// N-bin rows, partial row `row`; it runs in the base blocks k with
-// k mod p == slice, so a level's tail is spread evenly over its p base blocks.
+// partitions [i0, i1) of that level, partial row `row`; at base block k it
+// takes bin slice k mod p ([s B, (s + 1) B) of the level's N-bin rows) of
+// the level block after the one completing in this period, so a level's tail
+// is spread evenly over its p base blocks and every item works every block.
 struct EngItem {
   int32_t chan;  // -1: free
   int32_t i0, i1;
   int32_t row;
   int32_t lvl;
-  int32_t slice;
 };
 
 // One channel of an IR update: channel `chan`'s new IR, read from `src`
@@ -151,7 +151,7 @@ cudaError_t eng_launch_commit(int log2B, int spec, const EngChan* chans, const E
 // sums of the level items among [item0, item0 + nitems) for the level blocks
 // whose heads come at or after k (both parities), from the current delay lines.
 cudaError_t eng_launch_level_commit_items(int log2B, int spec, const EngChan* chans, const EngLevel* levels,
-                                          const EngItem* items, int item0, int nitems, int grid,
+                                          const EngItem* items, int item0, int nitems, int max_slices, int grid,
                                           const long long* block, cudaStream_t st);
 // A newly committed IR's output for the level blocks whose heads have run but
 // whose output is still to be played from block k on: recomputed over every

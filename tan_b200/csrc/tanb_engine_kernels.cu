@@ -446,13 +446,13 @@ __device__ __forceinline__ float2 lv_spec_bin(const EngLevel& lv, int slot, int 
 
 // One level work item for level block jb: sum over partitions i in
 // [w.i0, w.i1) of X_{jb - i} times IR partition i of `slot`, over the bins of
-// slice w.slice (B bins: units [slice B / 2, (slice + 1) B / 2)), into partial
+// slice `slice` (B bins: units [slice B / 2, (slice + 1) B / 2)), into partial
 // row w.row of parity jb & 1. B / 4 threads, two units each, as eng_item.
 template <int LOG2B, int SPEC>
-__device__ __noinline__ void eng_level_item(const EngLevel& lv, const EngItem& w, int slot, long long jb) {
+__device__ __noinline__ void eng_level_item(const EngLevel& lv, const EngItem& w, int slot, long long jb, int slice) {
   constexpr int Bn = 1 << LOG2B, T = Bn / 4, D = 2;
   const int n = 1 << lv.log2N, K = lv.K, Kr = lv.Kr;
-  const int u0 = w.slice * (Bn / 2) + threadIdx.x, u1 = u0 + T;
+  const int u0 = slice * (Bn / 2) + threadIdx.x, u1 = u0 + T;
   const bool dc = (u0 == 0);
   const float* sc = kScaled<SPEC> ? lv.scale + (size_t)slot * K : nullptr;
   float2 a0 = make_float2(0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
@@ -738,8 +738,7 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T, 1024 / FftShape<LOG2M>::T)
         // level block floor(k / p) + 1, its slice k mod p
         const EngLevel lv = levels[w.lvl];
         const int pshift = lv.log2N - LOG2M;
-        if ((int)(k & ((1LL << pshift) - 1)) != w.slice) continue;
-        eng_level_item<LOG2M, SPEC>(lv, w, slot, (k >> pshift) + 1);
+        eng_level_item<LOG2M, SPEC>(lv, w, slot, (k >> pshift) + 1, (int)(k & ((1LL << pshift) - 1)));
       }
     }
   }
@@ -858,22 +857,27 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T)
 
 // Level partial rows of a newly committed IR: the level block j_c = floor(k / p)
 // (head still to come at block (j_c + 1) p - 1 >= k) and j_c + 1 (its items
-// run from block j_c p on, some perhaps with the old IR), every slice.
+// run from block j_c p on, some perhaps with the old IR), every slice: one
+// (item, slice) pair per step of the grid-stride loop, max_slices per item.
 template <int LOG2B, int SPEC>
 __global__ void __launch_bounds__((1 << LOG2B) / 4)
     eng_level_commit_items_kernel(const EngChan* __restrict__ chans, const EngLevel* __restrict__ levels,
-                                  const EngItem* __restrict__ items, int item0, int nitems,
+                                  const EngItem* __restrict__ items, int item0, int nitems, int max_slices,
                                   const long long* __restrict__ block) {
   const long long k = *block;
-  for (int it = item0 + (int)blockIdx.x; it < item0 + nitems; it += gridDim.x) {
-    const EngItem w = items[it];
+  const long long total = (long long)nitems * max_slices;
+  for (long long v = blockIdx.x; v < total; v += gridDim.x) {
+    const EngItem w = items[item0 + (int)(v / max_slices)];
+    const int slice = (int)(v % max_slices);
     if (w.chan < 0 || w.lvl < 0) continue;
+    const EngLevel lv = levels[w.lvl];
+    const int pshift = lv.log2N - LOG2B;
+    if (slice >= (1 << pshift)) continue;
     const EngChan ch = chans[w.chan];
     if (!ch.pending) continue;
-    const EngLevel lv = levels[w.lvl];
-    const long long jc = k >> (lv.log2N - LOG2B);
-    eng_level_item<LOG2B, SPEC>(lv, w, 1 - ch.active, jc);
-    eng_level_item<LOG2B, SPEC>(lv, w, 1 - ch.active, jc + 1);
+    const long long jc = k >> pshift;
+    eng_level_item<LOG2B, SPEC>(lv, w, 1 - ch.active, jc, slice);
+    eng_level_item<LOG2B, SPEC>(lv, w, 1 - ch.active, jc + 1, slice);
   }
 }
 
@@ -1031,9 +1035,9 @@ cudaError_t commit_t(const EngChan* chans, const EngItem* items, int item0, int 
 
 template <int LOG2M, int SPEC>
 cudaError_t level_commit_items_t(const EngChan* chans, const EngLevel* levels, const EngItem* items, int item0,
-                                 int nitems, int grid, const long long* block, cudaStream_t st) {
+                                 int nitems, int max_slices, int grid, const long long* block, cudaStream_t st) {
   eng_level_commit_items_kernel<LOG2M, SPEC><<<grid, (1 << LOG2M) / 4, 0, st>>>(chans, levels, items, item0, nitems,
-                                                                                 block);
+                                                                                 max_slices, block);
   return cudaGetLastError();
 }
 
@@ -1168,10 +1172,10 @@ cudaError_t eng_launch_commit(int log2B, int spec, const EngChan* chans, const E
 }
 
 cudaError_t eng_launch_level_commit_items(int log2B, int spec, const EngChan* chans, const EngLevel* levels,
-                                          const EngItem* items, int item0, int nitems, int grid,
+                                          const EngItem* items, int item0, int nitems, int max_slices, int grid,
                                           const long long* block, cudaStream_t st) {
-  if (nitems <= 0) return cudaSuccess;
-  ENG_DISPATCH(log2B, spec, level_commit_items_t, chans, levels, items, item0, nitems, grid, block, st);
+  if (nitems <= 0 || max_slices <= 0) return cudaSuccess;
+  ENG_DISPATCH(log2B, spec, level_commit_items_t, chans, levels, items, item0, nitems, max_slices, grid, block, st);
 }
 
 cudaError_t eng_launch_level_commit_out(int log2B, int log2N, int spec, const EngChan* chans,
