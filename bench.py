@@ -616,6 +616,14 @@ def run_ours(args):
 
         configs = {"cfg3": bw.engine_uneven(ctx), "cfg4": bw.nonuniform_long(ctx),
                    "cfg5": bw.serving_cfg5(ctx, seconds=10.0)}
+    # several GPUs: the serving mix sharded over the ranks (sessions placed by
+    # the engines' admission rule, no audio crossing GPUs), every rank its own
+    # engine; latencies gathered to rank 0
+    sharded = None
+    if world > 1 and not args.no_configs:
+        from tan_b200 import serving
+
+        sharded = serving.serve_sharded(pg, ctx, sessions=300 * world, blocks=1000)
     # the CPU baseline loads every host core for seconds; it runs after the
     # latency measurements above, whose host-side copies it would slow down
     cpu = None
@@ -673,6 +681,8 @@ def run_ours(args):
             line["roofline_serving"] = roofline_serving
         if configs:
             line["configs"] = configs
+        if sharded:
+            line["serving_sharded"] = sharded
         print(json.dumps(line), flush=True)
     ctx.Release()
     if pg:

@@ -179,6 +179,79 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
     return out
 
 
+class EngineSlots:
+    """A rank's engine as the sharding control plane sees it: open(spec) ->
+    session or None (refused by the budget or the slot table), close(session)."""
+
+    def __init__(self, engine):
+        self.engine = engine
+
+    def open(self, spec):
+        if spec.levels:
+            rc, sess = self.engine.open_session_nu(spec.channels, spec.ir_length, list(spec.levels))
+        else:
+            rc, sess = self.engine.open_session(spec.channels, spec.ir_length)
+        return sess if rc == cv.AMF_OK else None
+
+    def close(self, sess):
+        sess.close()
+
+
+def serve_sharded(pg, ctx, sessions=600, blocks=1500, swap_rate=0.5, block=256, spectrum=eng.SPECTRUM_FP32,
+                  budget=150 << 30, ch_range=(1, 8), len_range=(8192, 524288), seed=20261203 + 4):
+    """Sessions sharded over the ranks of `pg` (one GPU each): rank 0 draws the
+    session mix (channels, IR lengths), sharding.RankServer places it by the
+    engines' admission rule (refused sessions re-placed on the other ranks),
+    and every rank serves its shard with its own engine for `blocks` blocks,
+    with Poisson IR swaps. No audio crosses GPUs; the per-rank block latencies
+    are gathered to rank 0. Returns (on every rank) the latency percentiles
+    over all ranks' blocks, and the channels per rank."""
+    import torch
+
+    from . import sharding as sh
+
+    rank, world = pg.get_rank(), pg.get_world_size()
+    g = np.random.Generator(np.random.PCG64(seed))
+    specs = []
+    for sid in range(sessions):
+        C = int(g.integers(ch_range[0], ch_range[1] + 1))
+        L = int(np.exp(g.uniform(np.log(len_range[0]), np.log(len_range[1]))))
+        specs.append(sh.SessionSpec(sid, C, L))
+    e = eng.Engine(ctx, block, spectrum, budget_bytes=budget, max_channels=1 << 16)
+    srv = sh.RankServer(pg, EngineSlots(e), block, budget)
+    placement = srv.place(specs)
+    gl = np.random.Generator(np.random.PCG64(seed + 100 + rank))
+    pool = IRPool(gl, length=len_range[1])
+    mine = {sid: s for sid, s in srv.handles.items()}
+    for sid, sess in mine.items():
+        sess.update_response_td(pool.get(gl, sess.channels, sess.ir_length), block_until_ready=True)
+    e.inp[:] = gl.uniform(-1.0, 1.0, e.inp.shape).astype(np.float32)
+    dt = block / FS
+    next_swap = {sid: gl.exponential(1.0 / swap_rate) for sid in mine}
+    lat = []
+    t = 0.0
+    for k in range(blocks):
+        t0 = time.perf_counter()
+        for sid, sess in mine.items():
+            if next_swap[sid] <= t:
+                sess.update_response_td(pool.get(gl, sess.channels, sess.ir_length))
+                next_swap[sid] = t + gl.exponential(1.0 / swap_rate)
+        if mine:
+            assert e.process() == cv.AMF_OK, cv.last_error()
+        lat.append(1000.0 * (time.perf_counter() - t0))
+        t += dt
+    chans = e.info()["channels"]
+    e.release()
+    all_lat = [None] * world
+    pg.all_gather_object(all_lat, (lat, chans))
+    lats = np.concatenate([np.asarray(a) for a, _ in all_lat])
+    torch.cuda.synchronize()
+    return {"ranks": world, "blocks": blocks, "deadline_ms": 1000.0 * block / FS, "latency_ms": percentiles(lats),
+            "deadline_misses": int((lats > 1000.0 * block / FS).sum()),
+            "channels_per_rank": [c for _, c in all_lat], "sessions": sessions,
+            "unplaced": int(sum(1 for r in placement.values() if r < 0))}
+
+
 def _block_latencies_batched(ctx, nsess, C, L, block, spectrum, blocks, g, pool):
     e = eng.Engine(ctx, block, spectrum, budget_bytes=170 << 30, max_channels=nsess * C + 8)
     sess = []

@@ -99,3 +99,100 @@ def test_failed_rank_ends_peers_with_an_error():
     errs = {r: e for r, _, _, e in out}
     assert errs[1] == "RuntimeError"
     assert errs[0] is not None  # the peer's collective failed or timed out, it did not hang
+
+
+class FakeEngine:
+    """Stand-in for a rank's engine on CPU: a byte budget (the engine's own
+    session size rule) and a set of sessions it refuses (as a fragmented arena
+    or a full slot table would)."""
+
+    def __init__(self, budget, refuse=()):
+        self.budget, self.used, self.refuse, self.open_ids = budget, 0, set(refuse), set()
+
+    def open(self, spec):
+        need = sh.device_bytes(spec, 256)
+        if spec.sid in self.refuse or self.used + need > self.budget:
+            return None
+        self.used += need
+        self.open_ids.add(spec.sid)
+        return (spec.sid, need)
+
+    def close(self, handle):
+        self.used -= handle[1]
+        self.open_ids.discard(handle[0])
+
+
+def _server_worker(rank, world, port, mode, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    import time
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=20))
+    try:
+        store = dist.distributed_c10d._get_default_store()
+        ss = _sessions(24, seed=11)
+        budget = sum(sh.device_bytes(s, 256) for s in ss)  # either rank could hold everything
+        refuse = {s.sid for s in ss[:5]} if rank == 1 else set()
+        srv = sh.RankServer(dist, FakeEngine(budget, refuse), 256, budget, store)
+        pl = srv.place(ss)
+        mine_first = sorted(srv.handles)
+        taken = []
+        if mode == "leave":
+            for k in range(200):  # blocks
+                if rank == 1 and k == 3:
+                    srv.leave()
+                    break
+                if rank == 0:
+                    taken += srv.check_peers()
+                    if srv.left:
+                        break
+                time.sleep(0.01)
+        q.put((rank, pl, mine_first, sorted(srv.engine.open_ids), taken, None))
+    except Exception as e:  # noqa: BLE001
+        q.put((rank, None, None, None, None, repr(e)))
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:
+            pass
+
+
+def _run_server(mode):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_server_worker, args=(r, 2, port, mode, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        if p.is_alive():
+            p.kill()
+    return out
+
+
+def test_rank_server_replaces_refused_sessions_on_the_other_rank():
+    (r0, pl0, m0, open0, _, e0), (r1, pl1, m1, open1, _, e1) = _run_server("ok")
+    assert e0 is None and e1 is None, (e0, e1)
+    assert pl0 == pl1  # every rank holds the same placement
+    ss = _sessions(24, seed=11)
+    assert sorted(pl0) == [s.sid for s in ss] and all(r in (0, 1) for r in pl0.values())
+    assert all(pl0[s.sid] == 0 for s in ss[:5])  # refused by rank 1, re-placed on rank 0
+    assert sorted(m0 + m1) == sorted(s.sid for s in ss) and not set(m0) & set(m1)
+    assert set(m0) == {sid for sid, r in pl0.items() if r == 0}
+
+
+def test_rank_leaving_between_blocks_hands_its_sessions_over():
+    (r0, pl0, m0, open0, taken, e0), (r1, pl1, m1, open1, _, e1) = _run_server("leave")
+    assert e0 is None and e1 is None, (e0, e1)
+    assert m1 and open1 == []  # rank 1 closed its sessions when it left
+    assert sorted(taken) == sorted(m1)  # rank 0 took every one of them over
+    assert sorted(open0) == sorted(m0 + m1)
+
+
+def test_device_bytes_follow_the_engine_rule_for_non_uniform_sessions():
+    u = sh.SessionSpec(0, 2, 1 << 20)
+    n = sh.SessionSpec(1, 2, 1 << 20, ((256, 2), (512, 2), (1024, 2), (2048, 2), (4096, 2), (8192, 2), (16384, 63)))
+    assert sh.device_bytes(n, 256) > 0 and sh.device_bytes(u, 256) > 0
+    assert sh.tail_bytes(n, 256) < sh.tail_bytes(u, 256) / 8  # the levels stream far fewer bytes per block
