@@ -182,7 +182,6 @@ struct tanb_engine {
   float* h_out = nullptr;  // pinned; written in place by the heads
   long long* d_block = nullptr;     // blocks processed (device)
   unsigned int* d_done = nullptr;   // CTAs finished in the running block
-  unsigned* d_item_count = nullptr; // [max_channels] work items done in the running block
   long long k_host = 0;             // blocks enqueued (the device counter after they ran)
   float* h_ir = nullptr;
   float* d_ir = nullptr;
@@ -224,7 +223,6 @@ size_t chan_bytes(const tanb_engine* e, int P, int nitem, const std::vector<Leve
   per += align_up((size_t)P * B * fdl_bytes(e->spec));                   // fdl
   per += align_up(B * 4);                                                // prev
   per += align_up(4 * (size_t)nitem * B * 8);                            // partials
-  per += align_up(2 * B * 8);                                            // tail rows
   if (!lv.empty()) {
     per += align_up(sizeof(EngNu)) + align_up((size_t)rin * 4);
     for (const LevelSpec& l : lv) {
@@ -260,7 +258,6 @@ void free_engine(tanb_engine* e) {
   cudaFree(e->d_items);
   cudaFree(e->d_levels);
   cudaFree(e->d_block);
-  cudaFree(e->d_item_count);
   cudaFree(e->d_ir);
   cudaFree(e->d_upd);
   cudaFree(e->d_lupd);
@@ -398,7 +395,7 @@ cudaError_t enqueue_block(tanb_engine* e, const tanb::EngRows& rows, unsigned du
     if ((r = cudaStreamWaitEvent(e->lstream, e->ev_fork, 0)) != cudaSuccess) return r;
   }
   r = tanb::eng_launch_block(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, e->d_items, (int)e->nitems_hwm, tc,
-                             e->d_levels, rows, e->d_tw, sync, total, e->d_item_count, e->stream);
+                             e->d_levels, rows, e->d_tw, sync, total, e->stream);
   if (r != cudaSuccess || !due) return r;
   for (int c = 0; c < e->nclass; ++c) {
     if (!(due >> c & 1u)) continue;
@@ -621,8 +618,6 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
     base += align_up(B * 4);
     ch.part = reinterpret_cast<float2*>(base);
     base += align_up(4 * (size_t)s.nitem * B * 8);
-    ch.tsum = reinterpret_cast<float2*>(base);
-    base += align_up(2 * B * 8);
     zero.push_back({z0, (size_t)(base - z0)});
     ch.P = s.P;
     ch.nitem = s.nitem;
@@ -898,7 +893,6 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   if (r == cudaSuccess) r = cudaMalloc(&e->d_items, e->max_items * sizeof(EngItem));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_levels, std::max<size_t>(1, nlev) * sizeof(EngLevel));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_block, 2 * sizeof(long long));
-  if (r == cudaSuccess) r = cudaMalloc(&e->d_item_count, e->max_channels * sizeof(unsigned));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_upd, e->max_channels * sizeof(EngUpd));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_lupd, tanb::kMaxLevels * e->max_channels * sizeof(EngLvlUpd));
   if (r == cudaSuccess) r = cudaMalloc(&e->d_tw, 2 * e->B * sizeof(float2));
@@ -952,7 +946,6 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   if (r == cudaSuccess) r = upload_levels(e, 0, nlev);
   if (e->d_block) e->d_done = reinterpret_cast<unsigned int*>(e->d_block + 1);
   if (r == cudaSuccess) r = cudaMemsetAsync(e->d_block, 0, 2 * sizeof(long long), e->stream);
-  if (r == cudaSuccess) r = cudaMemsetAsync(e->d_item_count, 0, e->max_channels * sizeof(unsigned), e->stream);
   if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
   // tail CTAs of the block launch: as many as fit on the GPU at once (B / 4
   // threads each at up to 64 registers: 1024 threads per SM)
@@ -1140,11 +1133,8 @@ int32_t tanb_engine_info(tanb_engine* e, int64_t out[8]) {
     // partitions [2, P) of IR spectrum and delay line and write their partial
     // rows; the head reads input, history, the partial rows, partitions 0 and
     // 1 of the spectrum and X_{k-1}, and writes output, history and X_k
-    // (the channel's last item reads the partial rows back and writes the
-    // tail row, which the head reads)
-    const int64_t tail = (s.P > 2 ? (int64_t)(s.P - 2) * B * (sb + xb) : 0) + (int64_t)s.nitem * B * 8 * 2 +
-                         (s.nitem ? B * 8 : 0);
-    int64_t head = 4 * B * 4 + (s.nitem ? B * 8 : 0) + (s.P > 1 ? 2 * B * sb + B * xb : B * sb) + B * xb;
+    const int64_t tail = (s.P > 2 ? (int64_t)(s.P - 2) * B * (sb + xb) : 0) + (int64_t)s.nitem * B * 8;
+    int64_t head = 4 * B * 4 + (int64_t)s.nitem * B * 8 + (s.P > 1 ? 2 * B * sb + B * xb : B * sb) + B * xb;
     // non-uniform levels, per base block on average over their periods: the
     // level items stream partitions [2, K) and write the partial rows; the
     // level head reads its frame, the partial rows, partitions 0 and 1 and

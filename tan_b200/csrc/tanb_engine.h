@@ -58,8 +58,6 @@ struct EngChan {
   float2* fdl;    // delay line [P][B]; slot (cur + i) mod P holds X_{k-i}
   float* prev;    // previous input block [B] (overlap-save history)
   float2* part;   // tail partial sums [2: block parity][2: IR in use, new IR][nitem][B]
-  float2* tsum;   // [2: block parity][B]: the partial rows of the IR in use summed in
-                  // row order by the last work item of the channel to finish
   const EngNu* nu;  // non-uniform extras, null for a uniformly partitioned channel
   int32_t P;      // partitions
   int32_t nitem;  // tail work items of this channel's base level
@@ -105,8 +103,7 @@ struct EngLvlUpd {
 
 // Block-level counters in device memory: blocks processed (its parity selects
 // the partial-sum rows) and CTAs finished in the running block (over every
-// kernel of the block). The block launch also takes a per-slot count of the
-// work items done in the running block (zero between blocks).
+// kernel of the block).
 struct EngSync {
   long long* block;
   unsigned int* done;
@@ -135,7 +132,7 @@ cudaError_t eng_launch_level_ir(int log2N, int spec, EngLevel* levels, const Eng
 // beside it): the last of them to finish advances the channel state.
 cudaError_t eng_launch_block(int log2B, int spec, EngChan* chans, int nslots, const EngItem* items, int nitems,
                              int tail_ctas, const EngLevel* levels, const EngRows& rows, const float2* tw,
-                             EngSync sync, unsigned total, unsigned* item_count, cudaStream_t st);
+                             EngSync sync, unsigned total, cudaStream_t st);
 // Level heads of one size class (2^log2N) for a block at which that size is
 // due: one CTA per level record [0, nlev) of `levels` (the class's table).
 cudaError_t eng_launch_level_heads(int log2B, int log2N, int spec, EngChan* chans, int nslots, const EngLevel* levels,

@@ -449,28 +449,26 @@ __device__ __forceinline__ float2 lv_spec_bin(const EngLevel& lv, int slot, int 
 // slice `slice` (B bins: units [slice B / 2, (slice + 1) B / 2)), into partial
 // row w.row of parity jb & 1. B / 4 threads, two units each, as eng_item.
 template <int LOG2B, int SPEC>
-__device__ __noinline__ void eng_level_item_body(const void* H, const float* scale, const float2* fdl, float2* part,
-                                                 int log2N, int K, int Kr, int ngroup, int i0, int i1, int row,
-                                                 int slot, long long jb, int slice) {
+__device__ __noinline__ void eng_level_item(const EngLevel& lv, const EngItem& w, int slot, long long jb, int slice) {
   constexpr int Bn = 1 << LOG2B, T = Bn / 4, D = 2;
-  const int n = 1 << log2N;
+  const int n = 1 << lv.log2N, K = lv.K, Kr = lv.Kr;
   const int u0 = slice * (Bn / 2) + threadIdx.x, u1 = u0 + T;
   const bool dc = (u0 == 0);
-  const float* sc = kScaled<SPEC> ? scale + (size_t)slot * K : nullptr;
+  const float* sc = kScaled<SPEC> ? lv.scale + (size_t)slot * K : nullptr;
   float2 a0 = make_float2(0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
-  int fs = lv_slot(jb - i0, Kr);
-  int i = i0;
-  for (; i + D <= i1; i += D) {
+  int fs = lv_slot(jb - w.i0, Kr);
+  int i = w.i0;
+  for (; i + D <= w.i1; i += D) {
     float4 f0[D], f1[D];
     float2 p0[D], q0[D], p1[D], q1[D];
     float s[D];
 #pragma unroll
     for (int q = 0; q < D; ++q) {
-      f0[q] = lv_x_unit<SPEC>(fdl, n, fs, u0);
-      f1[q] = lv_x_unit<SPEC>(fdl, n, fs, u1);
-      const size_t hrow = (size_t)slot * K + i + q;
-      lv_h2<SPEC>(H, n, hrow, u0, p0[q], q0[q]);
-      lv_h2<SPEC>(H, n, hrow, u1, p1[q], q1[q]);
+      f0[q] = lv_x_unit<SPEC>(lv.fdl, n, fs, u0);
+      f1[q] = lv_x_unit<SPEC>(lv.fdl, n, fs, u1);
+      const size_t row = (size_t)slot * K + i + q;
+      lv_h2<SPEC>(lv.H, n, row, u0, p0[q], q0[q]);
+      lv_h2<SPEC>(lv.H, n, row, u1, p1[q], q1[q]);
       s[q] = kScaled<SPEC> ? __ldg(sc + i + q) : 1.f;
       fs = (fs + 1 == Kr) ? 0 : fs + 1;
     }
@@ -488,12 +486,12 @@ __device__ __noinline__ void eng_level_item_body(const void* H, const float* sca
       b1 = c_mac(b1, gb, q1[q]);
     }
   }
-  for (; i < i1; ++i) {
-    const float4 g0 = lv_x_unit<SPEC>(fdl, n, fs, u0), g1 = lv_x_unit<SPEC>(fdl, n, fs, u1);
+  for (; i < w.i1; ++i) {
+    const float4 g0 = lv_x_unit<SPEC>(lv.fdl, n, fs, u0), g1 = lv_x_unit<SPEC>(lv.fdl, n, fs, u1);
     float2 pa, qa, pb, qb;
-    const size_t hrow = (size_t)slot * K + i;
-    lv_h2<SPEC>(H, n, hrow, u0, pa, qa);
-    lv_h2<SPEC>(H, n, hrow, u1, pb, qb);
+    const size_t row = (size_t)slot * K + i;
+    lv_h2<SPEC>(lv.H, n, row, u0, pa, qa);
+    lv_h2<SPEC>(lv.H, n, row, u1, pb, qb);
     if (kScaled<SPEC>) {
       const float s = __ldg(sc + i);
       pa.x *= s; pa.y *= s; qa.x *= s; qa.y *= s;
@@ -507,16 +505,9 @@ __device__ __noinline__ void eng_level_item_body(const void* H, const float* sca
     b0 = c_mac(b0, ga, pb);
     b1 = c_mac(b1, gb, qb);
   }
-  float4* dst = reinterpret_cast<float4*>(part + ((size_t)((jb & 1) * ngroup + row)) * n);
+  float4* dst = reinterpret_cast<float4*>(lv.part + ((size_t)((jb & 1) * lv.ngroup + w.row)) * n);
   dst[u0] = make_float4(a0.x, a0.y, a1.x, a1.y);
   dst[u1] = make_float4(b0.x, b0.y, b1.x, b1.y);
-}
-
-template <int LOG2B, int SPEC>
-__device__ __forceinline__ void eng_level_item(const EngLevel& lv, const EngItem& w, int slot, long long jb,
-                                               int slice) {
-  eng_level_item_body<LOG2B, SPEC>(lv.H, lv.scale, lv.fdl, lv.part, lv.log2N, lv.K, lv.Kr, lv.ngroup, w.i0, w.i1,
-                                   w.row, slot, jb, slice);
 }
 
 __device__ __forceinline__ const float* row_in(const EngRows& r, int c) {
@@ -526,43 +517,9 @@ __device__ __forceinline__ float* row_out(const EngRows& r, int c) {
   return r.out_tab ? r.out_tab[c] : (r.out_base ? r.out_base + (size_t)c * r.ld : nullptr);
 }
 
-// Counts a finished base work item of channel `chan` (its partial row for
-// block parity `parity` is stored); the channel's last item to finish sums the
-// partial rows in row order into the channel's tail row of that parity, so
-// that the head reads one row. The order is fixed, so the sum does not depend
-// on which item finishes last.
-template <int LOG2M>
-__device__ __noinline__ void eng_item_finish(const float2* part, float2* tsum, int nitem, int chan,
-                                             unsigned* __restrict__ count, int parity) {
-  constexpr int M = 1 << LOG2M, U = M / 2, T = M / 4;
-  __shared__ int last_item;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last_item = (atomicAdd(count + chan, 1u) == (unsigned)nitem - 1) ? 1 : 0;
-  __syncthreads();
-  if (!last_item) return;
-  __threadfence();
-  // mode-0 rows of this parity: part + (parity * 2 * nitem) rows
-  const float4* rows = reinterpret_cast<const float4*>(part + (size_t)parity * 2 * nitem * M);
-  float4* dst = reinterpret_cast<float4*>(tsum + (size_t)parity * M);
-  for (int u = threadIdx.x; u < U; u += T) {
-    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int r = 0; r < nitem; ++r) {
-      const float4 v = __ldcg(rows + (size_t)r * U + u);
-      a.x += v.x;
-      a.y += v.y;
-      a.z += v.z;
-      a.w += v.w;
-    }
-    dst[u] = a;
-  }
-  if (threadIdx.x == 0) count[chan] = 0u;
-}
-
 // Head of block k for one channel (state `ch` as at launch). Tail of the IR in
-// use: the channel's tail row of parity k (its items' partial rows, summed)
-// plus X_{k-1} * H_1; on a swap block the same for the new IR (the mode-1
-// rows, summed here), and the output crossfades. A non-uniform
+// use: the partial-sum rows of parity k plus X_{k-1} * H_1; on a swap block the
+// same for the new IR (mode-1 rows), and the output crossfades. A non-uniform
 // channel also appends x_k to its input history and adds its levels' output
 // rings (of the IR slot in use; on a swap block those of each IR to its side
 // of the crossfade) in level order.
@@ -620,18 +577,17 @@ __device__ __forceinline__ void eng_head(const EngChan& ch, float2* sm, const fl
 
   // X_k goes into delay-line slot cur; X_{k-1} (partition 1) is in ch.cur
   const float inv_n = 1.0f / (float)(2 * M);
-  const float2* ts = ch.tsum + (size_t)parity * M;
+  const float2* pa = part_row(ch, parity, 0, 0, M);
   const float2* pb = part_row(ch, parity, 1, 0, M);
   for (int k = threadIdx.x; k <= M / 2; k += T) {
     const int km = (k == 0) ? 0 : M - k;
-    // tails: the work items' sum (the tail row), then partition 1
+    // tails: partial sums of the work items in item order, then partition 1
     float2 tk = make_float2(0.f, 0.f), tm = tk, uk = tk, um = tk;
-    if (ch.nitem) {
-      tk = ts[k];
-      tm = ts[km];
-    }
-    if (swap) {
-      for (int r = 0; r < ch.nitem; ++r) {
+    for (int r = 0; r < ch.nitem; ++r) {
+      const float2 a = pa[(size_t)r * M + k], b = pa[(size_t)r * M + km];
+      tk.x += a.x; tk.y += a.y;
+      tm.x += b.x; tm.y += b.y;
+      if (swap) {
         const float2 a1 = pb[(size_t)r * M + k], b1 = pb[(size_t)r * M + km];
         uk.x += a1.x; uk.y += a1.y;
         um.x += b1.x; um.y += b1.y;
@@ -756,7 +712,7 @@ template <int LOG2M, int SPEC>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T, 1024 / FftShape<LOG2M>::T)
     eng_block_kernel(EngChan* __restrict__ chans, int nslots, const EngItem* __restrict__ items, int nitems,
                      const EngLevel* __restrict__ levels, EngRows rows, const float2* __restrict__ tw, EngSync sync,
-                     unsigned total, unsigned* __restrict__ item_count) {
+                     unsigned total) {
   extern __shared__ float2 sm[];
   const long long k = *sync.block;  // blocks processed before this one
   const int parity = (int)(k & 1);
@@ -778,7 +734,6 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T, 1024 / FftShape<LOG2M>::T)
       const int slot = ch.pending ? 1 - ch.active : ch.active;
       if (w.lvl < 0) {
         eng_item<LOG2M, SPEC>(ch, w, slot, -2, parity ^ 1, 0);
-        eng_item_finish<LOG2M>(ch.part, ch.tsum, ch.nitem, w.chan, item_count, parity ^ 1);
       } else {
         // level block floor(k / p) + 1, its slice k mod p
         const EngLevel lv = levels[w.lvl];
@@ -1054,10 +1009,10 @@ cudaError_t level_ir_t(EngLevel* levels, const EngLvlUpd* upd, int nupd, int max
 template <int LOG2M, int SPEC>
 cudaError_t block_t(EngChan* chans, int nslots, const EngItem* items, int nitems, int tail_ctas,
                     const EngLevel* levels, const EngRows& rows, const float2* tw, EngSync sync, unsigned total,
-                    unsigned* item_count, cudaStream_t st) {
+                    cudaStream_t st) {
   using S = FftShape<LOG2M>;
   eng_block_kernel<LOG2M, SPEC><<<nslots + tail_ctas, S::T, 2 * S::M * sizeof(float2), st>>>(
-      chans, nslots, items, nitems, levels, rows, tw, sync, total, item_count);
+      chans, nslots, items, nitems, levels, rows, tw, sync, total);
   return cudaGetLastError();
 }
 
@@ -1192,10 +1147,9 @@ unsigned eng_block_ctas(int nslots, int tail_ctas) { return (unsigned)(nslots + 
 
 cudaError_t eng_launch_block(int log2B, int spec, EngChan* chans, int nslots, const EngItem* items, int nitems,
                              int tail_ctas, const EngLevel* levels, const EngRows& rows, const float2* tw,
-                             EngSync sync, unsigned total, unsigned* item_count, cudaStream_t st) {
+                             EngSync sync, unsigned total, cudaStream_t st) {
   if (nslots <= 0) return cudaSuccess;
-  ENG_DISPATCH(log2B, spec, block_t, chans, nslots, items, nitems, tail_ctas, levels, rows, tw, sync, total,
-               item_count, st);
+  ENG_DISPATCH(log2B, spec, block_t, chans, nslots, items, nitems, tail_ctas, levels, rows, tw, sync, total, st);
 }
 
 cudaError_t eng_launch_level_heads(int log2B, int log2N, int spec, EngChan* chans, int nslots, const EngLevel* levels,
