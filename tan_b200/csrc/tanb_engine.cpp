@@ -341,7 +341,7 @@ cudaError_t commit_updates(tanb_engine* e) {
     if (s.nitem)
       r = tanb::eng_launch_commit(e->log2B, e->spec, e->d_chans, e->d_items, (int)s.item0, nit, grid, e->d_block,
                                   e->stream);
-    if (r == cudaSuccess && nit > s.C * s.nitem) {
+    if (r == cudaSuccess && nit > 2 * s.C * s.nitem) {
       int slices = 1;  // bin slices of the largest level with work items
       for (const LevelSpec& l : s.lv)
         if (l.ngroup) slices = std::max(slices, 1 << (l.log2N - e->log2B));
@@ -527,7 +527,7 @@ cudaError_t grow_items(tanb_engine* e, size_t need) {
     return r;
   }
   std::memcpy(h, e->h_items, e->max_items * sizeof(EngItem));
-  for (size_t i = e->max_items; i < cap; ++i) h[i] = EngItem{-1, 0, 0, 0, -1};
+  for (size_t i = e->max_items; i < cap; ++i) h[i] = EngItem{-1, 0, 0, 0, -1, 0};
   r = cudaMemcpyAsync(d, h, cap * sizeof(EngItem), cudaMemcpyHostToDevice, e->stream);
   if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
   if (r != cudaSuccess) {
@@ -562,7 +562,7 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
   }
   // work items cover partitions [2, P); the head does partitions 0 and 1
   s.nitem = s.P > 2 ? (s.P - 2 + e->Q - 1) / e->Q : 0;
-  s.items_per_chan = s.nitem;
+  s.items_per_chan = 2 * s.nitem;  // two halves of the bins per partition group
   for (const LevelSpec& l : s.lv) s.items_per_chan += l.ngroup;
   const size_t per_chan = chan_bytes(e, s.P, s.nitem, s.lv, s.rin);
   s.arena_bytes = per_chan * s.C;
@@ -629,7 +629,8 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
     size_t it = s.item0 + (size_t)j * s.items_per_chan;
     for (int r = 0; r < s.nitem; ++r) {
       const int i0 = 2 + r * e->Q;
-      e->h_items[it++] = EngItem{slot, i0, std::min(s.P, i0 + e->Q), r, -1};
+      for (int half = 0; half < 2; ++half)
+        e->h_items[it++] = EngItem{slot, i0, std::min(s.P, i0 + e->Q), r, -1, half};
     }
     if (!s.lv.empty()) {
       EngNu& nu = nus[j];
@@ -674,7 +675,7 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
         for (int g = 0; g < ls.ngroup; ++g) {
           const int i0 = 2 + g * ls.q;
           e->h_items[it++] = EngItem{slot, i0, std::min(ls.K, i0 + ls.q), g, (int)(c * e->max_channels +
-                                     s.lv_first[l] + j)};
+                                     s.lv_first[l] + j), 0};
         }
       }
     }
@@ -920,7 +921,7 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
                  cudaGetErrorString(r));
   }
   std::memset(e->h_chans, 0, e->max_channels * sizeof(EngChan));
-  for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0, -1};
+  for (size_t i = 0; i < e->max_items; ++i) e->h_items[i] = EngItem{-1, 0, 0, 0, -1, 0};
   for (size_t i = 0; i < nlev; ++i) {
     e->h_levels[i] = EngLevel{};
     e->h_levels[i].chan = -1;
@@ -1025,7 +1026,7 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   if (s.staged_ev) cudaEventDestroy(s.staged_ev);
   for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j] = EngChan{};
   const size_t nit_total = (size_t)s.C * s.items_per_chan;
-  for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0, -1};
+  for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0, -1, 0};
   for (size_t l = 0; l < s.lv.size(); ++l) {
     const size_t first = (size_t)level_class(e, s.lv[l].log2N) * e->max_channels + s.lv_first[l];
     for (int j = 0; j < s.C; ++j) {

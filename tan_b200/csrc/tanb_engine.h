@@ -70,8 +70,9 @@ struct EngChan {
 };
 
 // A tail work item. Base level (lvl < 0): partitions [i0, i1) (i0 >= 2;
-// partitions 0 and 1 belong to the head) of channel `chan`, partial sum row
-// `row`, every block. Level item (lvl >= 0, index into the level table):
+// partitions 0 and 1 belong to the head) of channel `chan`, bins of half
+// `slice` (0: [0, B/2), 1: [B/2, B)) of partial sum row `row`, every block.
+// Level item (lvl >= 0, index into the level table):
 // partitions [i0, i1) of that level, partial row `row`; at base block k it
 // takes bin slice k mod p ([s B, (s + 1) B) of the level's N-bin rows) of
 // the level block after the one completing in this period, so a level's tail
@@ -81,6 +82,7 @@ struct EngItem {
   int32_t i0, i1;
   int32_t row;
   int32_t lvl;
+  int32_t slice;  // base items: the half of the row's bins
 };
 
 // One channel of an IR update: channel `chan`'s new IR, read from `src`

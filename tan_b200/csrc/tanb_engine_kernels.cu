@@ -315,69 +315,56 @@ __device__ __forceinline__ float2* part_row(const EngChan& ch, int parity, int m
 
 // One work item: sum over partitions i in [w.i0, w.i1) of delay-line slot
 // (ch.cur + i + fs_off) mod P times IR-spectrum partition i of `slot`, into
-// part_row(parity, mode, w.row). M / 4 threads, units u and u + M / 4 each.
+// part_row(parity, mode, w.row), over half w.slice of the row's bins: M / 4
+// threads, one float4 unit (two bins) each, four partitions' loads in flight
+// (a base item covers half the bins, so the latency chain of one item is half
+// as long and a channel's two halves run as two items).
 template <int LOG2M, int SPEC>
 __device__ __forceinline__ void eng_item(const EngChan& ch, const EngItem& w, int slot, int fs_off, int parity,
                                          int mode) {
-  constexpr int M = 1 << LOG2M, U = M / 2, T = M / 4, D = 2;
+  constexpr int M = 1 << LOG2M, U = M / 2, T = M / 4, D = 4;
   const int P = ch.P;
   const size_t hb = ((size_t)slot * P * M) / 2;  // unit index of (slot, partition 0)
   const float* sc = kScaled<SPEC> ? ch.scale + (size_t)slot * P : nullptr;
-  const int u0 = threadIdx.x, u1 = threadIdx.x + T;
-  const bool dc = (u0 == 0);
-  float2 a0 = make_float2(0.f, 0.f), a1 = a0, b0 = a0, b1 = a0;
+  const int u = w.slice * T + threadIdx.x;
+  const bool dc = (u == 0);
+  float2 a0 = make_float2(0.f, 0.f), a1 = a0;
   int fs = (ch.cur + w.i0 + fs_off) % P;
   int i = w.i0;
   for (; i + D <= w.i1; i += D) {
-    float4 f0[D], f1[D];
-    float2 p0[D], q0[D], p1[D], q1[D];
+    float4 f[D];
+    float2 p[D], q[D];
     float s[D];
 #pragma unroll
-    for (int q = 0; q < D; ++q) {
-      f0[q] = x_unit<SPEC, M>(ch.fdl, fs, u0);
-      f1[q] = x_unit<SPEC, M>(ch.fdl, fs, u1);
-      const size_t hrow = hb + (size_t)(i + q) * U;
-      load_h2<SPEC, M>(ch.H, hrow + u0, p0[q], q0[q]);
-      load_h2<SPEC, M>(ch.H, hrow + u1, p1[q], q1[q]);
-      s[q] = kScaled<SPEC> ? __ldg(sc + i + q) : 1.f;
+    for (int j = 0; j < D; ++j) {
+      f[j] = x_unit<SPEC, M>(ch.fdl, fs, u);
+      load_h2<SPEC, M>(ch.H, hb + (size_t)(i + j) * U + u, p[j], q[j]);
+      s[j] = kScaled<SPEC> ? __ldg(sc + i + j) : 1.f;
       fs = (fs + 1 == P) ? 0 : fs + 1;
     }
 #pragma unroll
-    for (int q = 0; q < D; ++q) {
+    for (int j = 0; j < D; ++j) {
       if (kScaled<SPEC>) {
-        p0[q].x *= s[q]; p0[q].y *= s[q]; q0[q].x *= s[q]; q0[q].y *= s[q];
-        p1[q].x *= s[q]; p1[q].y *= s[q]; q1[q].x *= s[q]; q1[q].y *= s[q];
+        p[j].x *= s[j]; p[j].y *= s[j]; q[j].x *= s[j]; q[j].y *= s[j];
       }
-      const float2 fa = make_float2(f0[q].x, f0[q].y), fb = make_float2(f0[q].z, f0[q].w);
-      const float2 ga = make_float2(f1[q].x, f1[q].y), gb = make_float2(f1[q].z, f1[q].w);
-      a0 = dc ? c_mac_dc(a0, fa, p0[q]) : c_mac(a0, fa, p0[q]);
-      a1 = c_mac(a1, fb, q0[q]);
-      b0 = c_mac(b0, ga, p1[q]);
-      b1 = c_mac(b1, gb, q1[q]);
+      const float2 fa = make_float2(f[j].x, f[j].y), fb = make_float2(f[j].z, f[j].w);
+      a0 = dc ? c_mac_dc(a0, fa, p[j]) : c_mac(a0, fa, p[j]);
+      a1 = c_mac(a1, fb, q[j]);
     }
   }
   for (; i < w.i1; ++i) {
-    const float4 g0 = x_unit<SPEC, M>(ch.fdl, fs, u0), g1 = x_unit<SPEC, M>(ch.fdl, fs, u1);
-    float2 pa, qa, pb, qb;
-    const size_t hrow = hb + (size_t)i * U;
-    load_h2<SPEC, M>(ch.H, hrow + u0, pa, qa);
-    load_h2<SPEC, M>(ch.H, hrow + u1, pb, qb);
+    const float4 g = x_unit<SPEC, M>(ch.fdl, fs, u);
+    float2 pa, qa;
+    load_h2<SPEC, M>(ch.H, hb + (size_t)i * U + u, pa, qa);
     if (kScaled<SPEC>) {
       const float s = __ldg(sc + i);
       pa.x *= s; pa.y *= s; qa.x *= s; qa.y *= s;
-      pb.x *= s; pb.y *= s; qb.x *= s; qb.y *= s;
     }
     fs = (fs + 1 == P) ? 0 : fs + 1;
-    const float2 fa = make_float2(g0.x, g0.y), fb = make_float2(g0.z, g0.w);
-    const float2 ga = make_float2(g1.x, g1.y), gb = make_float2(g1.z, g1.w);
-    a0 = dc ? c_mac_dc(a0, fa, pa) : c_mac(a0, fa, pa);
-    a1 = c_mac(a1, fb, qa);
-    b0 = c_mac(b0, ga, pb);
-    b1 = c_mac(b1, gb, qb);
+    a0 = dc ? c_mac_dc(a0, make_float2(g.x, g.y), pa) : c_mac(a0, make_float2(g.x, g.y), pa);
+    a1 = c_mac(a1, make_float2(g.z, g.w), qa);
   }
-  float4* dst = reinterpret_cast<float4*>(part_row(ch, parity, mode, w.row, M));
-  dst[u0] = make_float4(a0.x, a0.y, a1.x, a1.y);
-  dst[u1] = make_float4(b0.x, b0.y, b1.x, b1.y);
+  reinterpret_cast<float4*>(part_row(ch, parity, mode, w.row, M))[u] = make_float4(a0.x, a0.y, a1.x, a1.y);
 }
 
 // ---------------------------------------------------------------------------
