@@ -200,6 +200,13 @@ struct tanb_engine {
   cudaEvent_t ev_out = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_audio = nullptr;  // audio-stream point an IR upload waits for
+  // Pinned staging of the table uploads of session opens and closes: they copy
+  // from here rather than from the live mirrors (which the audio path keeps
+  // advancing), so that an open or a close never waits for the audio stream.
+  char* h_stage = nullptr;
+  size_t stage_cap = 0, stage_used = 0;
+  cudaEvent_t ev_stage = nullptr;   // behind the last staged upload
+  cudaEvent_t ev_upd_done = nullptr;  // update-stream point a close orders the audio stream after
   std::map<int, Session> sessions;
   int next_id = 1;
   // accounting
@@ -271,6 +278,9 @@ void free_engine(tanb_engine* e) {
   cudaFreeHost(e->h_ir);
   cudaFreeHost(e->h_upd);
   cudaFreeHost(e->h_lupd);
+  cudaFreeHost(e->h_stage);
+  if (e->ev_stage) cudaEventDestroy(e->ev_stage);
+  if (e->ev_upd_done) cudaEventDestroy(e->ev_upd_done);
   if (e->ev_out) cudaEventDestroy(e->ev_out);
   if (e->ev_fork) cudaEventDestroy(e->ev_fork);
   if (e->ev_join) cudaEventDestroy(e->ev_join);
@@ -299,6 +309,35 @@ cudaError_t upload_levels(tanb_engine* e, size_t first, size_t n) {
   return cudaMemcpyAsync(e->d_levels + first, e->h_levels + first, n * sizeof(EngLevel), cudaMemcpyHostToDevice,
                          e->stream);
 }
+
+// Staged uploads (see tanb_engine::h_stage): begin_stage waits for the
+// previous staged uploads to have run (long done in practice) and makes room
+// for `bytes`; stage_copy queues one copy on the audio stream; end_stage marks
+// the point the next begin_stage waits for.
+cudaError_t begin_stage(tanb_engine* e, size_t bytes) {
+  cudaError_t r = cudaEventSynchronize(e->ev_stage);
+  if (r != cudaSuccess) return r;
+  if (bytes > e->stage_cap) {
+    cudaFreeHost(e->h_stage);
+    e->h_stage = nullptr;
+    e->stage_cap = 0;
+    if ((r = cudaMallocHost(&e->h_stage, bytes)) != cudaSuccess) return r;
+    e->stage_cap = bytes;
+  }
+  e->stage_used = 0;
+  return cudaSuccess;
+}
+
+cudaError_t stage_copy(tanb_engine* e, void* dev, const void* host, size_t bytes) {
+  if (!bytes) return cudaSuccess;
+  if (e->stage_used + bytes > e->stage_cap) return cudaErrorInvalidValue;
+  char* src = e->h_stage + e->stage_used;
+  std::memcpy(src, host, bytes);
+  e->stage_used += (bytes + 15) & ~size_t(15);
+  return cudaMemcpyAsync(dev, src, bytes, cudaMemcpyHostToDevice, e->stream);
+}
+
+cudaError_t end_stage(tanb_engine* e) { return cudaEventRecord(e->ev_stage, e->stream); }
 
 void update_hwm(tanb_engine* e) {
   e->nslots_hwm = e->slot_alloc.high_water();
@@ -594,7 +633,9 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
       return efail(TANB_OUT_OF_MEMORY, "level table full");
     }
   }
-  ENG_CUDA(cudaStreamSynchronize(e->stream));  // pinned mirrors are rewritten below
+  // the new session's memory is cleared on the audio stream, after every
+  // block already queued there (which may still read a closed session's data
+  // in the same range)
   char* base = e->arena + s.arena_off * kAlign;
   ENG_CUDA(cudaMemsetAsync(base, 0, s.arena_bytes, e->stream));
   const size_t B = e->B;
@@ -683,14 +724,17 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
   }
   if (base != e->arena + s.arena_off * kAlign + s.arena_bytes)
     return efail(TANB_FAIL, "session layout does not match its size (internal error)");
-  for (size_t j = 0; j < nus.size(); ++j)
-    ENG_CUDA(cudaMemcpyAsync(nu_dev[j], &nus[j], sizeof(EngNu), cudaMemcpyHostToDevice, e->stream));
-  for (size_t l = 0; l < s.lv.size(); ++l)
-    ENG_CUDA(upload_levels(e, (size_t)level_class(e, s.lv[l].log2N) * e->max_channels + s.lv_first[l], s.C));
-  ENG_CUDA(upload_chans(e, s.slot0, s.C));
-  ENG_CUDA(upload_items(e, s.item0, nit_total));
-  // the copies read the pinned mirrors (and nus), which change after this
-  ENG_CUDA(cudaStreamSynchronize(e->stream));
+  // table uploads from staging (the mirrors keep changing under the audio path)
+  ENG_CUDA(begin_stage(e, nus.size() * (sizeof(EngNu) + 16) + s.lv.size() * s.C * sizeof(EngLevel) + 16 * s.lv.size() +
+                              s.C * sizeof(EngChan) + nit_total * sizeof(EngItem) + 64));
+  for (size_t j = 0; j < nus.size(); ++j) ENG_CUDA(stage_copy(e, nu_dev[j], &nus[j], sizeof(EngNu)));
+  for (size_t l = 0; l < s.lv.size(); ++l) {
+    const size_t first = (size_t)level_class(e, s.lv[l].log2N) * e->max_channels + s.lv_first[l];
+    ENG_CUDA(stage_copy(e, e->d_levels + first, e->h_levels + first, s.C * sizeof(EngLevel)));
+  }
+  ENG_CUDA(stage_copy(e, e->d_chans + s.slot0, e->h_chans + s.slot0, s.C * sizeof(EngChan)));
+  ENG_CUDA(stage_copy(e, e->d_items + s.item0, e->h_items + s.item0, nit_total * sizeof(EngItem)));
+  ENG_CUDA(end_stage(e));
   ENG_CUDA(cudaEventCreateWithFlags(&s.staged_ev, cudaEventDisableTiming));
   s.staged_mask.assign(s.C, 0);
   s.id = e->next_id++;
@@ -908,6 +952,8 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_audio, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_stage, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_upd_done, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreate(&e->pa);
   if (r == cudaSuccess) r = cudaEventCreate(&e->pb);
   e->d_tw_lv.assign(e->nclass, nullptr);
@@ -1020,24 +1066,31 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   auto it = e->sessions.find(session);
   if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
   ENG_CUDA(cudaSetDevice(e->ctx->device));
-  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
-  ENG_CUDA(cudaStreamSynchronize(e->stream));
+  // No host wait: the audio stream waits for the update stream's work queued
+  // so far (an IR transform may still write this session's memory), and every
+  // later use of the freed memory, slots and table rows (a new session's
+  // clear and uploads) is queued on the audio stream after the blocks that
+  // still read them.
+  ENG_CUDA(cudaEventRecord(e->ev_upd_done, e->upd_stream));
+  ENG_CUDA(cudaStreamWaitEvent(e->stream, e->ev_upd_done, 0));
   const Session s = it->second;
   if (s.staged_ev) cudaEventDestroy(s.staged_ev);
   for (int j = 0; j < s.C; ++j) e->h_chans[s.slot0 + j] = EngChan{};
   const size_t nit_total = (size_t)s.C * s.items_per_chan;
   for (size_t i = 0; i < nit_total; ++i) e->h_items[s.item0 + i] = EngItem{-1, 0, 0, 0, -1, 0};
+  ENG_CUDA(begin_stage(e, s.lv.size() * (s.C * sizeof(EngLevel) + 16) + s.C * sizeof(EngChan) +
+                              nit_total * sizeof(EngItem) + 64));
   for (size_t l = 0; l < s.lv.size(); ++l) {
     const size_t first = (size_t)level_class(e, s.lv[l].log2N) * e->max_channels + s.lv_first[l];
     for (int j = 0; j < s.C; ++j) {
       e->h_levels[first + j] = EngLevel{};
       e->h_levels[first + j].chan = -1;
     }
-    ENG_CUDA(upload_levels(e, first, s.C));
+    ENG_CUDA(stage_copy(e, e->d_levels + first, e->h_levels + first, s.C * sizeof(EngLevel)));
   }
-  ENG_CUDA(upload_chans(e, s.slot0, s.C));
-  ENG_CUDA(upload_items(e, s.item0, nit_total));
-  ENG_CUDA(cudaStreamSynchronize(e->stream));  // the copies read the pinned mirrors
+  ENG_CUDA(stage_copy(e, e->d_chans + s.slot0, e->h_chans + s.slot0, s.C * sizeof(EngChan)));
+  ENG_CUDA(stage_copy(e, e->d_items + s.item0, e->h_items + s.item0, nit_total * sizeof(EngItem)));
+  ENG_CUDA(end_stage(e));
   e->arena_alloc.release(s.arena_off, s.arena_bytes / kAlign);
   e->slot_alloc.release(s.slot0, s.C);
   if (nit_total) e->item_alloc.release(s.item0, nit_total);
