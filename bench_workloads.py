@@ -9,6 +9,7 @@ engine_uneven  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096.
 nonuniform_long  non-uniform partitions, 256 ch, IR 2^20, base block 128, levels up to 16384,
       schedule from the autotuner, one engine session, FP32 / FP16; error vs FP64 on every channel
 serving  the serving loop (Poisson sessions, budget admission, swaps), FP32 / FP24
+nu_block  one fixed non-uniform engine session (64 ch, IR 2^20, levels to 16384), for profiling
 pipeline  the sample pipeline (int16 stereo sources, per-ear convolution, mix,
       int16 out): fused call vs separate GPU calls vs the CPU restatement
 Each prints one JSON object: throughput (GSamples/s), per-block latency
@@ -241,6 +242,37 @@ def nonuniform_long(ctx, quick=False):
     return out
 
 
+def nu_block(ctx, quick=False, C=64, blocks=300):
+    """A fixed non-uniform engine session for profiling: C channels, IR 2^20,
+    base block 128, levels 128x2, 256..8192 x1, 16384x63 (the cfg4 tuner's
+    choice), FP32, device rows, `blocks` blocks, CUDA events per block."""
+    import torch
+
+    g = _rng(3)
+    L, B0 = 1 << 20, 128
+    levels = [(128, 2), (256, 1), (512, 1), (1024, 1), (2048, 1), (4096, 1), (8192, 1), (16384, 63)]
+    e = eng.Engine(ctx, B0, eng.SPECTRUM_FP32, budget_bytes=eng.session_bytes(B0, C, L, levels), max_channels=C)
+    rc, s = e.open_session_nu(C, L, levels)
+    assert rc == 0, cv.last_error()
+    irs = np.stack([_ir(g, L, 8.0) for _ in range(C)])
+    assert s.update_response_td(irs, block_until_ready=True) == 0
+    x = torch.from_numpy(g.uniform(-1, 1, (C, blocks * B0)).astype(np.float32)).cuda()
+    y = torch.zeros_like(x)
+    st = torch.cuda.ExternalStream(e.stream())
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(blocks)]
+    for k in range(blocks):
+        ev[k][0].record(st)
+        assert e.process_device(x.data_ptr() + k * B0 * 4, y.data_ptr() + k * B0 * 4, blocks * B0) == 0
+        ev[k][1].record(st)
+    e.synchronize()
+    ms = np.array([a.elapsed_time(b) for a, b in ev])[128:]
+    info = e.info()
+    e.release()
+    return {"config": "nu_block", "channels": C, "levels": levels, "blocks": blocks,
+            "device_ms": {"mean": float(ms.mean()), "p99": float(np.percentile(ms, 99)), "max": float(ms.max())},
+            "avg_block_bytes": info["block_bytes"]}
+
+
 def serving_cfg5(ctx, seconds=10.0, quick=False):
     """cfg5: the serving loop at 48 kHz, block 256 (5.33 ms deadline), Poisson
     arrivals 20/s, exponential lifetimes (mean 30 s), 1-8 channels, IR lengths
@@ -344,7 +376,7 @@ def pipeline(ctx, quick=False, S=32, B=256, L=48000):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("which", choices=["dropin_small", "engine_uneven", "nonuniform_long", "nu-tune", "pipeline",
-                                      "serving"])
+                                      "serving", "nu_block"])
     ap.add_argument("--quick", action="store_true")
     a = ap.parse_args()
     ctx = cv.TANContext(0)
@@ -352,7 +384,8 @@ def main():
         r = autotune.tune_nu_engine(ctx, 64 if a.quick else 256, 1 << 20, 128)
     else:
         r = {"dropin_small": dropin_small, "engine_uneven": engine_uneven, "nonuniform_long": nonuniform_long,
-             "pipeline": pipeline, "serving": lambda c, q: serving_cfg5(c, quick=q)}[a.which](ctx, a.quick)
+             "pipeline": pipeline, "serving": lambda c, q: serving_cfg5(c, quick=q),
+             "nu_block": nu_block}[a.which](ctx, a.quick)
     print(json.dumps(r))
 
 

@@ -292,12 +292,6 @@ void free_engine(tanb_engine* e) {
   if (e->stream) cudaStreamDestroy(e->stream);
 }
 
-cudaError_t upload_chans(tanb_engine* e, size_t first, size_t n) {
-  if (!n) return cudaSuccess;
-  return cudaMemcpyAsync(e->d_chans + first, e->h_chans + first, n * sizeof(EngChan), cudaMemcpyHostToDevice,
-                         e->stream);
-}
-
 cudaError_t upload_items(tanb_engine* e, size_t first, size_t n) {
   if (!n) return cudaSuccess;
   return cudaMemcpyAsync(e->d_items + first, e->h_items + first, n * sizeof(EngItem), cudaMemcpyHostToDevice,

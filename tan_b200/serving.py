@@ -31,21 +31,24 @@ FS = 48000
 
 
 class IRPool:
-    """Pre-generated exp-decayed Gaussian noise IRs (unit L2 norm per prefix use)."""
+    """Pre-generated exp-decayed Gaussian noise IRs (unit L2 norm per prefix use).
+    The running sums of squares are kept, so a prefix's norm costs nothing and
+    a request is one scaled copy per channel."""
 
     def __init__(self, g, n=8, length=524288, rt60=(0.2, 3.0)):
         t = np.arange(length, dtype=np.float64)
-        self.irs = []
+        self.irs, self.energy = [], []
         for _ in range(n):
             r = g.uniform(*rt60)
             h = g.standard_normal(length) * np.exp(-np.log(1000.0) * t / (r * FS))
             self.irs.append(h.astype(np.float32))
+            self.energy.append(np.cumsum(h * h))
 
     def get(self, g, C, L):
         out = np.empty((C, L), np.float32)
         for c in range(C):
-            h = self.irs[int(g.integers(len(self.irs)))][:L]
-            out[c] = h / np.float32(np.linalg.norm(h))
+            i = int(g.integers(len(self.irs)))
+            np.multiply(self.irs[i][:L], np.float32(1.0 / np.sqrt(self.energy[i][L - 1])), out=out[c])
         return out
 
 
@@ -74,8 +77,14 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
     swap IRs and output rows are returned under "traces", so that a caller can
     check each against the same session run alone."""
     import queue
+    import sys
     import threading
 
+    # the audio loop and the control thread share the interpreter: hand it
+    # over often, so that the control thread's work delays a block by well
+    # under a millisecond rather than by the default 5 ms switch interval
+    old_switch = sys.getswitchinterval()
+    sys.setswitchinterval(2e-4)
     g = np.random.Generator(np.random.PCG64(seed))
     gw = np.random.Generator(np.random.PCG64(seed + 1))  # the control thread's own stream
     pool = IRPool(g, length=len_range[1])
@@ -165,6 +174,7 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
         t += dt
     work.put(None)
     ctl.join()
+    sys.setswitchinterval(old_switch)
     e.synchronize()
     info = e.info()
     e.release()
