@@ -338,16 +338,42 @@ def size_floor(torch, stream, flush_l2, nbytes, dev, reps=50):
         rc = lib.tanb_stream_read(buf.data_ptr(), nbytes, acc.data_ptr(), cps, thr, stream.cuda_stream)
         assert rc == 0, cv.last_error()
 
-    grids = {f"{cps} CTAs/SM x {thr}": timed(lambda: own(cps, thr))
-             for cps, thr in ((1, 1024), (2, 1024), (2, 512), (4, 512), (4, 256), (8, 256))}
+    shapes = ((1, 1024), (2, 1024), (2, 512), (4, 512), (4, 256), (8, 256))
+    grids = {f"{cps} CTAs/SM x {thr}": timed(lambda: own(cps, thr)) for cps, thr in shapes}
     best = min(grids, key=grids.get)
+    cps, thr = shapes[list(grids).index(best)]
     torch_us = timed(lambda: torch.sum(buf, 0, out=out))
-    del buf
     us = grids[best]
+    # the same launch over 16 bytes and over 1/4 and 1/2 of the bytes: a line
+    # through the sizes separates the fixed cost of one launch timed this way
+    # from the rate at which its bytes stream
+    empty_us = timed(lambda: lib.tanb_stream_read(buf.data_ptr(), 16, acc.data_ptr(), cps, thr, stream.cuda_stream))
+    sizes = [nbytes // 4 // 16 * 16, nbytes // 2 // 16 * 16, nbytes]
+    ts = []
+    for nb in sizes:
+        ts.append(timed(lambda: lib.tanb_stream_read(buf.data_ptr(), nb, acc.data_ptr(), cps, thr,
+                                                     stream.cuda_stream)))
+    slope, fixed = np.polyfit(np.array(sizes, float), np.array(ts), 1)
+    del buf
     return {"bytes": nbytes, "us": us, "gbs": nbytes / (us * 1e-6) / 1e9, "grid": best,
             "what": "tanb_stream_read (the library's 16-byte streaming read) over the same bytes, best grid, "
                     "one launch, L2 flushed, CUDA events (median)",
-            "grids_us": grids, "torch_sum_us": torch_us, "torch_sum_gbs": nbytes / (torch_us * 1e-6) / 1e9}
+            "grids_us": grids, "torch_sum_us": torch_us, "torch_sum_gbs": nbytes / (torch_us * 1e-6) / 1e9,
+            "empty_launch_us": empty_us,
+            "fit": {"sizes": sizes, "us": ts, "fixed_us": float(fixed), "marginal_gbs": float(1e-3 / slope),
+                    "what": "least-squares line through the streaming read at 1/4, 1/2 and all of the bytes"}}
+
+
+def marginal(nbytes, us, floor, peak):
+    """The launch's bytes over its time less the fixed cost of one launch timed
+    the same way (the streaming read's fitted line): the rate at which the
+    kernel streams once running. A derived figure beside `frac`, not instead."""
+    fixed = floor["fit"]["fixed_us"]
+    if us <= fixed:
+        return None
+    gbs = nbytes / ((us - fixed) * 1e-6) / 1e9
+    return {"fixed_us": fixed, "gbs": gbs, "frac": gbs / peak,
+            "what": "bytes_per_launch / (avg_launch_us - size_floor.fit.fixed_us)"}
 
 
 def hbm_peak():
@@ -663,7 +689,8 @@ def run_ours(args):
                          "bytes_per_launch": bytes_per_tail, "avg_launch_us": tail_ms_avg * 1e3,
                          "launches_timed": tail["timed"], "tiling": list(tiling),
                          "size_floor": dict(floor, frac_of_peak=floor["gbs"] / peak,
-                                            tail_vs_floor=achieved / floor["gbs"])},
+                                            tail_vs_floor=achieved / floor["gbs"]),
+                         "marginal": marginal(bytes_per_tail, tail_ms_avg * 1e3, floor, peak)},
             "kernel_ms": {k: v["ms"] for k, v in prof.items()},
             "e2e": {"value": e2e_value, "unit": "GSamples/s", "h2d_bytes_per_step": C * B * 4 + 32 * C,
                     "d2h_bytes_per_step": C * B * 4,

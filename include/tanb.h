@@ -258,6 +258,13 @@ int32_t tanb_convolution_profile(tanb_convolution* conv, int32_t enable);
  * summed device milliseconds. Waits for the timed launches to finish. */
 int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6], double ms[3]);
 
+/* No reference counterpart: host microseconds of the last Process call of the
+ * uniformly partitioned methods, by part -- us[0] staging the rows and
+ * descriptors, us[1] launching the kernels, us[2] waiting for the heads'
+ * completion signal (host outputs only), us[3] copying the outputs to the
+ * caller's rows, us[4] the whole call. */
+int32_t tanb_convolution_call_times(tanb_convolution* conv, double us[5]);
+
 /* No reference counterpart; a test hook for failure handling. Sets how many
  * times the tail kernel's cp.async.bulk pipelines poll a stage's barrier
  * before giving up (default and maximum 2^20; negative: the default). On a
@@ -378,6 +385,15 @@ int32_t tanb_engine_session_state(tanb_engine* engine, int32_t session, int64_t 
  * with profiling enabled), ms[1] 0. Reading resets. */
 int32_t tanb_engine_profile(tanb_engine* engine, int32_t enable);
 int32_t tanb_engine_profile_read(tanb_engine* engine, int64_t counts[4], double ms[2]);
+
+/* Host-side microseconds of the last tanb_engine_process: us[0] waiting for
+ * the engine's lock, us[1] committing staged IR updates, us[2] capturing and
+ * instantiating block graphs (0 unless the session tables' shape changed),
+ * us[3] launching the block graph, us[4] waiting for the block's outputs,
+ * us[5] the whole call; us[6] the longest call since the previous read, us[7]
+ * block graphs built since the engine was created. No reference counterpart:
+ * serving diagnostics for the real-time block deadline. */
+int32_t tanb_engine_block_times(tanb_engine* engine, double us[8]);
 
 /* ---------------------------------------------------------------------------
  * TANConverter (TrueAudioNext.h:344-398; TANCreateConverter :653-656) and

@@ -111,6 +111,8 @@ SIGNATURES = {
     "tanb_engine_session_state": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_int64)]),
     "tanb_engine_profile": (_i32, [_vp, _i32]),
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
+    "tanb_engine_block_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "tanb_convolution_call_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "tanb_convolution_process_mix_pcm16": (_i32, [_vp, _pp, _sz, ctypes.c_float, _u32p, _u32, _pp, _sz,
                                                   ctypes.c_float, _sz, ctypes.POINTER(ctypes.c_int32), _szp]),
     "tanb_room_generator_create": (_i32, [_vp, _i32, ctypes.POINTER(_vp)]),
@@ -386,6 +388,12 @@ class TANConvolution:
         out = (ctypes.c_int32 * 3)()
         rc = lib().tanb_convolution_tiling(self._h, index, out)
         return rc, tuple(out)
+
+    def call_times(self) -> dict:
+        """Host microseconds of the last Process call, by part."""
+        us = (ctypes.c_double * 5)()
+        lib().tanb_convolution_call_times(self._h, us)
+        return dict(zip(("stage_us", "launch_us", "wait_us", "copy_us", "total_us"), list(us)))
 
     def profile(self, enable: bool) -> int:
         return lib().tanb_convolution_profile(self._h, 1 if enable else 0)

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -87,6 +88,8 @@ enum class Mem { Host, Device };
 struct tanb_convolution {
   tanb_context* ctx = nullptr;
   std::mutex mu;
+  // host microseconds of the last uniform Process call (tanb_convolution_call_times)
+  double ct[5] = {0, 0, 0, 0, 0};
   bool initialized = false;
   bool terminated = false;
   bool finalize_mode = false;
@@ -612,7 +615,14 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   // and its scratch outputs): two base pointers describe every channel
   const bool staged = param && (pcm || (in_mem == Mem::Host && out_mem == Mem::Host));
   const bool host_out = out_mem == Mem::Host;  // outputs are read back from host staging
+  using Clock = std::chrono::steady_clock;
+  auto us = [](Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::micro>(b - a).count();
+  };
+  const Clock::time_point t_call = Clock::now();
+  double t_stage = 0, t_launch = 0, t_wait = 0, t_copy = 0;
   while (processed < nblocks && status == TANB_OK) {
+    const Clock::time_point t0 = Clock::now();
     int nb = (int)std::min<size_t>(kMaxBlocksPerChunk, nblocks - processed);
     TANB_CUDA(cudaEventSynchronize(v->ev_stage));
     if (v->staging_busy) {
@@ -692,6 +702,8 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     nb = filled;
     if (nb == 0) break;
     tanb::copy_for_device_fence();  // staged rows are visible before the launches
+    const Clock::time_point t1 = Clock::now();
+    t_stage += us(t0, t1);
     // ev_stage guards the host descriptor tables until their upload has run;
     // ev_out guards the host staging rows until the heads have read and
     // written them. A call on device rows with parameter descriptors uses
@@ -744,10 +756,14 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
       TANB_CUDA(cudaEventRecord(v->ev_out, v->stream));
       v->staging_busy = true;
     }
+    const Clock::time_point t2 = Clock::now();
+    t_launch += us(t1, t2);
     if (host_out) {
       // the outputs are final once the last head has signalled; the tail
       // launched behind it keeps running while they are scattered
       if (wait_heads(v, v->head_seq) != TANB_OK) return TANB_FAIL;
+      const Clock::time_point t3 = Clock::now();
+      t_wait += us(t2, t3);
       v->staging_busy = false;
       if (*v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
       if (pcm) {
@@ -764,6 +780,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
             if (run_b[b][c] && out[c])
               std::memcpy(out[c] + (processed + b) * B, v->h_out + ((size_t)b * C + c) * B, B * sizeof(float));
       }
+      t_copy += us(t3, Clock::now());
     }
     processed += nb;
     v->blocks += nb;
@@ -772,6 +789,11 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
     }
   }
   if (done) *done = processed * B;
+  v->ct[0] = t_stage;
+  v->ct[1] = t_launch;
+  v->ct[2] = t_wait;
+  v->ct[3] = t_copy;
+  v->ct[4] = us(t_call, Clock::now());
   return status;
 }
 
@@ -1500,6 +1522,13 @@ int32_t tanb_convolution_profile_read(tanb_convolution* v, int64_t counts[6], do
     v->timed_count[k] = 0;
     v->ms[k] = 0.0;
   }
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_call_times(tanb_convolution* v, double us[5]) {
+  if (!v || !us) return fail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(v->mu);
+  for (int k = 0; k < 5; ++k) us[k] = v->ct[k];
   return TANB_OK;
 }
 

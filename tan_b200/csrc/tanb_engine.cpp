@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -194,9 +195,15 @@ struct tanb_engine {
   int tail_grid = 0;
   size_t nslots_hwm = 0, nitems_hwm = 0;
   // graphs of the host-buffer block, one per set of due level size classes,
-  // valid for the high-water marks in graph_key
-  std::map<unsigned, cudaGraphExec_t> graphs;
-  std::vector<size_t> graph_key;
+  // each valid for the high-water marks in its key; executable graphs
+  // replaced on the audio path are retired, not destroyed, there (destroying
+  // one can wait for the device) and destroyed by synchronize and release
+  struct BlockGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<size_t> key;
+  };
+  std::map<unsigned, BlockGraph> graphs;
+  std::vector<cudaGraphExec_t> retired;
   cudaEvent_t ev_out = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_audio = nullptr;  // audio-stream point an IR upload waits for
@@ -214,9 +221,17 @@ struct tanb_engine {
   cudaEvent_t pa = nullptr, pb = nullptr;
   double ms_block = 0;
   int64_t n_block = 0, n_commit = 0, n_ir = 0, n_timed = 0;
+  // host microseconds of the last tanb_engine_process (tanb_engine_block_times)
+  double bt_lock = 0, bt_commit = 0, bt_build = 0, bt_launch = 0, bt_wait = 0, bt_total = 0, bt_max = 0;
+  int64_t n_graph_builds = 0;
 };
 
 namespace {
+
+using Clock = std::chrono::steady_clock;
+double us_since(Clock::time_point t0) {
+  return std::chrono::duration<double, std::micro>(Clock::now() - t0).count();
+}
 
 // Bytes per packed bin of an IR-spectrum row and of a delay-line row.
 size_t spec_bytes(int spec) { return spec == tanb::kSpecFP32 ? 8 : spec == tanb::kSpecFP24 ? 6 : 4; }
@@ -246,10 +261,17 @@ size_t chan_bytes(const tanb_engine* e, int P, int nitem, const std::vector<Leve
 
 int level_class(const tanb_engine* e, int log2N) { return log2N - e->log2B - 1; }
 
+constexpr size_t kMaxRetiredGraphs = 64;
+
+void destroy_retired(tanb_engine* e) {
+  for (cudaGraphExec_t g : e->retired) cudaGraphExecDestroy(g);
+  e->retired.clear();
+}
+
 void destroy_graphs(tanb_engine* e) {
-  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
   e->graphs.clear();
-  e->graph_key.clear();
+  destroy_retired(e);
 }
 
 void free_engine(tanb_engine* e) {
@@ -447,19 +469,19 @@ std::vector<size_t> graph_key(const tanb_engine* e) {
   return k;
 }
 
+// The block graph for `due`, captured anew when the high-water marks changed
+// since it was built: the cached executable is updated in place when the new
+// capture has its topology (grid sizes and parameters differ), else a new one
+// is instantiated and the old one retired.
 cudaError_t ensure_graph(tanb_engine* e, unsigned due, cudaGraphExec_t* out) {
   const std::vector<size_t> key = graph_key(e);
-  if (key != e->graph_key) {
-    destroy_graphs(e);
-    e->graph_key = key;
-  }
   auto it = e->graphs.find(due);
-  if (it != e->graphs.end()) {
-    *out = it->second;
+  if (it != e->graphs.end() && it->second.key == key) {
+    *out = it->second.exec;
     return cudaSuccess;
   }
+  const Clock::time_point t0 = Clock::now();
   cudaGraph_t g = nullptr;
-  cudaGraphExec_t ge = nullptr;
   cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
   if (r != cudaSuccess) return r;
   tanb::EngRows rows;
@@ -476,11 +498,29 @@ cudaError_t ensure_graph(tanb_engine* e, unsigned due, cudaGraphExec_t* out) {
     return r2;
   }
   if (r != cudaSuccess) return r;
+  if (it != e->graphs.end()) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(it->second.exec, g, &info) == cudaSuccess) {
+      cudaGraphDestroy(g);
+      it->second.key = key;
+      *out = it->second.exec;
+      e->n_graph_builds += 1;
+      e->bt_build += us_since(t0);
+      return cudaSuccess;
+    }
+    (void)cudaGetLastError();  // a refused update leaves the executable as it was
+    if (e->retired.size() >= kMaxRetiredGraphs) destroy_retired(e);
+    e->retired.push_back(it->second.exec);
+    e->graphs.erase(it);
+  }
+  cudaGraphExec_t ge = nullptr;
   r = cudaGraphInstantiate(&ge, g, 0);
   cudaGraphDestroy(g);
   if (r != cudaSuccess) return r;
-  e->graphs[due] = ge;
+  e->graphs[due] = tanb_engine::BlockGraph{ge, key};
   *out = ge;
+  e->n_graph_builds += 1;
+  e->bt_build += us_since(t0);
   return cudaSuccess;
 }
 
@@ -834,12 +874,17 @@ int32_t engine_update(tanb_engine* e, int32_t session, const float* const* ir, s
 // One block: commit staged updates, then the block (a graph for the host
 // buffers, direct launches for other rows). Caller holds mu.
 int32_t run_block(tanb_engine* e, const tanb::EngRows* rows) {
+  Clock::time_point t0 = Clock::now();
   ENG_CUDA(commit_updates(e));
+  e->bt_commit = us_since(t0);
   const unsigned due = due_mask(e, e->k_host);
   if (!rows) {
     cudaGraphExec_t ge = nullptr;
+    e->bt_build = 0;
     ENG_CUDA(ensure_graph(e, due, &ge));
+    t0 = Clock::now();
     ENG_CUDA(cudaGraphLaunch(ge, e->stream));
+    e->bt_launch = us_since(t0);
   } else {
     if (e->profiling) ENG_CUDA(cudaEventRecord(e->pa, e->stream));
     ENG_CUDA(enqueue_block(e, *rows, due));
@@ -922,9 +967,13 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   e->nclass = tanb::kMaxLog2Level - e->log2B;
   cudaError_t r = cudaSetDevice(ctx->device);
   if (r == cudaSuccess) r = tanb::eng_prepare();
-  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
-  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->lstream, cudaStreamNonBlocking);
-  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&e->upd_stream, cudaStreamNonBlocking);
+  // the audio streams at the device's highest priority, IR uploads at its
+  // lowest: when both have CTAs waiting for an SM, the block's go first
+  int prio_low = 0, prio_high = 0;
+  if (r == cudaSuccess) r = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  if (r == cudaSuccess) r = cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, prio_high);
+  if (r == cudaSuccess) r = cudaStreamCreateWithPriority(&e->lstream, cudaStreamNonBlocking, prio_high);
+  if (r == cudaSuccess) r = cudaStreamCreateWithPriority(&e->upd_stream, cudaStreamNonBlocking, prio_low);
   const size_t io = e->max_channels * e->B;
   const size_t nlev = (size_t)e->nclass * e->max_channels;
   if (r == cudaSuccess) r = cudaMalloc(&e->arena, std::max<size_t>(budget_bytes, kAlign));
@@ -1135,12 +1184,19 @@ int32_t tanb_engine_write_input(tanb_engine* e, uint32_t first_slot, const float
 
 int32_t tanb_engine_process(tanb_engine* e) {
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
+  const Clock::time_point t_call = Clock::now();
   std::lock_guard<std::mutex> lock(e->mu);
+  const Clock::time_point t_locked = Clock::now();
   ENG_CUDA(cudaSetDevice(e->ctx->device));
   if (e->sessions.empty()) return efail(TANB_WRONG_STATE, "no open sessions");
   const int32_t r = run_block(e, nullptr);
   if (r != TANB_OK) return r;
+  const Clock::time_point tw = Clock::now();
   ENG_CUDA(cudaEventSynchronize(e->ev_out));
+  e->bt_wait = us_since(tw);
+  e->bt_lock = std::chrono::duration<double, std::micro>(t_locked - t_call).count();
+  e->bt_total = us_since(t_call);
+  e->bt_max = std::max(e->bt_max, e->bt_total);
   return TANB_OK;
 }
 
@@ -1163,6 +1219,7 @@ int32_t tanb_engine_synchronize(tanb_engine* e) {
   ENG_CUDA(cudaSetDevice(e->ctx->device));
   ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
   ENG_CUDA(cudaStreamSynchronize(e->stream));
+  destroy_retired(e);
   return TANB_OK;
 }
 
@@ -1225,6 +1282,21 @@ int32_t tanb_engine_profile(tanb_engine* e, int32_t enable) {
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   std::lock_guard<std::mutex> lock(e->mu);
   e->profiling = enable != 0;
+  return TANB_OK;
+}
+
+int32_t tanb_engine_block_times(tanb_engine* e, double us[8]) {
+  if (!e || !us) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(e->mu);
+  us[0] = e->bt_lock;
+  us[1] = e->bt_commit;
+  us[2] = e->bt_build;
+  us[3] = e->bt_launch;
+  us[4] = e->bt_wait;
+  us[5] = e->bt_total;
+  us[6] = e->bt_max;
+  us[7] = (double)e->n_graph_builds;
+  e->bt_max = 0;
   return TANB_OK;
 }
 

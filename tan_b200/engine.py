@@ -148,6 +148,15 @@ class Engine:
                 "tail_grid")
         return dict(zip(keys, list(out)))
 
+    def block_times(self) -> dict:
+        """Host microseconds of the last process() call, by part; max_us is
+        the longest call since the previous read."""
+        us = (ctypes.c_double * 8)()
+        lib().tanb_engine_block_times(self._h, us)
+        keys = ("lock_us", "commit_us", "graph_build_us", "launch_us", "wait_us", "total_us", "max_us",
+                "graph_builds")
+        return dict(zip(keys, list(us)))
+
     def profile(self, enable: bool) -> int:
         return lib().tanb_engine_profile(self._h, 1 if enable else 0)
 

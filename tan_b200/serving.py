@@ -111,6 +111,8 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
                     errors.append((kind, rc, cv.last_error()))
             except Exception as ex:  # noqa: BLE001
                 errors.append((kind, -1, repr(ex)))
+            finally:
+                work.task_done()
 
     ctl = threading.Thread(target=control, daemon=True)
     ctl.start()
@@ -144,8 +146,11 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
     if prefill:  # start in steady state: rate x lifetime sessions already running
         for _ in range(int(rate * lifetime)):
             new_session(0.0)
-        while not work.empty():
-            time.sleep(0.01)
+        work.join()
+        # the prefilled sessions' IRs all take effect on the next block: run
+        # it before the loop, which then starts in steady state
+        assert e.synchronize() == cv.AMF_OK
+        assert e.process() == cv.AMF_OK, cv.last_error()
     for k in range(nblocks):
         k_now = k
         t0 = time.perf_counter()
@@ -174,6 +179,7 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
         t += dt
     work.put(None)
     ctl.join()
+    times = e.block_times()
     sys.setswitchinterval(old_switch)
     e.synchronize()
     info = e.info()
@@ -183,6 +189,7 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
            "deadline_misses": int((lat > deadline_ms).sum()), "concurrent_channels_mean": float(np.mean(chans)),
            "concurrent_channels_max": int(np.max(chans)), "admitted": admitted, "refused": refused,
            "control_errors": errors[:5], "arena_bytes_end": info["arena_bytes"],
+           "block_graphs_built": int(times["graph_builds"]),
            "spectrum": ["fp32", "fp16", "bf16", "fp24"][spectrum]}
     if trace:
         out["traces"] = [dict(tr, y=np.concatenate(tr["y"], axis=1)) for tr in traces.values()]
