@@ -315,7 +315,8 @@ def size_floor(torch, stream, flush_l2, nbytes, dev, reps=50):
 
     lib = cv.lib()
     nbytes = nbytes // 16 * 16
-    buf = torch.ones(nbytes // 4, dtype=torch.float32, device=f"cuda:{dev}")
+    # 4x the bytes: the same read at 1x, 2x and 4x its size gives the line below
+    buf = torch.ones(4 * nbytes // 4, dtype=torch.float32, device=f"cuda:{dev}")
     acc = torch.zeros(1, dtype=torch.float32, device=f"cuda:{dev}")
     out = torch.empty((), dtype=torch.float32, device=f"cuda:{dev}")
 
@@ -342,26 +343,27 @@ def size_floor(torch, stream, flush_l2, nbytes, dev, reps=50):
     grids = {f"{cps} CTAs/SM x {thr}": timed(lambda: own(cps, thr)) for cps, thr in shapes}
     best = min(grids, key=grids.get)
     cps, thr = shapes[list(grids).index(best)]
-    torch_us = timed(lambda: torch.sum(buf, 0, out=out))
+    head = buf[:nbytes // 4]
+    torch_us = timed(lambda: torch.sum(head, 0, out=out))
     us = grids[best]
-    # the same launch over 16 bytes and over 1/4 and 1/2 of the bytes: a line
+    # the same launch over 16 bytes and over 1x, 2x and 4x the bytes: a line
     # through the sizes separates the fixed cost of one launch timed this way
     # from the rate at which its bytes stream
     empty_us = timed(lambda: lib.tanb_stream_read(buf.data_ptr(), 16, acc.data_ptr(), cps, thr, stream.cuda_stream))
-    sizes = [nbytes // 4 // 16 * 16, nbytes // 2 // 16 * 16, nbytes]
+    sizes = [nbytes, 2 * nbytes, 4 * nbytes]
     ts = []
     for nb in sizes:
         ts.append(timed(lambda: lib.tanb_stream_read(buf.data_ptr(), nb, acc.data_ptr(), cps, thr,
                                                      stream.cuda_stream)))
     slope, fixed = np.polyfit(np.array(sizes, float), np.array(ts), 1)
-    del buf
+    del buf, head
     return {"bytes": nbytes, "us": us, "gbs": nbytes / (us * 1e-6) / 1e9, "grid": best,
             "what": "tanb_stream_read (the library's 16-byte streaming read) over the same bytes, best grid, "
                     "one launch, L2 flushed, CUDA events (median)",
             "grids_us": grids, "torch_sum_us": torch_us, "torch_sum_gbs": nbytes / (torch_us * 1e-6) / 1e9,
             "empty_launch_us": empty_us,
             "fit": {"sizes": sizes, "us": ts, "fixed_us": float(fixed), "marginal_gbs": float(1e-3 / slope),
-                    "what": "least-squares line through the streaming read at 1/4, 1/2 and all of the bytes"}}
+                    "what": "least-squares line through the streaming read of 1x, 2x and 4x the bytes"}}
 
 
 def marginal(nbytes, us, floor, peak):
@@ -567,12 +569,17 @@ def run_ours(args):
     conv = autotune.tuned(ctx, cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C)
     stream = torch.cuda.ExternalStream(conv.stream(), device=dev)
     lib = cv.lib()
-    y = np.zeros((C, B), np.float32)
-    xs_blocks = [np.ascontiguousarray(x[:, j * B:(j + 1) * B]) for j in range(xblocks)]
+    # the caller's audio buffers in page-locked host memory, as an audio
+    # host keeps the buffers it hands a GPU: input blocks, output block, IRs
+    pin_x = torch.from_numpy(np.ascontiguousarray(x.reshape(C, xblocks, B).transpose(1, 0, 2))).pin_memory()
+    pin_y = torch.zeros((C, B), dtype=torch.float32).pin_memory()
+    pin_ir = [torch.from_numpy(h).pin_memory() for h in irs]
+    xs_blocks = [pin_x[j].numpy() for j in range(xblocks)]
+    y = pin_y.numpy()
     # host row-pointer arrays built once, as a C caller would keep them
     in_rows = [(ctypes.c_void_p * C)(*[xb[c].ctypes.data for c in range(C)]) for xb in xs_blocks]
     out_rows = (ctypes.c_void_p * C)(*[y[c].ctypes.data for c in range(C)])
-    ir_rows = [(ctypes.c_void_p * C)(*[h[c].ctypes.data for c in range(C)]) for h in irs]
+    ir_rows = [(ctypes.c_void_p * C)(*[h.numpy()[c].ctypes.data for c in range(C)]) for h in pin_ir]
     done = ctypes.c_size_t(0)
 
     def host_step(k):
@@ -603,6 +610,7 @@ def run_ours(args):
     e2e_value = world * C * B * args.steps / e2e_s / 1e9
     lat_ms = np.array(lat) * 1e3
     p99 = float(max_over_ranks(pg, float(np.percentile(lat_ms, 99)), local))
+    e2e_in_place = conv.call_times()["in_place"]
     conv.Release()
 
     capacity = roofline_serving = None
@@ -692,11 +700,14 @@ def run_ours(args):
                                             tail_vs_floor=achieved / floor["gbs"]),
                          "marginal": marginal(bytes_per_tail, tail_ms_avg * 1e3, floor, peak)},
             "kernel_ms": {k: v["ms"] for k, v in prof.items()},
-            "e2e": {"value": e2e_value, "unit": "GSamples/s", "h2d_bytes_per_step": C * B * 4 + 32 * C,
+            "e2e": {"value": e2e_value, "unit": "GSamples/s", "h2d_bytes_per_step": C * B * 4,
                     "d2h_bytes_per_step": C * B * 4,
                     "ir_h2d_bytes_per_swap": C * L * 4,
-                    "what": "tanb_convolution_process with host rows + UpdateResponseTD every 32 blocks; "
-                            "wall clock per block including the tail kernel"},
+                    "rows_in_place": e2e_in_place,
+                    "what": "tanb_convolution_process with host rows in page-locked memory (read and written "
+                            "by the head over the bus: rows_in_place 3 = inputs and outputs) + "
+                            "UpdateResponseTD from page-locked IR rows at the timed swap steps; wall clock "
+                            "per block including the tail kernel"},
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }

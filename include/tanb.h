@@ -262,8 +262,10 @@ int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6],
  * uniformly partitioned methods, by part -- us[0] staging the rows and
  * descriptors, us[1] launching the kernels, us[2] waiting for the heads'
  * completion signal (host outputs only), us[3] copying the outputs to the
- * caller's rows, us[4] the whole call. */
-int32_t tanb_convolution_call_times(tanb_convolution* conv, double us[5]);
+ * caller's rows, us[4] the whole call -- and us[5] which caller rows the
+ * kernels read or wrote in place (1: inputs, 2: outputs; host rows that sit
+ * at one stride in one page-locked allocation are not staged). */
+int32_t tanb_convolution_call_times(tanb_convolution* conv, double us[6]);
 
 /* No reference counterpart; a test hook for failure handling. Sets how many
  * times the tail kernel's cp.async.bulk pipelines poll a stage's barrier

@@ -391,9 +391,11 @@ class TANConvolution:
 
     def call_times(self) -> dict:
         """Host microseconds of the last Process call, by part."""
-        us = (ctypes.c_double * 5)()
+        us = (ctypes.c_double * 6)()
         lib().tanb_convolution_call_times(self._h, us)
-        return dict(zip(("stage_us", "launch_us", "wait_us", "copy_us", "total_us"), list(us)))
+        out = dict(zip(("stage_us", "launch_us", "wait_us", "copy_us", "total_us"), list(us)))
+        out["in_place"] = int(us[5])  # 1: caller's input rows, 2: output rows (pinned, strided)
+        return out
 
     def profile(self, enable: bool) -> int:
         return lib().tanb_convolution_profile(self._h, 1 if enable else 0)

@@ -14,6 +14,7 @@
 //      dependent launch, so the two overlap), and waits for the last of them.
 // UpdateResponseTD transforms the new IR into the idle slot and precomputes
 // that IR's tail, so the swap block costs the same device time as any other.
+#include <cuda.h>  // CUpointer_attribute values only; the driver call is resolved at run time
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -88,8 +89,9 @@ enum class Mem { Host, Device };
 struct tanb_convolution {
   tanb_context* ctx = nullptr;
   std::mutex mu;
-  // host microseconds of the last uniform Process call (tanb_convolution_call_times)
-  double ct[5] = {0, 0, 0, 0, 0};
+  // host microseconds of the last uniform Process call by part, and which of
+  // its caller rows the kernels addressed in place (tanb_convolution_call_times)
+  double ct[6] = {0, 0, 0, 0, 0, 0};
   bool initialized = false;
   bool terminated = false;
   bool finalize_mode = false;
@@ -363,6 +365,95 @@ int32_t nu_update(tanb_convolution* v, Mem mem, const float* const* ir, size_t n
 int32_t nu_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
                    size_t n, const uint32_t* flags, size_t* done);
 
+// ---------------------------------------------------------------------------
+// Caller rows in page-locked host memory. When every row of a call sits at one
+// stride inside one pinned allocation that the device addresses at the same
+// virtual addresses, the head reads (and writes) the rows in place over the
+// bus instead of through the object's staging: no host copy in, none out.
+// Anything else -- pageable rows, rows spread over several allocations,
+// unequal strides, misalignment, input and output spans that overlap -- takes
+// the staging path.
+// ---------------------------------------------------------------------------
+using PtrAttrFn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+
+PtrAttrFn ptr_attr_fn() {
+  static const PtrAttrFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      (void)cudaGetLastError();
+      return static_cast<PtrAttrFn>(nullptr);
+    }
+    return reinterpret_cast<PtrAttrFn>(f);
+  }();
+  return fn;
+}
+
+bool host_mapped_same(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost && a.devicePointer == p;
+}
+
+// True when the bytes [lo, hi) lie in one pinned host allocation mapped at
+// the same addresses on the device.
+bool pinned_span(const void* lo, const void* hi) {
+  const PtrAttrFn fn = ptr_attr_fn();
+  if (!fn || hi <= lo) return false;
+  if (!host_mapped_same(lo)) return false;
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  const CUdeviceptr l = (CUdeviceptr) reinterpret_cast<uintptr_t>(lo);
+  if (fn(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, l) != CUDA_SUCCESS) return false;
+  if (fn(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, l) != CUDA_SUCCESS) return false;
+  const CUdeviceptr h = (CUdeviceptr) reinterpret_cast<uintptr_t>(hi);
+  if (l < start || h > start + size) return false;
+  return host_mapped_same(static_cast<const char*>(hi) - 1);
+}
+
+struct PinnedRows {
+  const float* base = nullptr;  // row c is base + c * stride (listed rows only)
+  long long stride = 0;
+  uintptr_t lo = 0, hi = 0;     // bytes the call reads or writes
+};
+
+// Rows of n samples each at one stride in one pinned, identity-mapped host
+// allocation; null rows allowed when `nulls`.
+bool pinned_rows(const float* const* rows, int C, size_t n, bool nulls, PinnedRows* out) {
+  int c0 = -1, c1 = -1;
+  for (int c = 0; c < C; ++c) {
+    if (rows[c]) {
+      if (c0 < 0) c0 = c;
+      c1 = c;
+    } else if (!nulls) {
+      return false;
+    }
+  }
+  if (c0 < 0 || n == 0) return false;
+  // byte offsets, so that a row off the float grid is seen as such
+  auto at = [&](int c) { return (long long)reinterpret_cast<uintptr_t>(rows[c]); };
+  long long s = 0;  // stride in floats
+  if (c1 > c0) {
+    const long long d = at(c1) - at(c0);
+    if (d <= 0 || d % (4LL * (c1 - c0))) return false;
+    s = d / (4LL * (c1 - c0));
+    if (s < (long long)n) return false;  // overlapping rows
+    for (int c = c0 + 1; c < c1; ++c)
+      if (rows[c] && at(c) - at(c0) != 4 * s * (c - c0)) return false;
+  }
+  if ((at(c0) & 15) || ((s * 4) & 15)) return false;
+  if (!pinned_span(rows[c0], rows[c1] + n)) return false;
+  out->stride = s;
+  out->base = rows[c0] - (ptrdiff_t)((long long)c0 * s);
+  out->lo = reinterpret_cast<uintptr_t>(rows[c0]);
+  out->hi = reinterpret_cast<uintptr_t>(rows[c1] + n);
+  return true;
+}
+
 // Per-update descriptors, one upload: [ChanCtl x C][int channel list x C]
 // [8-byte aligned: IR row pointers x C].
 size_t uctl_ptr_offset(size_t C) { return ((sizeof(ChanCtl) + sizeof(int)) * C + 7) & ~size_t(7); }
@@ -394,7 +485,17 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
   const int nch = (int)chans.size();
   tanb::IrRows rows;
   rows.n = (long long)n;
-  if (mem == Mem::Host) {
+  PinnedRows pin;
+  const bool direct = mem == Mem::Host && n && nch == C && pinned_rows(ir, C, n, false, &pin);
+  if (direct) {
+    // rows in one pinned allocation at one stride: a single strided transfer
+    // into the compact rows, no host copy (the call waits for the transfer,
+    // so that the caller's rows are free again when it returns)
+    TANB_CUDA(cudaMemcpy2DAsync(v->d_ir, n * sizeof(float), pin.base, (size_t)pin.stride * sizeof(float),
+                                n * sizeof(float), (size_t)C, cudaMemcpyHostToDevice, v->stream));
+    rows.base = v->d_ir;
+    rows.stride = (long long)n;
+  } else if (mem == Mem::Host) {
     // Compact staging (row stride n; the kernel reads zeros past n). Large
     // updates copy rows on the host pool in channel groups and send each group
     // as soon as it is staged, so its transfer overlaps the next group's copy.
@@ -444,7 +545,10 @@ int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size
                         ref.ctl = d_uctl;
                         return tanb::launch_tail(v->ds, ref, 1, v->cur, 2, v->tiling, v->stream);
                       }));
-  if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY) TANB_CUDA(cudaStreamSynchronize(v->stream));
+  if (op & TANB_OPERATION_FLAG_BLOCK_UNTIL_READY)
+    TANB_CUDA(cudaStreamSynchronize(v->stream));
+  else if (direct)
+    TANB_CUDA(cudaEventSynchronize(v->ev_ir));  // behind the transfer from the caller's rows
   return TANB_OK;
 }
 
@@ -614,7 +718,15 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   // rows in the object's staging (host rows, the fused pipeline's int16 rows
   // and its scratch outputs): two base pointers describe every channel
   const bool staged = param && (pcm || (in_mem == Mem::Host && out_mem == Mem::Host));
-  const bool host_out = out_mem == Mem::Host;  // outputs are read back from host staging
+  const bool host_out = out_mem == Mem::Host;  // the call returns once the heads have signalled
+  // Caller rows the kernels can address in place (pinned host memory), on
+  // calls that wait for the heads anyway, so that the caller's rows are free
+  // again when the call returns.
+  PinnedRows pin_in, pin_out;
+  bool direct_in = staged && !pcm && pinned_rows(in, C, n, true, &pin_in);
+  bool direct_out = staged && !pcm && pinned_rows(out, C, n, false, &pin_out);
+  if (direct_in && direct_out && pin_in.lo < pin_out.hi && pin_out.lo < pin_in.hi)
+    direct_in = direct_out = false;  // in place or aliased: staging keeps the reads before the writes
   using Clock = std::chrono::steady_clock;
   auto us = [](Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::micro>(b - a).count();
@@ -663,6 +775,8 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
           const int16_t* src = pcm->in[c] + blk * B * pcm->in_step;
           for (int i = 0; i < B; ++i) row[i] = src[(size_t)i * pcm->in_step];
           x = v->stage_in(v->h_stage, b, c);
+        } else if (in_mem == Mem::Host && direct_in) {
+          x = in[c] ? in[c] + blk * B : nullptr;
         } else if (in_mem == Mem::Host) {
           x = in[c] ? v->stage_in(v->h_stage, b, c) : nullptr;
           if (run[c] && in[c])
@@ -672,6 +786,8 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         }
         if (pcm) {
           y = v->d_mix_scratch + (size_t)c * B;
+        } else if (direct_out) {
+          y = out[c] + blk * B;
         } else if (out_mem == Mem::Host) {
           y = v->h_out + ((size_t)b * C + c) * B;
         } else {
@@ -690,9 +806,20 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
         }
       }
       if (sd) {
-        sd->in = v->stage_in(v->h_stage, b, 0);
-        sd->out = pcm ? v->d_mix_scratch : v->h_out + (size_t)b * C * B;
-        sd->stride = B;
+        if (direct_in) {
+          sd->in = pin_in.base + blk * B;
+          sd->stride = pin_in.stride;
+        } else {
+          sd->in = v->stage_in(v->h_stage, b, 0);
+          sd->stride = B;
+        }
+        if (direct_out) {
+          sd->out = const_cast<float*>(pin_out.base) + blk * B;
+          sd->ostride = pin_out.stride;
+        } else {
+          sd->out = pcm ? v->d_mix_scratch : v->h_out + (size_t)b * C * B;
+          sd->ostride = B;
+        }
       }
       run_b[b] = run;
       v->cur = (v->cur - 1 + P) % P;
@@ -774,7 +901,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
             for (int i = 0; i < B; ++i) dst[(size_t)i * pcm->out_step] = st[(size_t)g * B + i];
           }
         }
-      } else {
+      } else if (!direct_out) {
         for (int b = 0; b < nb; ++b)
           for (int c = 0; c < C; ++c)
             if (run_b[b][c] && out[c])
@@ -794,6 +921,7 @@ int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, 
   v->ct[2] = t_wait;
   v->ct[3] = t_copy;
   v->ct[4] = us(t_call, Clock::now());
+  v->ct[5] = (direct_in ? 1 : 0) + (direct_out ? 2 : 0);
   return status;
 }
 
@@ -1525,10 +1653,10 @@ int32_t tanb_convolution_profile_read(tanb_convolution* v, int64_t counts[6], do
   return TANB_OK;
 }
 
-int32_t tanb_convolution_call_times(tanb_convolution* v, double us[5]) {
+int32_t tanb_convolution_call_times(tanb_convolution* v, double us[6]) {
   if (!v || !us) return fail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(v->mu);
-  for (int k = 0; k < 5; ++k) us[k] = v->ct[k];
+  for (int k = 0; k < 6; ++k) us[k] = v->ct[k];
   return TANB_OK;
 }
 

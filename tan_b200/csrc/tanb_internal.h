@@ -125,13 +125,15 @@ struct ParamDesc {
   const float* in[kParamChannels];
   float* out[kParamChannels];
 };
-// Rows in staging: channel c reads in + c * stride (when kCtlHasIn is set)
-// and writes out + c * stride.
+// Rows at fixed strides (the object's staging, or the caller's rows when they
+// sit in one pinned host allocation): channel c reads in + c * stride (when
+// kCtlHasIn is set) and writes out + c * ostride.
 struct StageDesc {
   CtlParam c;
   const float* in;
   float* out;
   long long stride;
+  long long ostride;
 };
 
 // Where a launch finds its per-channel descriptors: a ParamDesc or StageDesc

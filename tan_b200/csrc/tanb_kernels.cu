@@ -97,7 +97,7 @@ struct StgDesc {
   __device__ __forceinline__ const float* get_in(int c) const {
     return (p.c.ctl[c] & kCtlHasIn) ? p.in + c * p.stride : nullptr;
   }
-  __device__ __forceinline__ float* get_out(int c) const { return p.out + c * p.stride; }
+  __device__ __forceinline__ float* get_out(int c) const { return p.out + c * p.ostride; }
 };
 // Channel states only (the tail reads no rows).
 struct CtlDesc {
