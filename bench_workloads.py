@@ -183,7 +183,7 @@ def nonuniform_long(ctx, quick=False):
     cands = autotune.tune_nu_engine(ctx, C, L, B0)
     ok = [r for r in cands if r["max_ms"] < deadline] or cands
     best = ok[0]
-    nb = 600 if quick else 2000
+    nb = 600 if quick else 5000
     x = g.uniform(-1, 1, (C, nb * B0)).astype(np.float32)
     irs = np.stack([_ir(g, L, 8.0) for _ in range(C)])
     out = {"config": "nonuniform_long (cfg4)", "channels": C, "ir": L, "base_block": B0, "blocks": nb,
