@@ -643,7 +643,7 @@ def run_ours(args):
                             **{k: v for k, v in rs.items() if k != "achieved_gbs"}}
     # the other configurations: the uneven batch (cfg3, error vs FP64 for every
     # channel), the non-uniform 2^20-tap IRs (cfg4, on the engine, with its
-    # autotuned schedule) and the serving loop (cfg5, FP32 and FP24)
+    # autotuned schedule) and the serving loop (cfg5, FP32, FP16 and FP24)
     configs = None
     if rank == 0 and world == 1 and not args.no_configs:
         import bench_workloads as bw

@@ -8,7 +8,7 @@ engine_uneven  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096.
       input at -6 dBFS, FP32 / FP24 / FP16 / BF16 spectra; error vs FP64 for every channel
 nonuniform_long  non-uniform partitions, 256 ch, IR 2^20, base block 128, levels up to 16384,
       schedule from the autotuner, one engine session, FP32 / FP16; error vs FP64 on every channel
-serving  the serving loop (Poisson sessions, budget admission, swaps), FP32 / FP24
+serving  the serving loop (Poisson sessions, budget admission, swaps), FP32 / FP16 / FP24
 nu_block  one fixed non-uniform engine session (64 ch, IR 2^20, levels to 16384), for profiling
 pipeline  the sample pipeline (int16 stereo sources, per-ear convolution, mix,
       int16 out): fused call vs separate GPU calls vs the CPU restatement
@@ -277,11 +277,12 @@ def serving_cfg5(ctx, seconds=10.0, quick=False):
     """cfg5: the serving loop at 48 kHz, block 256 (5.33 ms deadline), Poisson
     arrivals 20/s, exponential lifetimes (mean 30 s), 1-8 channels, IR lengths
     log-uniform 8192..524288, IR swaps at 0.5/s per session, 150 GB budget,
-    starting in steady state; FP32 and FP24 forms."""
+    starting in steady state; the plain FP32 form, the FP16-spectrum form the
+    configuration names (per-partition scales, FP32 accumulation) and FP24."""
     from tan_b200 import serving
 
     out = {"config": "serving (cfg5)", "seconds": seconds, "data": "synthetic (seeded)"}
-    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp24", eng.SPECTRUM_FP24)):
+    for name, spec in (("fp32", eng.SPECTRUM_FP32), ("fp16", eng.SPECTRUM_FP16), ("fp24", eng.SPECTRUM_FP24)):
         r = serving.serve(ctx, seconds=(2.0 if quick else seconds), spectrum=spec)
         out[name] = {k: r[k] for k in ("blocks", "deadline_ms", "latency_ms", "deadline_misses",
                                        "concurrent_channels_mean", "concurrent_channels_max", "admitted",

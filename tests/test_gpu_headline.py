@@ -2,7 +2,8 @@
 delay-line slot is reused: 64 channels, B = 512, IR 65536 (P = 128), an IR
 swap every 32 blocks, 224 blocks (the slot ring of 128 spectra wraps 1.75
 times, so partitions up to 127 multiply signal and the tail's slot arithmetic
-(cur + i - 1) mod P wraps at every start position). Also an engine session
+(cur + i - 1) mod P wraps at every start position), and the configuration's
+full 2000 blocks. Also an engine session
 with P = 256 over 300 blocks, finalize mode against the oracle, and the
 reference's dense IR fixture.
 
@@ -82,6 +83,49 @@ def test_headline_shape_ring_wraps_matches_restatement_and_fp64(tan_ctx):
     exp = fp64.stream_fp64(x, B, fp_events)
     worst = max(fp64.error_db(y[c], exp[c]) for c in range(C))
     assert worst < -120, worst
+
+
+def test_headline_config_2000_blocks_matches_restatement(tan_ctx):
+    """The headline configuration at its stated length: 64 channels, B = 512,
+    IR 65536, every channel's IR replaced every 32 blocks (eight IR sets
+    cycled), 2000 blocks through the plugin call with page-locked host rows
+    (read and written in place by the head), block by block against the
+    restatement on every channel; FP64 on two channels over the first 320
+    blocks (the FP64 statement convolves the whole stream once per IR
+    version)."""
+    import torch
+
+    C, B, L, nb, every = 64, 512, 65536, 2000, 32
+    g = H.rng(20261203 + 21)
+    sets = [H.irs(g, C, L, (0.2, 1.5)) for _ in range(8)]
+    tx = torch.from_numpy(H.noise(g, C, nb * B)).pin_memory()
+    x = tx.numpy()
+    events = {k: (sets[(k // every) % 8], None) for k in range(0, nb, every)}
+    oracle = ref.RefConvolution(L, B, C, threads=os.cpu_count() or 4)
+    yr, codes = H.run_stream(oracle, x, B, events)
+    oracle.close()
+    assert all(c == 0 for c in codes)
+    ty = torch.zeros((C, nb * B), dtype=torch.float32).pin_memory()
+    y = ty.numpy()
+    conv = cv.TANConvolution(tan_ctx)
+    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == cv.AMF_OK
+    in_place = set()
+    for k in range(nb):
+        if k in events:
+            assert conv.UpdateResponseTD(events[k][0], L) == cv.AMF_OK
+        rc, done = conv.Process([x[c, k * B:(k + 1) * B] for c in range(C)],
+                                [y[c, k * B:(k + 1) * B] for c in range(C)], B)
+        assert rc == cv.AMF_OK and done == B
+        in_place.add(conv.call_times()["in_place"])
+    conv.Release()
+    assert in_place == {3}
+    err = _blockwise_rel_err(y, yr, B)
+    assert err < TOL, err
+    n1 = 320
+    exp = fp64.stream_fp64(x[:2, :n1 * B], B, [(k, {c: ir[c] for c in range(2)}) for k, (ir, _) in events.items()
+                                             if k < n1])
+    for c in range(2):
+        assert fp64.error_db(y[c, :n1 * B], exp[c]) < -120
 
 
 def test_engine_session_p256_long_run_mix_equals_alone(tan_ctx):
