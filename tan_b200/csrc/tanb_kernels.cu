@@ -171,36 +171,87 @@ __device__ __forceinline__ void dft8_fwd(float2* v) {
 }
 
 // IR partition spectra with radix-8 Stockham stages in registers: M / 8
-// threads, one shared-memory pass per stage instead of two for radix 4
-// (8192 transforms of 512 points: 32 us against 45 us). When log2 M is not a
-// multiple of 3, a radix-2 or radix-4 stage comes first; it reads the row
-// directly, where the upper half of the frame is zero. Shared memory is
+// threads per partition, one shared-memory pass per stage instead of two for
+// radix 4 (8192 transforms of 512 points: 32 us against 45 us). When log2 M is
+// not a multiple of 3, a radix-2 or radix-4 stage comes first; it reads the
+// row directly, where the upper half of the frame is zero. Shared memory is
 // padded by one slot per 8 so that the strided stage stores spread over the
 // banks. Same inputs, twiddle table and output as ir_spectrum_kernel.
+//
+// Up to M = 1024 a CTA transforms G partitions side by side (256 threads) and
+// first gathers each stage's twiddles into shared memory, ordered so that a
+// warp reads consecutive entries: read from the table in global memory, the
+// stages' scattered twiddle loads kept the L1 pipe 93% busy (29 us for 8192
+// transforms of 512 points, which move 50 MB). The values are the table's, so
+// the spectra are the same bit for bit.
 template <int LOG2M>
-__global__ void __launch_bounds__((1 << LOG2M) / 8)
+struct IrR8Shape {
+  static constexpr int M = 1 << LOG2M, T = M / 8;
+  static constexpr int R0 = LOG2M % 3;
+  static constexpr int NS0 = R0 == 0 ? 8 : (R0 == 1 ? 2 : 4);  // span after the first stage
+  static constexpr bool TWS = T <= 128;                // stage twiddles in shared memory
+  static constexpr int G = TWS ? 256 / T : 1;          // partitions per CTA
+  static constexpr int THREADS = G * T;
+  // the stages' twiddles W^(r k tstep), r = 1..7, k < Ns, stored [stage][r - 1][k]
+  // so that a warp's lanes (consecutive k) read consecutive entries
+  static constexpr int stage_entries() {
+    int n = 0;
+    for (int ns = NS0; ns < M; ns *= 8) n += 7 * ns;
+    return n;
+  }
+  static constexpr int TWN = stage_entries();
+};
+
+template <int LOG2M>
+__global__ void __launch_bounds__(IrR8Shape<LOG2M>::THREADS)
     ir_spectrum_r8_kernel(DevState s, IrRows ir, const int* __restrict__ chans, const ChanCtl* __restrict__ ctl) {
-  constexpr int M = 1 << LOG2M, T = M / 8, R0 = LOG2M % 3;  // first stage radix 2^R0 (1: none)
-  __shared__ float2 sm[M + M / 8];
+  using Sh = IrR8Shape<LOG2M>;
+  constexpr int M = Sh::M, T = Sh::T, G = Sh::G, R0 = Sh::R0;  // first stage radix 2^R0 (1: none)
+  constexpr int PADDED = M + M / 8;
+  __shared__ float2 sm_all[G * PADDED];
+  __shared__ float2 tw_st[Sh::TWS ? Sh::TWN : 1];
   auto pad = [](int i) { return i + (i >> 3); };
-  const int part = blockIdx.x;
+  const int grp = (G > 1) ? (int)threadIdx.x / T : 0;
+  const int j = (G > 1) ? (int)threadIdx.x % T : (int)threadIdx.x;
+  float2* sm = sm_all + grp * PADDED;
+  const int part = blockIdx.x * G + grp;
+  const bool live = part < s.P;
   const int row = blockIdx.y;
   const int c = chans[row];
   const int slot = ctl[c].slot_new;
   const float* h = ir.ptrs ? ir.ptrs[row] : ir.base + (size_t)row * ir.stride;
   const long long t0 = (long long)part * M;
-  const int j = threadIdx.x;
-  // z[n] = (h[t0 + 2n], h[t0 + 2n + 1]) for n < M / 2, zero above
+  const float2* tw = s.tw;
+  if constexpr (Sh::TWS) {
+    // gathered once per CTA from the table; made visible by the barrier after
+    // the first stage
+    int base = 0;
+    for (int ns = Sh::NS0; ns < M; ns *= 8) {
+      const int tstep = (2 * M) / (8 * ns);
+      for (int q = threadIdx.x; q < 7 * ns; q += Sh::THREADS) {
+        const int r = 1 + q / ns, k = q % ns;
+        tw_st[base + q] = __ldg(s.tw + r * k * tstep);
+      }
+      base += 7 * ns;
+    }
+  }
+  // z[n] = (h[t0 + 2n], h[t0 + 2n + 1]) for n < M / 2, zero above (and for a
+  // group past the last partition, which runs the stages for their barriers)
+  const bool h8 = (reinterpret_cast<uintptr_t>(h) & 7) == 0;  // t is even: pairs load as one float2
   auto load = [&](int n) {
     float2 v = make_float2(0.f, 0.f);
-    if (n < M / 2) {
+    if (live && n < M / 2) {
       const long long t = t0 + 2 * n;
-      if (t < ir.n) v.x = h[t];
-      if (t + 1 < ir.n) v.y = h[t + 1];
+      if (h8 && t + 1 < ir.n) {
+        v = __ldg(reinterpret_cast<const float2*>(h + t));
+      } else {
+        if (t < ir.n) v.x = h[t];
+        if (t + 1 < ir.n) v.y = h[t + 1];
+      }
     }
     return v;
   };
-  constexpr int NS0 = R0 == 0 ? 8 : (R0 == 1 ? 2 : 4);  // span after the first stage
+  constexpr int NS0 = Sh::NS0;
   float2 v[8];
   if constexpr (R0 == 0) {
     // radix-8 stage with Ns = 1: inputs j + r M / 8, zero for r >= 4
@@ -233,13 +284,19 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
     }
   }
   __syncthreads();
-  auto stage = [&](const int Ns) {
+  auto stage = [&](const int Ns, const int tbase) {
     const int k = j & (Ns - 1);
     const int tstep = (2 * M) / (8 * Ns);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const float2 x = sm[pad(j + r * T)];
-      v[r] = r ? c_mul(x, __ldg(s.tw + r * k * tstep)) : x;
+      if (r == 0) {
+        v[r] = x;
+      } else if constexpr (Sh::TWS) {
+        v[r] = c_mul(x, tw_st[tbase + (r - 1) * Ns + k]);
+      } else {
+        v[r] = c_mul(x, __ldg(tw + r * k * tstep));
+      }
     }
     __syncthreads();
     dft8_fwd(v);
@@ -251,12 +308,21 @@ __global__ void __launch_bounds__((1 << LOG2M) / 8)
   // Powers of 8 unroll the stages (compile-time spans and twiddle strides);
   // the others keep one loop body, which ptxas fits without spilling.
   if constexpr (R0 == 0) {
+    int tb = 0;
 #pragma unroll
-    for (int Ns = NS0; Ns < M; Ns <<= 3) stage(Ns);
+    for (int Ns = NS0; Ns < M; Ns <<= 3) {
+      stage(Ns, tb);
+      tb += 7 * Ns;
+    }
   } else {
+    int tb = 0;
 #pragma unroll 1
-    for (int Ns = NS0; Ns < M; Ns <<= 3) stage(Ns);
+    for (int Ns = NS0; Ns < M; Ns <<= 3) {
+      stage(Ns, tb);
+      tb += 7 * Ns;
+    }
   }
+  if (!live) return;
   float2* H = s.H + h_index(s, c, slot, part);
   for (int k = j; k <= M / 2; k += T) {
     if (k == 0) {
@@ -742,11 +808,12 @@ template <int LOG2M>
 cudaError_t launch_ir_t(const DevState& s, const IrRows& ir, const int* chans, int nch, const ChanCtl* ctl,
                         cudaStream_t st) {
   using S = FftShape<LOG2M>;
-  dim3 grid(s.P, nch);
-  if constexpr (LOG2M <= 12)  // the padded buffer of 8192 points exceeds static shared memory
-    ir_spectrum_r8_kernel<LOG2M><<<grid, S::M / 8, 0, st>>>(s, ir, chans, ctl);
-  else
-    ir_spectrum_kernel<LOG2M><<<grid, S::T, S::M * sizeof(float2), st>>>(s, ir, chans, ctl);
+  if constexpr (LOG2M <= 12) {  // the padded buffer of 8192 points exceeds static shared memory
+    using R = IrR8Shape<LOG2M>;
+    ir_spectrum_r8_kernel<LOG2M><<<dim3((s.P + R::G - 1) / R::G, nch), R::THREADS, 0, st>>>(s, ir, chans, ctl);
+  } else {
+    ir_spectrum_kernel<LOG2M><<<dim3(s.P, nch), S::T, S::M * sizeof(float2), st>>>(s, ir, chans, ctl);
+  }
   return cudaGetLastError();
 }
 
