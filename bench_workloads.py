@@ -1,7 +1,7 @@
 """Measurements of the path on each benchmark configuration (seeded synthetic
 inputs with the configurations' shapes; no public dataset is involved).
 
-    python bench_workloads.py dropin_small|engine_uneven|nonuniform_long|nu-tune|pipeline [--quick]
+    python bench_workloads.py dropin_small|engine_uneven|nonuniform_long|nu-tune|pipeline|serving|nu_block|ir_swap [--quick]
 
 dropin_small  drop-in TANConvolution, 2 ch, B=1024, IR 8192, 200 blocks, FP32
 engine_uneven  engine, 1024 single-channel sessions, B=256, IR log-uniform 4096..262144,
@@ -10,6 +10,7 @@ nonuniform_long  non-uniform partitions, 256 ch, IR 2^20, base block 128, levels
       schedule from the autotuner, one engine session, FP32 / FP16; error vs FP64 on every channel
 serving  the serving loop (Poisson sessions, budget admission, swaps), FP32 / FP16 / FP24
 nu_block  one fixed non-uniform engine session (64 ch, IR 2^20, levels to 16384), for profiling
+ir_swap  the bench workload's IR swap step on the drop-in (64 ch x 128 partitions), for profiling
 pipeline  the sample pipeline (int16 stereo sources, per-ear convolution, mix,
       int16 out): fused call vs separate GPU calls vs the CPU restatement
 Each prints one JSON object: throughput (GSamples/s), per-block latency
@@ -242,6 +243,30 @@ def nonuniform_long(ctx, quick=False):
     return out
 
 
+def ir_swap(ctx, quick=False, C=64, B=512, L=65536, updates=20):
+    """The bench workload's IR swap step on the drop-in, for profiling: device
+    IR rows, UpdateResponseTDDevice with BLOCK_UNTIL_READY `updates` times
+    after three untimed ones; per-kernel device time from the object's
+    accounting (CUDA events around every launch)."""
+    import torch
+
+    g = _rng(7)
+    conv = cv.TANConvolution(ctx)
+    assert conv.Init(cv.TAN_CONVOLUTION_METHOD_FFT_UNIFORM_PARTITIONED, L, B, C) == 0
+    h = torch.from_numpy(np.stack([_ir(g, L, 1.0) for _ in range(C)])).cuda()
+    for _ in range(3):
+        assert conv.UpdateResponseTDDevice(h, L, None, cv.TAN_CONVOLUTION_OPERATION_FLAG_BLOCK_UNTIL_READY) == 0
+    conv.profile(True)
+    conv.profile_read()
+    for _ in range(2 if quick else updates):
+        assert conv.UpdateResponseTDDevice(h, L, None, cv.TAN_CONVOLUTION_OPERATION_FLAG_BLOCK_UNTIL_READY) == 0
+    p = conv.profile_read()
+    conv.profile(False)
+    conv.Release()
+    return {"config": "ir_swap", "channels": C, "block": B, "ir": L, "partitions": -(-L // B),
+            "us_per_launch": {k: 1e3 * v["ms"] / max(1, v["timed"]) for k, v in p.items() if v["timed"]}}
+
+
 def nu_block(ctx, quick=False, C=64, blocks=300):
     """A fixed non-uniform engine session for profiling: C channels, IR 2^20,
     base block 128, levels 128x2, 256..8192 x1, 16384x63 (the cfg4 tuner's
@@ -377,7 +402,7 @@ def pipeline(ctx, quick=False, S=32, B=256, L=48000):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("which", choices=["dropin_small", "engine_uneven", "nonuniform_long", "nu-tune", "pipeline",
-                                      "serving", "nu_block"])
+                                      "serving", "nu_block", "ir_swap"])
     ap.add_argument("--quick", action="store_true")
     a = ap.parse_args()
     ctx = cv.TANContext(0)
@@ -386,7 +411,7 @@ def main():
     else:
         r = {"dropin_small": dropin_small, "engine_uneven": engine_uneven, "nonuniform_long": nonuniform_long,
              "pipeline": pipeline, "serving": lambda c, q: serving_cfg5(c, quick=q),
-             "nu_block": nu_block}[a.which](ctx, a.quick)
+             "nu_block": nu_block, "ir_swap": ir_swap}[a.which](ctx, a.quick)
     print(json.dumps(r))
 
 
