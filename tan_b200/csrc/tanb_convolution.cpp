@@ -461,6 +461,7 @@ size_t uctl_bytes(size_t C) { return uctl_ptr_offset(C) + C * sizeof(void*); }
 
 int32_t update_common(tanb_convolution* v, Mem mem, const float* const* ir, size_t n, const uint32_t* flags,
                       uint32_t op) {
+  tanb::NvtxRange range("tanb UpdateResponseTD");
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
   std::lock_guard<std::mutex> lock(v->mu);
   if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "UpdateResponseTD before Init");
@@ -685,6 +686,7 @@ cudaError_t ensure_mix(tanb_convolution* v, const PcmIO& pcm, tanb::MixEpi* epi)
 
 int32_t process_common(tanb_convolution* v, Mem in_mem, const float* const* in, Mem out_mem, float* const* out,
                        size_t n, const uint32_t* flags, size_t* done, const PcmIO* pcm = nullptr) {
+  tanb::NvtxRange range("tanb Process");
   if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
   std::lock_guard<std::mutex> lock(v->mu);
   if (done) *done = 0;

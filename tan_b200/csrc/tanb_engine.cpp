@@ -620,6 +620,7 @@ cudaError_t grow_items(tanb_engine* e, size_t need) {
 int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint32_t nlevels,
                      const uint32_t* level_block, const uint32_t* level_parts, int32_t* session,
                      uint32_t* first_slot) {
+  tanb::NvtxRange range("tanb engine open session");
   if (!e || !session) return efail(TANB_INVALID_POINTER, "null argument");
   std::lock_guard<std::mutex> lock(e->mu);
   if (channels == 0 || ir_length == 0) return efail(TANB_INVALID_ARG, "channels and IR length must be > 0");
@@ -781,6 +782,7 @@ int32_t open_session(tanb_engine* e, uint32_t channels, uint32_t ir_length, uint
 
 int32_t engine_update(tanb_engine* e, int32_t session, const float* const* ir, size_t n, bool device, uint32_t op,
                       const uint8_t* mask) {
+  tanb::NvtxRange range("tanb engine IR update");
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   if (!ir) return efail(TANB_INVALID_ARG, "ppBuffer == NULL");
   std::lock_guard<std::mutex> ulock(e->upd_mu);
@@ -1103,6 +1105,7 @@ int32_t tanb_engine_open_session_nu(tanb_engine* e, uint32_t channels, uint32_t 
 }
 
 int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
+  tanb::NvtxRange range("tanb engine close session");
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   std::lock_guard<std::mutex> ulock(e->upd_mu);  // no IR upload may still write this session's memory
   std::lock_guard<std::mutex> lock(e->mu);
@@ -1183,6 +1186,7 @@ int32_t tanb_engine_write_input(tanb_engine* e, uint32_t first_slot, const float
 }
 
 int32_t tanb_engine_process(tanb_engine* e) {
+  tanb::NvtxRange range("tanb engine block");
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   const Clock::time_point t_call = Clock::now();
   std::lock_guard<std::mutex> lock(e->mu);
@@ -1201,6 +1205,7 @@ int32_t tanb_engine_process(tanb_engine* e) {
 }
 
 int32_t tanb_engine_process_device(tanb_engine* e, const float* in, float* out, uint32_t ld) {
+  tanb::NvtxRange range("tanb engine block (device rows)");
   if (!e) return efail(TANB_INVALID_POINTER, "null engine");
   std::lock_guard<std::mutex> lock(e->mu);
   if (!out) return efail(TANB_INVALID_ARG, "null output");

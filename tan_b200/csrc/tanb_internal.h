@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <mutex>
@@ -16,6 +17,16 @@ namespace tanb {
 
 // Records the text returned by tanb_last_error() on this thread.
 void set_last_error(const char* msg);
+
+// An NVTX range over a scope: the entry points name their host work so that
+// Nsight tools (and ncu's --nvtx filters) can place it; without a tool
+// attached a push or pop costs a few nanoseconds.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // A set-up step that must run once on every CUDA device a process uses (kernel
 // attributes such as the dynamic shared-memory limit are held per device):
