@@ -258,6 +258,22 @@ int32_t tanb_convolution_profile(tanb_convolution* conv, int32_t enable);
  * summed device milliseconds. Waits for the timed launches to finish. */
 int32_t tanb_convolution_profile_read(tanb_convolution* conv, int64_t counts[6], double ms[3]);
 
+/* No reference counterpart (checkpoint / migration): a snapshot of the object's
+ * stream state -- both IR slots' spectra, the delay line, the overlap-save
+ * history, the tail rows (a pending IR's too), the delay-line position, the
+ * block count and the per-channel swap and flag state -- in a caller buffer
+ * of tanb_convolution_snapshot_bytes bytes (host memory, pageable or not).
+ * tanb_convolution_restore loads one into an object with the same Init
+ * (method, IR length, block, channels), on this GPU or another: its stream
+ * then continues with the same output, bit for bit. Snapshot runs a tail that
+ * finalize mode deferred and waits for the object's stream; restore discards
+ * the target's own state. Uniformly partitioned methods only
+ * (TANB_NOT_SUPPORTED for TIME_DOMAIN and the non-uniform methods);
+ * TANB_INVALID_ARG for a short buffer or a snapshot of another configuration. */
+int32_t tanb_convolution_snapshot_bytes(tanb_convolution* conv, uint64_t* bytes);
+int32_t tanb_convolution_snapshot(tanb_convolution* conv, void* buffer, uint64_t bytes);
+int32_t tanb_convolution_restore(tanb_convolution* conv, const void* buffer, uint64_t bytes);
+
 /* No reference counterpart: host microseconds of the last Process call of the
  * uniformly partitioned methods, by part -- us[0] staging the rows and
  * descriptors, us[1] launching the kernels, us[2] waiting for the heads'

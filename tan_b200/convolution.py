@@ -113,6 +113,9 @@ SIGNATURES = {
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_engine_block_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "tanb_convolution_call_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "tanb_convolution_snapshot_bytes": (_i32, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "tanb_convolution_snapshot": (_i32, [_vp, _vp, ctypes.c_uint64]),
+    "tanb_convolution_restore": (_i32, [_vp, _vp, ctypes.c_uint64]),
     "tanb_convolution_process_mix_pcm16": (_i32, [_vp, _pp, _sz, ctypes.c_float, _u32p, _u32, _pp, _sz,
                                                   ctypes.c_float, _sz, ctypes.POINTER(ctypes.c_int32), _szp]),
     "tanb_room_generator_create": (_i32, [_vp, _i32, ctypes.POINTER(_vp)]),
@@ -388,6 +391,21 @@ class TANConvolution:
         out = (ctypes.c_int32 * 3)()
         rc = lib().tanb_convolution_tiling(self._h, index, out)
         return rc, tuple(out)
+
+    def Snapshot(self):
+        """(AMF_RESULT, uint8 array): the object's stream state (no reference counterpart)."""
+        n = ctypes.c_uint64(0)
+        rc = lib().tanb_convolution_snapshot_bytes(self._h, ctypes.byref(n))
+        if rc != AMF_OK:
+            return rc, None
+        buf = np.empty(n.value, np.uint8)
+        rc = lib().tanb_convolution_snapshot(self._h, buf.ctypes.data, n.value)
+        return rc, (buf if rc == AMF_OK else None)
+
+    def Restore(self, snapshot) -> int:
+        """Loads a Snapshot() of an object with the same Init into this one."""
+        buf = np.ascontiguousarray(snapshot, dtype=np.uint8)
+        return lib().tanb_convolution_restore(self._h, buf.ctypes.data, buf.size)
 
     def call_times(self) -> dict:
         """Host microseconds of the last Process call, by part."""

@@ -1662,6 +1662,153 @@ int32_t tanb_convolution_call_times(tanb_convolution* v, double us[6]) {
   return TANB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Stream-state snapshot and restore (no reference counterpart): everything a
+// uniformly partitioned object carries from one block to the next -- both IR
+// slots' spectra, the delay line, the overlap-save history, the tail rows
+// (including a pending IR's), the delay-line position, the block count (the
+// tail rows alternate with its parity) and the per-channel swap and flag
+// state -- so that another object with the same Init, on this GPU or on
+// another, resumes the stream with the same output bit for bit: a checkpoint,
+// or a session's migration between GPUs through host memory.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SnapHeader {
+  char magic[8];
+  uint32_t method, L, B, C, P, length;
+  int32_t cur;
+  int64_t blocks;
+};
+constexpr char kSnapMagic[8] = {'T', 'A', 'N', 'B', 'S', 'N', 'P', '1'};
+
+size_t snap_bytes(const tanb_convolution* v) {
+  const size_t C = v->C, P = v->P, B = v->B;
+  return sizeof(SnapHeader) + C * (4 * sizeof(int32_t) + 2) +
+         (C * 2 * P * B + C * P * B + C * 3 * B) * sizeof(float2) + C * B * sizeof(float);
+}
+
+int32_t snap_check(tanb_convolution* v) {
+  if (!v) return fail(TANB_INVALID_POINTER, "null convolution");
+  if (!v->initialized) return fail(TANB_NOT_INITIALIZED, "snapshot before Init");
+  if (v->td || v->nu_eng)
+    return fail(TANB_NOT_SUPPORTED, "snapshots cover the uniformly partitioned methods");
+  return TANB_OK;
+}
+
+}  // namespace
+
+int32_t tanb_convolution_snapshot_bytes(tanb_convolution* v, uint64_t* bytes) {
+  if (bytes) *bytes = 0;
+  if (!v || !bytes) return fail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(v->mu);
+  const int32_t r = snap_check(v);
+  if (r != TANB_OK) return r;
+  *bytes = snap_bytes(v);
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_snapshot(tanb_convolution* v, void* buffer, uint64_t bytes) {
+  if (!v || !buffer) return fail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(v->mu);
+  int32_t r = snap_check(v);
+  if (r != TANB_OK) return r;
+  if (bytes < snap_bytes(v)) return fail(TANB_INVALID_ARG, "snapshot buffer of %llu bytes, %zu needed",
+                                         (unsigned long long)bytes, snap_bytes(v));
+  TANB_CUDA(cudaSetDevice(v->ctx->device));
+  // a tail deferred by finalize mode belongs to the state: run it first
+  if (run_pending_finalize(v) != TANB_OK) return TANB_FAIL;
+  TANB_CUDA(cudaStreamSynchronize(v->stream));
+  v->staging_busy = false;
+  if (*v->h_err != tanb::kErrNone) return fail(TANB_FAIL, "device wait timed out (error %d)", *v->h_err);
+  const size_t C = v->C, P = v->P, B = v->B;
+  char* p = static_cast<char*>(buffer);
+  SnapHeader h{};
+  std::memcpy(h.magic, kSnapMagic, sizeof(h.magic));
+  h.method = v->method;
+  h.L = (uint32_t)v->L;
+  h.B = (uint32_t)v->B;
+  h.C = (uint32_t)v->C;
+  h.P = (uint32_t)v->P;
+  h.length = (uint32_t)v->length;
+  h.cur = v->cur;
+  h.blocks = v->blocks;
+  std::memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  for (const std::vector<int>* a : {&v->active, &v->pending, &v->slot_new, &v->tail_left}) {
+    for (size_t c = 0; c < C; ++c) {
+      const int32_t x = (*a)[c];
+      std::memcpy(p, &x, sizeof(x));
+      p += sizeof(x);
+    }
+  }
+  std::memcpy(p, v->available.data(), C);
+  p += C;
+  std::memcpy(p, v->flushed.data(), C);
+  p += C;
+  const size_t nh = C * 2 * P * B * sizeof(float2), nf = C * P * B * sizeof(float2), np_ = C * B * sizeof(float),
+               nt = C * 3 * B * sizeof(float2);
+  TANB_CUDA(cudaMemcpy(p, v->ds.H, nh, cudaMemcpyDeviceToHost));
+  p += nh;
+  TANB_CUDA(cudaMemcpy(p, v->ds.fdl, nf, cudaMemcpyDeviceToHost));
+  p += nf;
+  TANB_CUDA(cudaMemcpy(p, v->ds.prev, np_, cudaMemcpyDeviceToHost));
+  p += np_;
+  TANB_CUDA(cudaMemcpy(p, v->ds.tail, nt, cudaMemcpyDeviceToHost));
+  return TANB_OK;
+}
+
+int32_t tanb_convolution_restore(tanb_convolution* v, const void* buffer, uint64_t bytes) {
+  if (!v || !buffer) return fail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(v->mu);
+  int32_t r = snap_check(v);
+  if (r != TANB_OK) return r;
+  if (bytes < snap_bytes(v)) return fail(TANB_INVALID_ARG, "snapshot of %llu bytes, %zu expected",
+                                         (unsigned long long)bytes, snap_bytes(v));
+  const char* p = static_cast<const char*>(buffer);
+  SnapHeader h;
+  std::memcpy(&h, p, sizeof(h));
+  p += sizeof(h);
+  if (std::memcmp(h.magic, kSnapMagic, sizeof(h.magic)) != 0) return fail(TANB_INVALID_ARG, "not a snapshot");
+  if (h.method != v->method || h.L != (uint32_t)v->L || h.B != (uint32_t)v->B || h.C != (uint32_t)v->C ||
+      h.P != (uint32_t)v->P || h.length != (uint32_t)v->length)
+    return fail(TANB_INVALID_ARG, "snapshot of another configuration (method %u, L %u, B %u, C %u)", h.method, h.L,
+                h.B, h.C);
+  if (h.cur < 0 || h.cur >= v->P || h.blocks < 0) return fail(TANB_INVALID_ARG, "corrupt snapshot header");
+  TANB_CUDA(cudaSetDevice(v->ctx->device));
+  // nothing of this object's own stream may still run on the buffers
+  v->finalize_due = false;
+  TANB_CUDA(cudaStreamSynchronize(v->stream));
+  v->staging_busy = false;
+  const size_t C = v->C, P = v->P, B = v->B;
+  for (std::vector<int>* a : {&v->active, &v->pending, &v->slot_new, &v->tail_left}) {
+    for (size_t c = 0; c < C; ++c) {
+      int32_t x;
+      std::memcpy(&x, p, sizeof(x));
+      p += sizeof(x);
+      (*a)[c] = x;
+    }
+  }
+  for (size_t c = 0; c < C; ++c)
+    if ((v->active[c] | v->slot_new[c] | v->pending[c]) & ~1) return fail(TANB_INVALID_ARG, "corrupt snapshot state");
+  std::memcpy(v->available.data(), p, C);
+  p += C;
+  std::memcpy(v->flushed.data(), p, C);
+  p += C;
+  const size_t nh = C * 2 * P * B * sizeof(float2), nf = C * P * B * sizeof(float2), np_ = C * B * sizeof(float),
+               nt = C * 3 * B * sizeof(float2);
+  TANB_CUDA(cudaMemcpy(v->ds.H, p, nh, cudaMemcpyHostToDevice));
+  p += nh;
+  TANB_CUDA(cudaMemcpy(v->ds.fdl, p, nf, cudaMemcpyHostToDevice));
+  p += nf;
+  TANB_CUDA(cudaMemcpy(v->ds.prev, p, np_, cudaMemcpyHostToDevice));
+  p += np_;
+  TANB_CUDA(cudaMemcpy(v->ds.tail, p, nt, cudaMemcpyHostToDevice));
+  v->cur = h.cur;
+  v->blocks = h.blocks;
+  return TANB_OK;
+}
+
 int32_t tanb_convolution_info(tanb_convolution* v, int64_t out[4]) {
   if (!v || !out) return fail(TANB_INVALID_POINTER, "null argument");
   out[0] = v->nu_eng ? (int64_t)v->nu_parts[0] : v->P;  // non-uniform: the base level's partitions
