@@ -84,12 +84,18 @@ def config_dict(P):
     }
 
 
-def make_inputs(nblocks, seed=SEED):
-    from oracle import fp64
+def exp_decay_ir(g, n, rt60_s, fs=FS):
+    """Gaussian noise times exp(-ln(1000) t / (RT60 fs)), unit L2 norm (float32)."""
+    t = np.arange(n, dtype=np.float64)
+    h = g.standard_normal(n) * np.exp(-np.log(1000.0) * t / (rt60_s * fs))
+    h /= np.linalg.norm(h)
+    return h.astype(np.float32)
 
+
+def make_inputs(nblocks, seed=SEED):
     g = np.random.Generator(np.random.PCG64(seed))
     x = g.uniform(-1.0, 1.0, (C, nblocks * B)).astype(np.float32)
-    irs = [np.stack([fp64.exp_decay_ir(g, L, float(g.uniform(0.2, 1.5))) for _ in range(C)])
+    irs = [np.stack([exp_decay_ir(g, L, float(g.uniform(0.2, 1.5))) for _ in range(C)])
            for _ in range(N_IR_SETS)]
     return x, irs
 
@@ -641,14 +647,14 @@ def run_ours(args):
                             "what": "batched FP32 engine at its real-time capacity (sessions of 4 ch, IR 48000, "
                                     "block 256), device I/O, CUDA events per block; working set >> L2",
                             **{k: v for k, v in rs.items() if k != "achieved_gbs"}}
-    # the other configurations: the uneven batch (cfg3, error vs FP64 for every
+    # the other configurations: the small drop-in case (cfg1), the uneven batch (cfg3, error vs FP64 for every
     # channel), the non-uniform 2^20-tap IRs (cfg4, on the engine, with its
     # autotuned schedule) and the serving loop (cfg5, FP32, FP16 and FP24)
     configs = None
     if rank == 0 and world == 1 and not args.no_configs:
         import bench_workloads as bw
 
-        configs = {"cfg3": bw.engine_uneven(ctx), "cfg4": bw.nonuniform_long(ctx),
+        configs = {"cfg1": bw.dropin_small(ctx), "cfg3": bw.engine_uneven(ctx), "cfg4": bw.nonuniform_long(ctx),
                    "cfg5": bw.serving_cfg5(ctx, seconds=10.0)}
     # several GPUs: the serving mix sharded over the ranks (sessions placed by
     # the engines' admission rule, no audio crossing GPUs), every rank its own
