@@ -241,6 +241,36 @@ def cpu_baseline(sample_s, threads=None):
                       f"{dt:.1f} s wall", "ms_per_block": 1000.0 * dt / done_blocks}
 
 
+def cpu_pipeline_chain(S=32, B=256, L=48000, blocks=100):
+    """The sample pipeline's chain (int16 -> convolution -> mix per ear ->
+    int16, bench_workloads.py pipeline) on the oracle restatement, per block,
+    on all host cores: the CPU baseline of the fused GPU call."""
+    from oracle import ref
+
+    import bench_workloads as bw
+
+    C = 2 * S
+    src, h, group, rows_in = bw.pipeline_inputs(S, B, L, blocks)
+    threads = os.cpu_count()
+    conv = ref.RefConvolution(L, B, C, threads=threads)
+    conv.update_response_td(h)
+    lat = []
+    for k in range(blocks):
+        t0 = time.perf_counter()
+        x = np.stack([ref.convert_s16_f32(r[2 * k * B:], 1.0, in_step=2, n=B) for r in rows_in])
+        y = np.zeros_like(x)
+        conv.process(x, None, y)
+        for ear in range(2):
+            ref.convert_f32_s16(ref.mix(y[ear::2]), 1.0)
+        lat.append(1e3 * (time.perf_counter() - t0))
+    conv.close()
+    lat = np.asarray(lat[5:])
+    return {"what": "the sample pipeline's chain on the restatement (32 int16 stereo sources, 64 channels, "
+                    "1 s IRs, B = 256), per block", "cores": threads,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "gsamples_per_s": float(C * B / (lat.mean() / 1e3) / 1e9)}
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -673,6 +703,7 @@ def run_ours(args):
         # the host's processors (FFTImpl.cpp:245-249, MathImpl.cpp:154-158)
         cpu["reference_default_threads"] = cpu_baseline(min(5.0, args.cpu_sample_s),
                                                          threads=max(1, (os.cpu_count() or 4) // 4))
+        cpu["pipeline_chain"] = cpu_pipeline_chain()
 
     if rank == 0:
         deadline_ms = 1000.0 * B / FS

@@ -315,24 +315,32 @@ def serving_cfg5(ctx, seconds=10.0, quick=False):
     return out
 
 
-def pipeline(ctx, quick=False, S=32, B=256, L=48000):
-    """The sample pipeline (int16 stereo sources -> per-ear convolution -> mix
-    per ear -> int16 interleaved stereo) per block: the fused call, the same
-    chain through the separate GPU entry points (converter, Process, mixer,
-    converter), and the chain on the CPU restatement. Outputs of the two GPU
-    forms must be identical."""
-    from oracle import ref
-
-    from tan_b200 import converter as cvt
-
+def pipeline_inputs(S=32, B=256, L=48000, nb=400):
+    """Seeded inputs of the sample pipeline: S int16 stereo sources of nb
+    blocks (interleaved), one IR per ear and source (channel c = 2 s + ear),
+    the per-ear group map and each channel's input row (stride 2)."""
     g = _rng(6)
     C = 2 * S
-    nb = 60 if quick else 400
     T = nb * B
     src = [(g.uniform(-0.5, 0.5, 2 * T) * 32767).astype(np.int16) for _ in range(S)]
     h = np.stack([_ir(g, L, float(g.uniform(0.2, 1.0))) for _ in range(C)])
     group = np.array([c % 2 for c in range(C)], np.uint32)
     rows_in = [src[c // 2][c % 2:] for c in range(C)]
+    return src, h, group, rows_in
+
+
+def pipeline(ctx, quick=False, S=32, B=256, L=48000):
+    """The sample pipeline (int16 stereo sources -> per-ear convolution -> mix
+    per ear -> int16 interleaved stereo) per block: the fused call and the same
+    chain through the separate GPU entry points (converter, Process, mixer,
+    converter). Outputs of the two GPU forms must be identical. The chain on
+    the CPU restatement is bench.py's cpu_baseline (its pipeline_chain)."""
+    from tan_b200 import converter as cvt
+
+    C = 2 * S
+    nb = 60 if quick else 400
+    T = nb * B
+    src, h, group, rows_in = pipeline_inputs(S, B, L, nb)
     out = {"config": "pipeline", "sources": S, "channels": C, "block": B, "ir": L, "blocks": nb,
            "deadline_ms": 1000.0 * B / FS}
 
@@ -380,22 +388,6 @@ def pipeline(ctx, quick=False, S=32, B=256, L=48000):
     # after restating the fused rules on the separate chain's float outputs
     diff = np.abs(pout.astype(np.int32) - pout2.astype(np.int32))
     out["fused_vs_unfused_max_lsb"] = int(diff.max())
-
-    rc_ = ref.RefConvolution(L, B, C, threads=__import__("os").cpu_count())
-    rc_.update_response_td(h)
-    lat = []
-    nb_cpu = min(nb, 100)
-    for k in range(nb_cpu):
-        t0 = time.perf_counter()
-        x = np.stack([ref.convert_s16_f32(r[2 * k * B:], 1.0, in_step=2, n=B) for r in rows_in])
-        y = np.zeros_like(x)
-        rc_.process(x, None, y)
-        for ear in range(2):
-            ref.convert_f32_s16(ref.mix(y[ear::2]), 1.0)
-        lat.append(1e3 * (time.perf_counter() - t0))
-    rc_.close()
-    out["cpu_restatement"] = {"latency_ms": _pct(lat[5:]), "threads": __import__("os").cpu_count(),
-                              "gsamples_per_s": C * B / (np.mean(lat[5:]) / 1e3) / 1e9}
     return out
 
 
