@@ -392,6 +392,23 @@ void* tanb_engine_stream(tanb_engine* engine);
  * CTAs of the block launch at most. */
 int32_t tanb_engine_info(tanb_engine* engine, int64_t out[8]);
 
+/* No reference counterpart (checkpoint / migration of a session): a snapshot
+ * of a uniformly partitioned session -- both IR slots' spectra (and scales),
+ * delay lines, input history, partial-sum rows, each channel's delay-line
+ * position and IR slot, the session's block count and an IR update staged but
+ * not yet in effect -- in a caller buffer of
+ * tanb_engine_session_snapshot_bytes bytes (host memory). The snapshot waits
+ * for the engine's streams. tanb_engine_open_session_restore opens a session
+ * from one in an engine with the same block, spectrum and partitions per item
+ * (on this GPU or another) whose output continues bit for bit from the next
+ * block on. TANB_NOT_SUPPORTED for non-uniform sessions; TANB_INVALID_ARG for
+ * a short buffer or a snapshot of another engine configuration; admission as
+ * for tanb_engine_open_session. */
+int32_t tanb_engine_session_snapshot_bytes(tanb_engine* engine, int32_t session, uint64_t* bytes);
+int32_t tanb_engine_session_snapshot(tanb_engine* engine, int32_t session, void* buffer, uint64_t bytes);
+int32_t tanb_engine_open_session_restore(tanb_engine* engine, const void* buffer, uint64_t bytes, int32_t* session,
+                                         uint32_t* first_slot);
+
 /* out[0] blocks the session has processed, out[1] its block index at which the
  * last IR update took effect (-1: none yet), out[2] 1 while an update is
  * uploaded but not yet in effect. */

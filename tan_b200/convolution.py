@@ -113,6 +113,10 @@ SIGNATURES = {
     "tanb_engine_profile_read": (_i32, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     "tanb_engine_block_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
     "tanb_convolution_call_times": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
+    "tanb_engine_session_snapshot_bytes": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_uint64)]),
+    "tanb_engine_session_snapshot": (_i32, [_vp, _i32, _vp, ctypes.c_uint64]),
+    "tanb_engine_open_session_restore": (_i32, [_vp, _vp, ctypes.c_uint64, ctypes.POINTER(_i32),
+                                                ctypes.POINTER(ctypes.c_uint32)]),
     "tanb_convolution_snapshot_bytes": (_i32, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "tanb_convolution_snapshot": (_i32, [_vp, _vp, ctypes.c_uint64]),
     "tanb_convolution_restore": (_i32, [_vp, _vp, ctypes.c_uint64]),

@@ -1146,6 +1146,175 @@ int32_t tanb_engine_close_session(tanb_engine* e, int32_t session) {
   return TANB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Session snapshot and restore (uniformly partitioned sessions): the session's
+// arena range (both IR slots' spectra with their scales, delay lines, input
+// history, partial-sum rows), each channel's delay-line position and IR slot,
+// the session's block count and a staged IR update not yet in effect. Another
+// engine with the same block, spectrum and work-item size (on this GPU or
+// another) opens a session from it whose output continues bit for bit. The
+// partial-sum rows are indexed by the parity of the engine's block counter;
+// when the two engines' parities differ the restore swaps the halves.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SessSnapHeader {
+  char magic[8];
+  uint32_t B, spec, Q, C, L, P, nitem, next_parity;
+  uint32_t staged, pad;
+  uint64_t arena_bytes;
+  int64_t blocks, last_swap_block;
+};
+constexpr char kSessSnapMagic[8] = {'T', 'A', 'N', 'B', 'E', 'S', 'N', '1'};
+
+size_t sess_snap_bytes(const Session& s) {
+  return sizeof(SessSnapHeader) + (size_t)s.C * (3 * sizeof(int32_t) + 1) + s.arena_bytes;
+}
+
+// Offset of a channel's partial-sum rows within its arena bytes (the layout
+// open_session lays down).
+size_t part_offset(const tanb_engine* e, int P) {
+  const size_t B = e->B;
+  size_t off = align_up(2 * (size_t)P * B * spec_bytes(e->spec));
+  if (spec_scaled(e->spec)) off += align_up(2 * (size_t)P * 4);
+  off += align_up((size_t)P * B * fdl_bytes(e->spec));
+  off += align_up(B * 4);
+  return off;
+}
+
+}  // namespace
+
+int32_t tanb_engine_session_snapshot_bytes(tanb_engine* e, int32_t session, uint64_t* bytes) {
+  if (bytes) *bytes = 0;
+  if (!e || !bytes) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->sessions.find(session);
+  if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
+  if (!it->second.lv.empty()) return efail(TANB_NOT_SUPPORTED, "snapshots cover uniformly partitioned sessions");
+  *bytes = sess_snap_bytes(it->second);
+  return TANB_OK;
+}
+
+int32_t tanb_engine_session_snapshot(tanb_engine* e, int32_t session, void* buffer, uint64_t bytes) {
+  if (!e || !buffer) return efail(TANB_INVALID_POINTER, "null argument");
+  std::lock_guard<std::mutex> ulock(e->upd_mu);  // no IR upload may still write the session's memory
+  std::lock_guard<std::mutex> lock(e->mu);
+  auto it = e->sessions.find(session);
+  if (it == e->sessions.end()) return efail(TANB_INVALID_ARG, "no session %d", session);
+  const Session& s = it->second;
+  if (!s.lv.empty()) return efail(TANB_NOT_SUPPORTED, "snapshots cover uniformly partitioned sessions");
+  if (bytes < sess_snap_bytes(s))
+    return efail(TANB_INVALID_ARG, "snapshot buffer of %llu bytes, %zu needed", (unsigned long long)bytes,
+                 sess_snap_bytes(s));
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
+  ENG_CUDA(cudaStreamSynchronize(e->stream));
+  ENG_CUDA(cudaStreamSynchronize(e->lstream));
+  char* p = static_cast<char*>(buffer);
+  SessSnapHeader h{};
+  std::memcpy(h.magic, kSessSnapMagic, sizeof(h.magic));
+  h.B = (uint32_t)e->B;
+  h.spec = (uint32_t)e->spec;
+  h.Q = (uint32_t)e->Q;
+  h.C = (uint32_t)s.C;
+  h.L = (uint32_t)s.L;
+  h.P = (uint32_t)s.P;
+  h.nitem = (uint32_t)s.nitem;
+  // the next block's heads read the partial rows of this parity
+  h.next_parity = (uint32_t)(e->k_host & 1);
+  h.staged = s.staged ? 1u : 0u;
+  h.arena_bytes = s.arena_bytes;
+  h.blocks = s.blocks;
+  h.last_swap_block = s.last_swap_block;
+  std::memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  for (int j = 0; j < s.C; ++j) {
+    const EngChan& ch = e->h_chans[s.slot0 + j];
+    const int32_t v[3] = {ch.cur, ch.active, ch.pending};
+    std::memcpy(p, v, sizeof(v));
+    p += sizeof(v);
+  }
+  for (int j = 0; j < s.C; ++j) *p++ = (char)(s.staged && s.staged_mask[j] ? 1 : 0);
+  ENG_CUDA(cudaMemcpy(p, e->arena + s.arena_off * kAlign, s.arena_bytes, cudaMemcpyDeviceToHost));
+  return TANB_OK;
+}
+
+int32_t tanb_engine_open_session_restore(tanb_engine* e, const void* buffer, uint64_t bytes, int32_t* session,
+                                         uint32_t* first_slot) {
+  if (!e || !buffer || !session) return efail(TANB_INVALID_POINTER, "null argument");
+  *session = -1;
+  if (bytes < sizeof(SessSnapHeader)) return efail(TANB_INVALID_ARG, "not a session snapshot");
+  const char* p = static_cast<const char*>(buffer);
+  SessSnapHeader h;
+  std::memcpy(&h, p, sizeof(h));
+  p += sizeof(h);
+  if (std::memcmp(h.magic, kSessSnapMagic, sizeof(h.magic)) != 0) return efail(TANB_INVALID_ARG, "not a session snapshot");
+  if (h.B != (uint32_t)e->B || h.spec != (uint32_t)e->spec || h.Q != (uint32_t)e->Q)
+    return efail(TANB_INVALID_ARG, "snapshot of an engine with block %u, spectrum %u, %u partitions per item", h.B,
+                 h.spec, h.Q);
+  if (h.C == 0 || h.L == 0 || bytes < sizeof(SessSnapHeader) + (size_t)h.C * 13 + h.arena_bytes)
+    return efail(TANB_INVALID_ARG, "short or corrupt session snapshot");
+  int32_t sid = -1;
+  uint32_t slot0 = 0;
+  int32_t r = open_session(e, h.C, h.L, 0, nullptr, nullptr, &sid, &slot0);
+  if (r != TANB_OK) return r;
+  bool match;
+  {
+    std::lock_guard<std::mutex> lock(e->mu);
+    const Session& s = e->sessions[sid];
+    match = (uint32_t)s.P == h.P && (uint32_t)s.nitem == h.nitem && s.arena_bytes == h.arena_bytes;
+  }
+  if (!match) {
+    tanb_engine_close_session(e, sid);
+    return efail(TANB_INVALID_ARG, "snapshot layout does not match this engine's");
+  }
+  std::lock_guard<std::mutex> lock(e->mu);
+  Session& s = e->sessions[sid];
+  ENG_CUDA(cudaSetDevice(e->ctx->device));
+  const char* chan_state = p;
+  p += (size_t)h.C * 3 * sizeof(int32_t);
+  const char* staged_mask = p;
+  p += h.C;
+  // the arena bytes, with the partial-sum halves exchanged when this engine's
+  // next block has the other parity
+  std::vector<char> arena(p, p + h.arena_bytes);
+  if (h.next_parity != (uint32_t)(e->k_host & 1) && s.nitem > 0) {
+    const size_t per = s.arena_bytes / s.C, half = 2 * (size_t)s.nitem * e->B * sizeof(float2);
+    const size_t off = part_offset(e, s.P);
+    for (int j = 0; j < s.C; ++j) {
+      char* a = arena.data() + j * per + off;
+      std::swap_ranges(a, a + half, a + half);
+    }
+  }
+  // the session's clear and table uploads are queued on the audio stream: the
+  // copy goes after them
+  ENG_CUDA(cudaStreamSynchronize(e->stream));
+  ENG_CUDA(cudaMemcpy(e->arena + s.arena_off * kAlign, arena.data(), s.arena_bytes, cudaMemcpyHostToDevice));
+  for (uint32_t j = 0; j < h.C; ++j) {
+    int32_t v[3];
+    std::memcpy(v, chan_state + j * sizeof(v), sizeof(v));
+    EngChan& ch = e->h_chans[s.slot0 + j];
+    ch.cur = ((v[0] % s.P) + s.P) % s.P;
+    ch.active = v[1] & 1;
+    ch.pending = v[2] & 1;
+  }
+  ENG_CUDA(begin_stage(e, h.C * sizeof(EngChan) + 64));
+  ENG_CUDA(stage_copy(e, e->d_chans + s.slot0, e->h_chans + s.slot0, h.C * sizeof(EngChan)));
+  ENG_CUDA(end_stage(e));
+  s.blocks = h.blocks;
+  s.last_swap_block = h.last_swap_block;
+  if (h.staged) {
+    // an IR already transformed into the idle slot: it takes effect on the
+    // next block, as it would have on the source engine
+    s.staged = true;
+    for (uint32_t j = 0; j < h.C; ++j) s.staged_mask[j] = staged_mask[j] ? 1 : 0;
+    ENG_CUDA(cudaEventRecord(s.staged_ev, e->stream));
+  }
+  *session = sid;
+  if (first_slot) *first_slot = slot0;
+  return TANB_OK;
+}
+
 int32_t tanb_engine_update_response_td(tanb_engine* e, int32_t session, const float* const* ir, size_t n,
                                        uint32_t operationFlags) {
   return engine_update(e, session, ir, n, false, operationFlags, nullptr);

@@ -65,6 +65,18 @@ class Session:
         lib().tanb_engine_session_state(self.engine._h, self.id, out)
         return {"blocks": out[0], "last_swap_block": out[1], "staged": bool(out[2])}
 
+    def snapshot(self):
+        """(AMF_RESULT, uint8 array): the session's state, for
+        Engine.open_session_restore on an engine with the same block, spectrum
+        and partitions per item (uniformly partitioned sessions)."""
+        n = ctypes.c_uint64(0)
+        rc = lib().tanb_engine_session_snapshot_bytes(self.engine._h, self.id, ctypes.byref(n))
+        if rc != AMF_OK:
+            return rc, None
+        buf = np.empty(n.value, np.uint8)
+        rc = lib().tanb_engine_session_snapshot(self.engine._h, self.id, buf.ctypes.data, n.value)
+        return rc, (buf if rc == AMF_OK else None)
+
     def close(self) -> int:
         return lib().tanb_engine_close_session(self.engine._h, self.id)
 
@@ -106,6 +118,18 @@ class Engine:
         rc = lib().tanb_engine_open_session(self._h, channels, ir_length, ctypes.byref(sid), ctypes.byref(first))
         if rc != AMF_OK:
             return rc, None
+        return rc, Session(self, sid.value, first.value, channels, ir_length)
+
+    def open_session_restore(self, snapshot):
+        """Opens a session from Session.snapshot(); returns (AMF_RESULT, Session or None)."""
+        buf = np.ascontiguousarray(snapshot, dtype=np.uint8)
+        sid = ctypes.c_int32(0)
+        first = ctypes.c_uint32(0)
+        rc = lib().tanb_engine_open_session_restore(self._h, buf.ctypes.data, buf.size, ctypes.byref(sid),
+                                                    ctypes.byref(first))
+        if rc != AMF_OK:
+            return rc, None
+        channels, ir_length = (int(v) for v in np.frombuffer(buf[20:28].tobytes(), np.uint32))
         return rc, Session(self, sid.value, first.value, channels, ir_length)
 
     def open_session_nu(self, channels: int, ir_length: int, levels):

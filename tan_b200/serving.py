@@ -198,7 +198,9 @@ def serve(ctx, seconds=30.0, rate=20.0, lifetime=30.0, swap_rate=0.5, block=256,
 
 class EngineSlots:
     """A rank's engine as the sharding control plane sees it: open(spec) ->
-    session or None (refused by the budget or the slot table), close(session)."""
+    session or None (refused by the budget or the slot table), close(session),
+    snapshot(session) -> bytes or None (the session's state; uniformly
+    partitioned sessions) and restore(spec, bytes) -> session or None."""
 
     def __init__(self, engine):
         self.engine = engine
@@ -212,6 +214,14 @@ class EngineSlots:
 
     def close(self, sess):
         sess.close()
+
+    def snapshot(self, sess):
+        rc, buf = sess.snapshot()
+        return buf.tobytes() if rc == cv.AMF_OK else None
+
+    def restore(self, spec, blob):
+        rc, sess = self.engine.open_session_restore(np.frombuffer(blob, np.uint8))
+        return sess if rc == cv.AMF_OK else None
 
 
 def serve_sharded(pg, ctx, sessions=600, blocks=1500, swap_rate=0.5, block=256, spectrum=eng.SPECTRUM_FP32,

@@ -13,7 +13,8 @@ RankServer runs the control plane on every rank: the initial placement, the
 re-placement of sessions a rank's engine refused (on the ranks that did not
 refuse them), and, between blocks, the take-over of the sessions of a rank that
 left (announced through the process group's store, so the others learn it on
-the host before their next block and no collective is pending when it goes).
+the host before their next block and no collective is pending when it goes),
+optionally with each session's state handed over so that its audio continues.
 """
 from __future__ import annotations
 
@@ -118,6 +119,7 @@ class RankServer:
         self.handles = {}  # sid -> engine handle of the sessions this rank serves
         self.sessions = {}
         self.left = set()
+        self.restored = []  # sids taken over with their state (leave(handover=True))
 
     def place(self, sessions, rounds: int | None = None):
         """Places `sessions` over the live ranks; sessions a rank's engine
@@ -161,9 +163,19 @@ class RankServer:
             self.placement[s.sid] = -1
         return dict(self.placement)
 
-    def leave(self):
+    def leave(self, handover: bool = False):
         """This rank stops between blocks: it closes its sessions and announces
-        it; the other ranks take its sessions over before their next block."""
+        it; the other ranks take its sessions over before their next block.
+        With handover, each session's state (engine.snapshot) goes into the
+        store first, and the rank that takes the session over restores it, so
+        that its audio continues instead of restarting from silence. (The store
+        carries it here; between GPUs of one node a device-to-device copy
+        would.)"""
+        if handover and self.store is not None:
+            for sid, h in self.handles.items():
+                blob = self.engine.snapshot(h) if hasattr(self.engine, "snapshot") else None
+                if blob is not None:
+                    self.store.set(f"tanb/state/{sid}", blob)
         for h in self.handles.values():
             self.engine.close(h)
         self.handles.clear()
@@ -192,7 +204,14 @@ class RankServer:
             for s in orphans:
                 self.placement[s.sid] = new[s.sid]
                 if new[s.sid] == self.rank:
-                    h = self.engine.open(s)
+                    key = f"tanb/state/{s.sid}"
+                    h = None
+                    if hasattr(self.engine, "restore") and self.store.check([key]):
+                        h = self.engine.restore(s, self.store.get(key))
+                        if h is not None:
+                            self.restored.append(s.sid)
+                    if h is None:
+                        h = self.engine.open(s)
                     if h is not None:
                         self.handles[s.sid] = h
                         taken.append(s.sid)

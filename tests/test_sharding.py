@@ -108,6 +108,7 @@ class FakeEngine:
 
     def __init__(self, budget, refuse=()):
         self.budget, self.used, self.refuse, self.open_ids = budget, 0, set(refuse), set()
+        self.blocks = {}
 
     def open(self, spec):
         need = sh.device_bytes(spec, 256)
@@ -120,6 +121,22 @@ class FakeEngine:
     def close(self, handle):
         self.used -= handle[1]
         self.open_ids.discard(handle[0])
+
+    # session state: blocks served, carried by a handover
+    def tick(self, handles):
+        for h in handles:
+            self.blocks[h[0]] = self.blocks.get(h[0], 0) + 1
+
+    def snapshot(self, handle):
+        return f"{handle[0]}:{self.blocks.get(handle[0], 0)}".encode()
+
+    def restore(self, spec, blob):
+        sid, blocks = (int(v) for v in bytes(blob).decode().split(":"))
+        assert sid == spec.sid
+        h = self.open(spec)
+        if h is not None:
+            self.blocks[sid] = blocks
+        return h
 
 
 def _server_worker(rank, world, port, mode, q):
@@ -137,19 +154,21 @@ def _server_worker(rank, world, port, mode, q):
         pl = srv.place(ss)
         mine_first = sorted(srv.handles)
         taken = []
-        if mode == "leave":
+        if mode in ("leave", "handover"):
             for k in range(200):  # blocks
                 if rank == 1 and k == 3:
-                    srv.leave()
+                    srv.leave(handover=(mode == "handover"))
                     break
                 if rank == 0:
                     taken += srv.check_peers()
                     if srv.left:
                         break
+                srv.engine.tick(srv.handles.values())
                 time.sleep(0.01)
-        q.put((rank, pl, mine_first, sorted(srv.engine.open_ids), taken, None))
+        states = {sid: srv.engine.blocks.get(sid, 0) for sid in taken}
+        q.put((rank, pl, mine_first, sorted(srv.engine.open_ids), taken, None, sorted(srv.restored), states))
     except Exception as e:  # noqa: BLE001
-        q.put((rank, None, None, None, None, repr(e)))
+        q.put((rank, None, None, None, None, repr(e), None, None))
     finally:
         try:
             dist.destroy_process_group()
@@ -173,7 +192,7 @@ def _run_server(mode):
 
 
 def test_rank_server_replaces_refused_sessions_on_the_other_rank():
-    (r0, pl0, m0, open0, _, e0), (r1, pl1, m1, open1, _, e1) = _run_server("ok")
+    (r0, pl0, m0, open0, _, e0, _, _), (r1, pl1, m1, open1, _, e1, _, _) = _run_server("ok")
     assert e0 is None and e1 is None, (e0, e1)
     assert pl0 == pl1  # every rank holds the same placement
     ss = _sessions(24, seed=11)
@@ -184,11 +203,20 @@ def test_rank_server_replaces_refused_sessions_on_the_other_rank():
 
 
 def test_rank_leaving_between_blocks_hands_its_sessions_over():
-    (r0, pl0, m0, open0, taken, e0), (r1, pl1, m1, open1, _, e1) = _run_server("leave")
+    (r0, pl0, m0, open0, taken, e0, restored, _), (r1, pl1, m1, open1, _, e1, _, _) = _run_server("leave")
     assert e0 is None and e1 is None, (e0, e1)
     assert m1 and open1 == []  # rank 1 closed its sessions when it left
     assert sorted(taken) == sorted(m1)  # rank 0 took every one of them over
     assert sorted(open0) == sorted(m0 + m1)
+    assert restored == []  # opened afresh: no state was handed over
+
+
+def test_rank_leaving_with_handover_passes_each_sessions_state():
+    (r0, pl0, m0, open0, taken, e0, restored, states), (r1, _, m1, open1, _, e1, _, _) = _run_server("handover")
+    assert e0 is None and e1 is None, (e0, e1)
+    assert sorted(taken) == sorted(m1) and open1 == []
+    assert restored == sorted(m1)  # every one restored from its state
+    assert all(states[sid] == 3 for sid in m1), states  # the blocks rank 1 had served them
 
 
 def test_device_bytes_follow_the_engine_rule_for_non_uniform_sessions():
