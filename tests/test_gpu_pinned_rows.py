@@ -81,6 +81,31 @@ def test_pinned_rows_equal_staged_rows_and_the_oracle(tan_ctx):
     assert H.rel_err(yp, yr) < TOL
 
 
+def test_pinned_rows_in_one_long_call(tan_ctx):
+    """One Process call of 20 blocks (more than one chunk of staged blocks)
+    on page-locked rows equals the same blocks one call each on pageable rows."""
+    g = H.rng(20261204 + 4)
+    C, B, L, nb = 6, 128, 9000, 20
+    x = H.noise(g, C, nb * B)
+    h = H.irs(g, C, L)
+    conv = make(tan_ctx, L, B, C)
+    assert conv.UpdateResponseTD(h, L) == cv.AMF_OK
+    y0 = np.zeros_like(x)
+    drive(conv, lambda a, b: [np.ascontiguousarray(x[c, a * B:b * B]) for c in range(C)],
+          lambda a, b: [y0[c, a * B:b * B] for c in range(C)], B, nb, {}, per_call=1)
+    conv.Release()
+    tx, xp = pinned((C, nb * B))
+    ty, yp = pinned((C, nb * B))
+    xp[:] = x
+    conv = make(tan_ctx, L, B, C)
+    assert conv.UpdateResponseTD(h, L) == cv.AMF_OK
+    rc, done = conv.Process([xp[c] for c in range(C)], [yp[c] for c in range(C)], nb * B)
+    assert rc == cv.AMF_OK and done == nb * B
+    assert conv.call_times()["in_place"] == 3
+    conv.Release()
+    assert np.array_equal(yp, y0)
+
+
 def test_pinned_rows_with_silent_channels_and_flags(tan_ctx):
     """Null input rows read as silence in place too; a channel stopped with
     STOP_INPUT rings out and its output row is left as the staged path leaves it."""
