@@ -675,7 +675,7 @@ __global__ void __launch_bounds__(UX* SY)
 // the next chunk. Up to NS x RS x BR x 16 bytes are in flight per CTA without
 // holding them in registers. Waits are bounded: on timeout the kernel records
 // kErrBulkWaitTimeout, waits (bounded) for its copies in flight and returns.
-// No multicast; every load reads this GPU's own memory.
+// Every copy lands in this CTA's own shared memory and reads this GPU's own memory.
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
