@@ -10,6 +10,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <vector>
+
 #include "tanb.h"
 
 namespace tanb {
@@ -110,6 +112,16 @@ class TANConvolution {
 
   // No reference counterpart.
   AMF_RESULT Synchronize() { return tanb_convolution_synchronize(conv_); }
+  // The stream state to and from host memory (checkpoint, or a move to an
+  // object with the same Init on another GPU).
+  AMF_RESULT Snapshot(std::vector<uint8_t>& out) {
+    uint64_t n = 0;
+    AMF_RESULT r = tanb_convolution_snapshot_bytes(conv_, &n);
+    if (r != TANB_OK) return r;
+    out.resize((size_t)n);
+    return tanb_convolution_snapshot(conv_, out.data(), n);
+  }
+  AMF_RESULT Restore(const std::vector<uint8_t>& in) { return tanb_convolution_restore(conv_, in.data(), in.size()); }
   tanb_convolution* get() const { return conv_; }
 
  private:

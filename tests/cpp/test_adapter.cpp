@@ -1,7 +1,8 @@
 // C++ caller of the TANConvolution-shaped adapter (include/tanb_convolution.hpp),
 // written the way tan/tests/src/TALibTestConvolution/TALibTestConvolution.cpp
 // drives amf::TANConvolution: create context, create convolution, Init,
-// UpdateResponseTD with BLOCK_UNTIL_READY, then Process block by block.
+// UpdateResponseTD with BLOCK_UNTIL_READY, then Process block by block; halfway
+// the stream moves to a second object by Snapshot / Restore.
 // Known answer: a delta IR at tap 10 with gain 0.9 (the testresponse.wav
 // channel-0 response) delays and scales the input; block 0 is the crossfade
 // from the initial zero IR. Exit code 0 on success.
@@ -38,11 +39,23 @@ int main() {
       s = (float)((seed >> 8) & 0xFFFF) / 32768.0f - 1.0f;
     }
   uint32_t flags[2] = {0, 0};
+  // halfway through, the stream moves to a second object through a snapshot
+  tanb::TANConvolution moved;
+  if (moved.Create(ctx) != TANB_OK || moved.InitGpu(TANB_METHOD_FHT_UNIFORM_PARTITIONED, L, B, C) != TANB_OK) return 7;
+  tanb::TANConvolution* cur = &conv;
   for (uint32_t b = 0; b < nblocks; ++b) {
+    if (b == nblocks / 2) {
+      std::vector<uint8_t> snap;
+      if (conv.Snapshot(snap) != TANB_OK || moved.Restore(snap) != TANB_OK) {
+        std::printf("snapshot / restore failed: %s\n", tanb_last_error());
+        return 8;
+      }
+      cur = &moved;
+    }
     float* ip[2] = {in[0].data() + b * B, in[1].data() + b * B};
     float* op[2] = {out[0].data() + b * B, out[1].data() + b * B};
     size_t done = 0;
-    if (conv.Process(ip, op, B, flags, &done) != TANB_OK || done != B) {
+    if (cur->Process(ip, op, B, flags, &done) != TANB_OK || done != B) {
       std::printf("Process failed at block %u: %s\n", b, tanb_last_error());
       return 6;
     }
@@ -56,6 +69,7 @@ int main() {
     }
   std::printf("adapter known-answer max error %.3e\n", maxerr);
   conv.Release();
+  moved.Release();
   ctx.Release();
   return maxerr < 2e-6 ? 0 : 1;
 }
