@@ -448,7 +448,10 @@ bool pinned_rows(const float* const* rows, int C, size_t n, bool nulls, PinnedRo
   if ((at(c0) & 15) || ((s * 4) & 15)) return false;
   if (!pinned_span(rows[c0], rows[c1] + n)) return false;
   out->stride = s;
-  out->base = rows[c0] - (ptrdiff_t)((long long)c0 * s);
+  // row c is base + c * stride for the listed rows; the base itself is only an
+  // address the kernels offset from (it may precede the first listed row)
+  out->base = reinterpret_cast<const float*>(reinterpret_cast<uintptr_t>(rows[c0]) -
+                                             (uintptr_t)(4LL * c0 * s));
   out->lo = reinterpret_cast<uintptr_t>(rows[c0]);
   out->hi = reinterpret_cast<uintptr_t>(rows[c1] + n);
   return true;
