@@ -196,15 +196,20 @@ def _rows_host(buf, channels: int):
     if isinstance(buf, np.ndarray) and buf.ndim == 2:
         if buf.dtype != np.float32 or not buf.flags.c_contiguous:
             raise TypeError("host buffers must be C-contiguous float32 (channels, samples)")
-        rows = [buf[c] for c in range(buf.shape[0])]
-    else:
-        rows = list(buf)
-        for r in rows:
-            if r is not None and (not isinstance(r, np.ndarray) or r.dtype != np.float32 or not r.flags.c_contiguous):
-                raise TypeError("host rows must be C-contiguous float32 arrays")
+        if buf.shape[0] != channels:
+            raise ValueError(f"expected {channels} channel rows, got {buf.shape[0]}")
+        # row addresses computed at once (a view per row costs microseconds each)
+        ptrs = np.uint64(buf.__array_interface__["data"][0]) + np.arange(channels, dtype=np.uint64) * np.uint64(
+            buf.strides[0])
+        return buf, (ctypes.c_void_p * channels).from_buffer_copy(ptrs.tobytes())
+    rows = list(buf)
+    for r in rows:
+        if r is not None and (not isinstance(r, np.ndarray) or r.dtype != np.float32 or not r.flags.c_contiguous):
+            raise TypeError("host rows must be C-contiguous float32 arrays")
     if len(rows) != channels:
         raise ValueError(f"expected {channels} channel rows, got {len(rows)}")
-    arr = (ctypes.c_void_p * channels)(*[(r.ctypes.data if r is not None else None) for r in rows])
+    arr = (ctypes.c_void_p * channels)(*[(r.__array_interface__["data"][0] if r is not None else None)
+                                         for r in rows])
     return rows, arr
 
 
