@@ -31,7 +31,7 @@ def run(engine, sess, x, B, k0, k1, events, others=()):
 
 
 @pytest.mark.parametrize("spectrum,target_pre", [(eng.SPECTRUM_FP32, 2), (eng.SPECTRUM_FP32, 3),
-                                                 (eng.SPECTRUM_FP16, 2)])
+                                                 (eng.SPECTRUM_FP16, 2), (eng.SPECTRUM_FP24, 2)])
 def test_restored_session_continues_bit_for_bit(tan_ctx, spectrum, target_pre):
     g = H.rng(20261204 + 40 + target_pre + 10 * spectrum)
     B, C, L, nb, cut = 256, 3, 30000, 50, 25
