@@ -193,6 +193,7 @@ struct tanb_engine {
   EngLvlUpd* d_lupd = nullptr;
   float2* d_tw = nullptr;
   int tail_grid = 0;
+  int sms = 148;  // SMs of the device
   size_t nslots_hwm = 0, nitems_hwm = 0;
   // graphs of the host-buffer block, one per set of due level size classes,
   // each valid for the high-water marks in its key; executable graphs
@@ -449,8 +450,12 @@ cudaError_t enqueue_block(tanb_engine* e, const tanb::EngRows& rows, unsigned du
     if ((r = cudaEventRecord(e->ev_fork, e->stream)) != cudaSuccess) return r;
     if ((r = cudaStreamWaitEvent(e->lstream, e->ev_fork, 0)) != cudaSuccess) return r;
   }
+  // at most two heads per SM: their transforms read the twiddles from shared
+  // memory (the latency of the heads bounds such a launch); more heads share
+  // them in L1 (the item CTAs' streaming bounds it)
+  const bool tw_stage = e->nslots_hwm <= 2 * (size_t)e->sms;
   r = tanb::eng_launch_block(e->log2B, e->spec, e->d_chans, (int)e->nslots_hwm, e->d_items, (int)e->nitems_hwm, tc,
-                             e->d_levels, rows, e->d_tw, sync, total, e->stream);
+                             e->d_levels, rows, e->d_tw, tw_stage, sync, total, e->stream);
   if (r != cudaSuccess || !due) return r;
   for (int c = 0; c < e->nclass; ++c) {
     if (!(due >> c & 1u)) continue;
@@ -1041,10 +1046,9 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
   // tail CTAs of the block launch: as many as fit on the GPU at once (B / 4
   // threads each at up to 64 registers: 1024 threads per SM)
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, ctx->device);
   const int per_sm = std::max(1, std::min(32, 1024 / (e->B / 4)));
-  e->tail_grid = sms * per_sm;
+  e->tail_grid = e->sms * per_sm;
   if (r != cudaSuccess) {
     free_engine(e);
     delete e;

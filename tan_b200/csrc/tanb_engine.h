@@ -132,9 +132,11 @@ cudaError_t eng_launch_level_ir(int log2N, int spec, EngLevel* levels, const Eng
 // persistent CTAs over the work items [0, nitems). `total` is the number of
 // CTAs of every kernel of this block (this one and the level heads launched
 // beside it): the last of them to finish advances the channel state.
+// `tw_stage`: the heads copy the twiddle table into shared memory (a launch
+// of few heads) instead of reading it through L1.
 cudaError_t eng_launch_block(int log2B, int spec, EngChan* chans, int nslots, const EngItem* items, int nitems,
                              int tail_ctas, const EngLevel* levels, const EngRows& rows, const float2* tw,
-                             EngSync sync, unsigned total, cudaStream_t st);
+                             bool tw_stage, EngSync sync, unsigned total, cudaStream_t st);
 // Level heads of one size class (2^log2N) for a block at which that size is
 // due: one CTA per level record [0, nlev) of `levels` (the class's table).
 cudaError_t eng_launch_level_heads(int log2B, int log2N, int spec, EngChan* chans, int nslots, const EngLevel* levels,

@@ -307,6 +307,27 @@ __device__ __forceinline__ float2 spec_bin(const EngChan& ch, int slot, int part
   }
 }
 
+// spec_bin with the partition's scale already loaded (`sc`, FP16 / BF16 only):
+// the same value, for loops that read many bins of one partition.
+template <int SPEC, int M>
+__device__ __forceinline__ float2 spec_bin_sc(const EngChan& ch, int slot, int part, int k, float sc) {
+  if constexpr (kScaled<SPEC>) {
+    float2 h = SpecT<SPEC>::get(ch.H, spec_index(ch, slot, part, M) + k);
+    h.x *= sc;
+    h.y *= sc;
+    return h;
+  } else {
+    return spec_bin<SPEC, M>(ch, slot, part, k);
+  }
+}
+
+// Scale of IR partition `part` of `slot` (1 for unscaled spectra).
+template <int SPEC>
+__device__ __forceinline__ float spec_scale(const EngChan& ch, int slot, int part) {
+  if constexpr (kScaled<SPEC>) return ch.scale[(size_t)slot * ch.P + part];
+  else return 1.f;
+}
+
 // Partial-sum row of a channel: rows [2 parity][2 mode][nitem][M] float2; mode
 // 0 = the IR in use for that block, 1 = a newly committed IR (swap block).
 __device__ __forceinline__ float2* part_row(const EngChan& ch, int parity, int mode, int row, int M) {
@@ -510,14 +531,44 @@ __device__ __forceinline__ float* row_out(const EngRows& r, int c) {
 // channel also appends x_k to its input history and adds its levels' output
 // rings (of the IR slot in use; on a swap block those of each IR to its side
 // of the crossfade) in level order.
+//
+// The head shares the GPU with the launch's item CTAs, which keep HBM busy
+// and stream through L1, so each dependent round trip to memory costs
+// microseconds. Every load of the head is therefore issued before the forward
+// transform: the frame to registers, and the tails (partial-sum rows,
+// X_{k-1} * H_1) and H_0 reduced and parked in shared memory (st, sh; on a
+// swap block the new IR's tail in z2, which the bin loop reads before it
+// overwrites it). Each thread reads back only the bins it wrote. The
+// operations and their order are those of a single bin loop.
+// With `tw_stage` the twiddle table also goes to shared memory, by
+// asynchronous copies (no registers held): for launches of few heads, whose
+// transforms would otherwise wait on L2 at every stage. Launches of many
+// heads read it from global memory, where the heads on one SM share it in
+// L1 and the item CTAs keep the L1 capacity for their loads in flight.
 template <int LOG2M, int SPEC>
 __device__ __forceinline__ void eng_head(const EngChan& ch, float2* sm, const float* x, float* y,
-                                         const float2* __restrict__ tw, long long kblk) {
+                                         const float2* __restrict__ twg, bool tw_stage, long long kblk) {
   using S = FftShape<LOG2M>;
-  constexpr int M = S::M, T = S::T;
+  constexpr int M = S::M, T = S::T, E = S::E;
   const int parity = (int)(kblk & 1);
   float2* z = sm;
   float2* z2 = sm + M;
+  float2* st = sm + 2 * M;  // tail of the IR in use, per bin
+  float2* sh = sm + 3 * M;  // H_0 of the IR in use, per bin
+  // twiddles W_2M^j, j < 3M/2 (all the transforms read)
+  const float2* tw = twg;
+  if (tw_stage) {
+    float2* tws = sm + 4 * M;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const int i = threadIdx.x + e * T;  // float4 i of 3M/4
+      const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(reinterpret_cast<float4*>(tws) + i));
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
+                   "l"(reinterpret_cast<const float4*>(twg) + i)
+                   : "memory");
+    }
+    tw = tws;
+  }
   const bool swap = ch.pending != 0;
   const int P = ch.P;
   const int cur = (ch.cur - 1 + P) % P;  // slot of X_k
@@ -534,18 +585,78 @@ __device__ __forceinline__ void eng_head(const EngChan& ch, float2* sm, const fl
     s_nu = ch.nu;
   }
   const bool x_vec = x && (reinterpret_cast<uintptr_t>(x) & 7) == 0;
-  for (int n = threadIdx.x; n < M; n += T) {
+  float2 zr[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int n = threadIdx.x + e * T;
     if (n < M / 2) {
-      z[n] = reinterpret_cast<const float2*>(ch.prev)[n];
+      zr[e] = reinterpret_cast<const float2*>(ch.prev)[n];
     } else if (!x) {
-      z[n] = make_float2(0.f, 0.f);
+      zr[e] = make_float2(0.f, 0.f);
     } else if (x_vec) {
-      z[n] = reinterpret_cast<const float2*>(x)[n - M / 2];
+      zr[e] = reinterpret_cast<const float2*>(x)[n - M / 2];
     } else {
       const float* src = x + 2 * (n - M / 2);
-      z[n] = make_float2(src[0], src[1]);
+      zr[e] = make_float2(src[0], src[1]);
     }
   }
+  // tails: partial sums of the work items in item order, then partition 1;
+  // and partition 0 for the product with X_k. Bins k and M - k per thread,
+  // k < M/2, with bin M/2 beside bin 0 (both use one bin of the pair alone):
+  // two pairs for each of the M/4 threads.
+  constexpr int KQ = (M / 2) / T;
+  static_assert(KQ * T == M / 2, "the head runs M/4 threads");
+  const float2* pa = part_row(ch, parity, 0, 0, M);
+  const float sc0 = spec_scale<SPEC>(ch, slot_old, 0), sc1 = P > 1 ? spec_scale<SPEC>(ch, slot_old, 1) : 1.f;
+#pragma unroll
+  for (int q = 0; q < KQ; ++q) {
+    const int k = threadIdx.x + q * T;
+    const int km = (k == 0) ? M / 2 : M - k;
+    float2 tk = make_float2(0.f, 0.f), tm = tk;
+#pragma unroll 4
+    for (int r = 0; r < ch.nitem; ++r) {
+      const float2 a = pa[(size_t)r * M + k], b = pa[(size_t)r * M + km];
+      tk.x += a.x; tk.y += a.y;
+      tm.x += b.x; tm.y += b.y;
+    }
+    const float2 h0k = spec_bin_sc<SPEC, M>(ch, slot_old, 0, k, sc0);
+    const float2 h0m = spec_bin_sc<SPEC, M>(ch, slot_old, 0, km, sc0);
+    if (P > 1) {
+      const float2 xk = x_bin<SPEC, M>(ch.fdl, ch.cur, k), xm = x_bin<SPEC, M>(ch.fdl, ch.cur, km);
+      const float2 h1k = spec_bin_sc<SPEC, M>(ch, slot_old, 1, k, sc1);
+      tk = (k == 0) ? c_mac_dc(tk, xk, h1k) : c_mac(tk, xk, h1k);
+      tm = c_mac(tm, xm, spec_bin_sc<SPEC, M>(ch, slot_old, 1, km, sc1));
+    }
+    st[k] = tk;
+    st[km] = tm;
+    sh[k] = h0k;
+    sh[km] = h0m;
+  }
+  if (swap) {
+    // the same for the new IR, into z2
+    const float2* pb = part_row(ch, parity, 1, 0, M);
+    for (int q = 0; q < KQ; ++q) {
+      const int k = threadIdx.x + q * T;
+      const int km = (k == 0) ? M / 2 : M - k;
+      float2 uk = make_float2(0.f, 0.f), um = uk;
+      for (int r = 0; r < ch.nitem; ++r) {
+        const float2 a1 = pb[(size_t)r * M + k], b1 = pb[(size_t)r * M + km];
+        uk.x += a1.x; uk.y += a1.y;
+        um.x += b1.x; um.y += b1.y;
+      }
+      if (P > 1) {
+        const float2 xk = x_bin<SPEC, M>(ch.fdl, ch.cur, k), xm = x_bin<SPEC, M>(ch.fdl, ch.cur, km);
+        uk = (k == 0) ? c_mac_dc(uk, xk, spec_bin<SPEC, M>(ch, slot_new, 1, 0))
+                      : c_mac(uk, xk, spec_bin<SPEC, M>(ch, slot_new, 1, k));
+        um = c_mac(um, xm, spec_bin<SPEC, M>(ch, slot_new, 1, km));
+      }
+      z2[k] = uk;
+      z2[km] = um;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) z[threadIdx.x + e * T] = zr[e];
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
   for (int n = threadIdx.x; n < M / 2; n += T) reinterpret_cast<float2*>(ch.prev)[n] = z[n + M / 2];
   if (ch.nu) {
@@ -564,56 +675,36 @@ __device__ __forceinline__ void eng_head(const EngChan& ch, float2* sm, const fl
 
   // X_k goes into delay-line slot cur; X_{k-1} (partition 1) is in ch.cur
   const float inv_n = 1.0f / (float)(2 * M);
-  const float2* pa = part_row(ch, parity, 0, 0, M);
-  const float2* pb = part_row(ch, parity, 1, 0, M);
   for (int k = threadIdx.x; k <= M / 2; k += T) {
     const int km = (k == 0) ? 0 : M - k;
-    // tails: partial sums of the work items in item order, then partition 1
-    float2 tk = make_float2(0.f, 0.f), tm = tk, uk = tk, um = tk;
-    for (int r = 0; r < ch.nitem; ++r) {
-      const float2 a = pa[(size_t)r * M + k], b = pa[(size_t)r * M + km];
-      tk.x += a.x; tk.y += a.y;
-      tm.x += b.x; tm.y += b.y;
-      if (swap) {
-        const float2 a1 = pb[(size_t)r * M + k], b1 = pb[(size_t)r * M + km];
-        uk.x += a1.x; uk.y += a1.y;
-        um.x += b1.x; um.y += b1.y;
-      }
-    }
-    if (P > 1) {
-      const float2 xk = x_bin<SPEC, M>(ch.fdl, ch.cur, k), xm = x_bin<SPEC, M>(ch.fdl, ch.cur, km);
-      const float2 hk = spec_bin<SPEC, M>(ch, slot_old, 1, k);
-      if (k == 0) {
-        tk = c_mac_dc(tk, xk, hk);
-        if (swap) uk = c_mac_dc(uk, xk, spec_bin<SPEC, M>(ch, slot_new, 1, 0));
-      } else {
-        tk = c_mac(tk, xk, hk);
-        tm = c_mac(tm, xm, spec_bin<SPEC, M>(ch, slot_old, 1, km));
-        if (swap) {
-          uk = c_mac(uk, xk, spec_bin<SPEC, M>(ch, slot_new, 1, k));
-          um = c_mac(um, xm, spec_bin<SPEC, M>(ch, slot_new, 1, km));
-        }
-      }
+    const float2 tk = st[k], tm = st[km];
+    // the new IR's tail and H_0 on a swap block
+    float2 uk = make_float2(0.f, 0.f), um = uk, gk = uk, gm = uk;
+    if (swap) {
+      uk = z2[k];
+      um = z2[km];
+      gk = spec_bin<SPEC, M>(ch, slot_new, 0, k);
+      gm = spec_bin<SPEC, M>(ch, slot_new, 0, km);
     }
     if (k == 0) {
       const float2 X = rfft_post_dc(z[0]);
       x_put<SPEC, M>(ch.fdl, cur, 0, X);
-      z[0] = irfft_pre_dc(c_mac_dc(tk, X, spec_bin<SPEC, M>(ch, slot_old, 0, 0)), inv_n);
-      if (swap) z2[0] = irfft_pre_dc(c_mac_dc(uk, X, spec_bin<SPEC, M>(ch, slot_new, 0, 0)), inv_n);
+      z[0] = irfft_pre_dc(c_mac_dc(tk, X, sh[0]), inv_n);
+      if (swap) z2[0] = irfft_pre_dc(c_mac_dc(uk, X, gk), inv_n);
     } else {
-      const float2 wk = __ldg(tw + k), wm = __ldg(tw + km);
+      const float2 wk = tw[k], wm = tw[km];
       const float2 a = z[k], b = z[km];
       const float2 Xk = rfft_post(a, b, wk);
       const float2 Xm = rfft_post(b, a, wm);
       x_put<SPEC, M>(ch.fdl, cur, k, Xk);
       if (km != k) x_put<SPEC, M>(ch.fdl, cur, km, Xm);
-      const float2 Ak = c_mac(tk, Xk, spec_bin<SPEC, M>(ch, slot_old, 0, k));
-      const float2 Am = c_mac(tm, Xm, spec_bin<SPEC, M>(ch, slot_old, 0, km));
+      const float2 Ak = c_mac(tk, Xk, sh[k]);
+      const float2 Am = c_mac(tm, Xm, sh[km]);
       z[k] = irfft_pre(Ak, Am, wk, inv_n);
       if (km != k) z[km] = irfft_pre(Am, Ak, wm, inv_n);
       if (swap) {
-        const float2 Bk = c_mac(uk, Xk, spec_bin<SPEC, M>(ch, slot_new, 0, k));
-        const float2 Bm = c_mac(um, Xm, spec_bin<SPEC, M>(ch, slot_new, 0, km));
+        const float2 Bk = c_mac(uk, Xk, gk);
+        const float2 Bm = c_mac(um, Xm, gm);
         z2[k] = irfft_pre(Bk, Bm, wk, inv_n);
         if (km != k) z2[km] = irfft_pre(Bm, Bk, wm, inv_n);
       }
@@ -698,9 +789,9 @@ __device__ __forceinline__ void finish_block(EngChan* __restrict__ chans, int ns
 template <int LOG2M, int SPEC>
 __global__ void __launch_bounds__(FftShape<LOG2M>::T, 1024 / FftShape<LOG2M>::T)
     eng_block_kernel(EngChan* __restrict__ chans, int nslots, const EngItem* __restrict__ items, int nitems,
-                     const EngLevel* __restrict__ levels, EngRows rows, const float2* __restrict__ tw, EngSync sync,
-                     unsigned total) {
-  extern __shared__ float2 sm[];
+                     const EngLevel* __restrict__ levels, EngRows rows, const float2* __restrict__ tw, int tw_stage,
+                     EngSync sync, unsigned total) {
+  extern __shared__ __align__(16) float2 sm[];  // 16-byte copies into the head's twiddle table
   const long long k = *sync.block;  // blocks processed before this one
   const int parity = (int)(k & 1);
   // CTAs [0, stride) stream the work items and are dispatched first; the
@@ -710,7 +801,7 @@ __global__ void __launch_bounds__(FftShape<LOG2M>::T, 1024 / FftShape<LOG2M>::T)
   if ((int)blockIdx.x >= stride) {
     const int c = (int)blockIdx.x - stride;
     const EngChan ch = chans[c];
-    if (ch.run) eng_head<LOG2M, SPEC>(ch, sm, row_in(rows, c), row_out(rows, c), tw, k);
+    if (ch.run) eng_head<LOG2M, SPEC>(ch, sm, row_in(rows, c), row_out(rows, c), tw, tw_stage != 0, k);
   } else {
     for (int it = (int)blockIdx.x; it < nitems; it += stride) {
       const EngItem w = items[it];
@@ -936,13 +1027,22 @@ __global__ void eng_mark_pending_kernel(EngChan* __restrict__ chans, int first, 
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) chans[first + i].pending = 1;
 }
 
+// Dynamic shared memory of the block kernel: the head's transform buffers
+// (z, z2) and its prefetched tail and H_0 bins (st, sh), M complex values
+// each, and with `tw_stage` 3M/2 twiddles. At B / 4 threads per CTA and 1024
+// threads per SM that is 128 KB (176 KB) per SM at every block size.
+template <int LOG2M>
+constexpr int eng_block_smem(bool tw_stage) {
+  return (4 * (1 << LOG2M) + (tw_stage ? 3 * (1 << LOG2M) / 2 : 0)) * (int)sizeof(float2);
+}
+
 template <int LOG2M, int SPEC>
 cudaError_t attrs_t() {
-  const int smem = 2 * (1 << LOG2M) * (int)sizeof(float2);
-  cudaError_t e =
-      cudaFuncSetAttribute(eng_block_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(eng_block_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       eng_block_smem<LOG2M>(true));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(eng_ir_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem / 2);
+  return cudaFuncSetAttribute(eng_ir_kernel<LOG2M, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (1 << LOG2M) * (int)sizeof(float2));
 }
 
 template <int LOG2M>
@@ -995,11 +1095,11 @@ cudaError_t level_ir_t(EngLevel* levels, const EngLvlUpd* upd, int nupd, int max
 
 template <int LOG2M, int SPEC>
 cudaError_t block_t(EngChan* chans, int nslots, const EngItem* items, int nitems, int tail_ctas,
-                    const EngLevel* levels, const EngRows& rows, const float2* tw, EngSync sync, unsigned total,
-                    cudaStream_t st) {
+                    const EngLevel* levels, const EngRows& rows, const float2* tw, bool tw_stage, EngSync sync,
+                    unsigned total, cudaStream_t st) {
   using S = FftShape<LOG2M>;
-  eng_block_kernel<LOG2M, SPEC><<<nslots + tail_ctas, S::T, 2 * S::M * sizeof(float2), st>>>(
-      chans, nslots, items, nitems, levels, rows, tw, sync, total);
+  eng_block_kernel<LOG2M, SPEC><<<nslots + tail_ctas, S::T, eng_block_smem<LOG2M>(tw_stage), st>>>(
+      chans, nslots, items, nitems, levels, rows, tw, tw_stage ? 1 : 0, sync, total);
   return cudaGetLastError();
 }
 
@@ -1134,9 +1234,10 @@ unsigned eng_block_ctas(int nslots, int tail_ctas) { return (unsigned)(nslots + 
 
 cudaError_t eng_launch_block(int log2B, int spec, EngChan* chans, int nslots, const EngItem* items, int nitems,
                              int tail_ctas, const EngLevel* levels, const EngRows& rows, const float2* tw,
-                             EngSync sync, unsigned total, cudaStream_t st) {
+                             bool tw_stage, EngSync sync, unsigned total, cudaStream_t st) {
   if (nslots <= 0) return cudaSuccess;
-  ENG_DISPATCH(log2B, spec, block_t, chans, nslots, items, nitems, tail_ctas, levels, rows, tw, sync, total, st);
+  ENG_DISPATCH(log2B, spec, block_t, chans, nslots, items, nitems, tail_ctas, levels, rows, tw, tw_stage, sync, total,
+               st);
 }
 
 cudaError_t eng_launch_level_heads(int log2B, int log2N, int spec, EngChan* chans, int nslots, const EngLevel* levels,
