@@ -285,3 +285,43 @@ def test_engine_scaled_spectra_with_denormal_partitions_stay_finite(tan_ctx, spe
     exp = fp64.stream_fp64(x, B, [(0, {c: h[c] for c in range(C)})])
     for c in range(C):
         assert fp64.error_db(y[c], exp[c]) < (-60 if spectrum == eng.SPECTRUM_FP16 else -40)
+
+
+@pytest.mark.parametrize("B", [128, 512, 1024, 2048])
+def test_engine_block_sizes_match_alone_and_fp64(tan_ctx, B):
+    """Every block size the engine runs besides 256: sessions of one, two and
+    eight partitions with IR swaps (on the first block, mid-stream, and on
+    the block a later session opens) equal each session alone through the
+    single-object path and the FP64 statement."""
+    g = H.rng(20261204 + 60 + B)
+    nb = 20
+    specs = [(2, B, 0, [0, 9]), (1, 2 * B, 1, [0, 5]), (3, 7 * B + 5, 0, [0, 1, 13])]
+    sessions = make_sessions(g, B, specs, nb)
+    engine = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=1 << 30, max_channels=16, partitions_per_item=2)
+    outs = run_engine(engine, sessions, nb)
+    engine.release()
+    for s, y in zip(sessions, outs):
+        ya = alone(tan_ctx, s["x"], B, s["events"])
+        rms = np.sqrt(np.mean(ya.astype(np.float64) ** 2))
+        assert np.max(np.abs(y - ya)) <= TOL * rms, (B, s["C"], s["L"])
+        exp = fp64.stream_fp64(s["x"], B, [(k, {c: ir[c] for c in range(s["C"])}) for k, ir in s["events"].items()])
+        for c in range(s["C"]):
+            assert fp64.error_db(y[c], exp[c]) < -120, (B, s["L"], c)
+
+
+def test_engine_many_heads_same_bits(tan_ctx):
+    """A launch with more heads than twice the SM count reads the twiddle table
+    through L1 instead of copying it to shared memory: a session in it gives
+    the samples it gives in a launch of few heads, bit for bit."""
+    g = H.rng(20261204 + 70)
+    B, nb = 256, 12
+    test = make_sessions(g, B, [(2, 5000, 0, [0, 6])], nb)[0]
+    crowd = make_sessions(g, B, [(8, 1000, 0, [0])] * 40, nb)  # 320 more channel slots
+    big = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=1 << 30, max_channels=400, partitions_per_item=8)
+    y_big = run_engine(big, crowd + [test], nb)[-1]
+    assert big.info()["slot_hwm"] > 2 * 148
+    big.release()
+    small = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=1 << 28, max_channels=8, partitions_per_item=8)
+    y_small = run_engine(small, [test], nb)[0]
+    small.release()
+    assert np.array_equal(y_big, y_small)
