@@ -163,7 +163,7 @@ struct tanb_engine {
   int B = 0, log2B = 0, spec = 0, Q = 32;
   size_t budget = 0, max_channels = 0, max_items = 0;
   cudaStream_t stream = nullptr;      // audio path: blocks, commits
-  cudaStream_t lstream = nullptr;     // level heads beside the block launch
+  std::vector<cudaStream_t> lstreams;  // level heads beside the block launch, one stream per size class
   cudaStream_t upd_stream = nullptr;  // IR uploads and transforms
   std::mutex upd_mu;                  // serialises IR updates (taken before mu)
   char* arena = nullptr;
@@ -206,7 +206,8 @@ struct tanb_engine {
   std::map<unsigned, BlockGraph> graphs;
   std::vector<cudaGraphExec_t> retired;
   cudaEvent_t ev_out = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_joins;  // one per level size class
   cudaEvent_t ev_audio = nullptr;  // audio-stream point an IR upload waits for
   // Pinned staging of the table uploads of session opens and closes: they copy
   // from here rather than from the live mirrors (which the audio path keeps
@@ -278,7 +279,8 @@ void destroy_graphs(tanb_engine* e) {
 void free_engine(tanb_engine* e) {
   if (e->upd_stream) cudaStreamSynchronize(e->upd_stream);
   if (e->stream) cudaStreamSynchronize(e->stream);
-  if (e->lstream) cudaStreamSynchronize(e->lstream);
+  for (cudaStream_t ls : e->lstreams)
+    if (ls) cudaStreamSynchronize(ls);
   for (auto& kv : e->sessions)
     if (kv.second.staged_ev) cudaEventDestroy(kv.second.staged_ev);
   e->sessions.clear();
@@ -306,12 +308,14 @@ void free_engine(tanb_engine* e) {
   if (e->ev_upd_done) cudaEventDestroy(e->ev_upd_done);
   if (e->ev_out) cudaEventDestroy(e->ev_out);
   if (e->ev_fork) cudaEventDestroy(e->ev_fork);
-  if (e->ev_join) cudaEventDestroy(e->ev_join);
+  for (cudaEvent_t ev : e->ev_joins)
+    if (ev) cudaEventDestroy(ev);
   if (e->ev_audio) cudaEventDestroy(e->ev_audio);
   if (e->pa) cudaEventDestroy(e->pa);
   if (e->pb) cudaEventDestroy(e->pb);
   if (e->upd_stream) cudaStreamDestroy(e->upd_stream);
-  if (e->lstream) cudaStreamDestroy(e->lstream);
+  for (cudaStream_t ls : e->lstreams)
+    if (ls) cudaStreamDestroy(ls);
   if (e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -436,7 +440,7 @@ unsigned due_mask(const tanb_engine* e, long long k) {
 }
 
 // Enqueues one block: the block launch over all slots and work items, and the
-// heads of the due level classes on the level stream beside it (forked from
+// heads of each due level class on that class's stream beside it (forked from
 // and joined back into the audio stream, so that a captured graph holds them
 // as parallel branches).
 cudaError_t enqueue_block(tanb_engine* e, const tanb::EngRows& rows, unsigned due) {
@@ -448,7 +452,8 @@ cudaError_t enqueue_block(tanb_engine* e, const tanb::EngRows& rows, unsigned du
   cudaError_t r;
   if (due) {
     if ((r = cudaEventRecord(e->ev_fork, e->stream)) != cudaSuccess) return r;
-    if ((r = cudaStreamWaitEvent(e->lstream, e->ev_fork, 0)) != cudaSuccess) return r;
+    for (int c = 0; c < e->nclass; ++c)
+      if ((due >> c & 1u) && (r = cudaStreamWaitEvent(e->lstreams[c], e->ev_fork, 0)) != cudaSuccess) return r;
   }
   // at most two heads per SM: their transforms read the twiddles from shared
   // memory (the latency of the heads bounds such a launch); more heads share
@@ -461,11 +466,12 @@ cudaError_t enqueue_block(tanb_engine* e, const tanb::EngRows& rows, unsigned du
     if (!(due >> c & 1u)) continue;
     r = tanb::eng_launch_level_heads(e->log2B, e->log2B + 1 + c, e->spec, e->d_chans, (int)e->nslots_hwm,
                                      e->d_levels + (size_t)c * e->max_channels, (int)e->lvl_hwm[c], rows,
-                                     e->d_tw_lv[c], sync, total, e->lstream);
+                                     e->d_tw_lv[c], sync, total, e->lstreams[c]);
     if (r != cudaSuccess) return r;
+    if ((r = cudaEventRecord(e->ev_joins[c], e->lstreams[c])) != cudaSuccess) return r;
+    if ((r = cudaStreamWaitEvent(e->stream, e->ev_joins[c], 0)) != cudaSuccess) return r;
   }
-  if ((r = cudaEventRecord(e->ev_join, e->lstream)) != cudaSuccess) return r;
-  return cudaStreamWaitEvent(e->stream, e->ev_join, 0);
+  return cudaSuccess;
 }
 
 std::vector<size_t> graph_key(const tanb_engine* e) {
@@ -979,7 +985,14 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   int prio_low = 0, prio_high = 0;
   if (r == cudaSuccess) r = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   if (r == cudaSuccess) r = cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, prio_high);
-  if (r == cudaSuccess) r = cudaStreamCreateWithPriority(&e->lstream, cudaStreamNonBlocking, prio_high);
+  // the level heads of each size class on a stream of their own, so that the
+  // classes due at one block run side by side
+  e->lstreams.assign(e->nclass, nullptr);
+  e->ev_joins.assign(e->nclass, nullptr);
+  for (int c = 0; c < e->nclass && r == cudaSuccess; ++c) {
+    r = cudaStreamCreateWithPriority(&e->lstreams[c], cudaStreamNonBlocking, prio_high);
+    if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_joins[c], cudaEventDisableTiming);
+  }
   if (r == cudaSuccess) r = cudaStreamCreateWithPriority(&e->upd_stream, cudaStreamNonBlocking, prio_low);
   const size_t io = e->max_channels * e->B;
   const size_t nlev = (size_t)e->nclass * e->max_channels;
@@ -1000,7 +1013,6 @@ int32_t tanb_engine_create(tanb_context* ctx, uint32_t block, uint32_t spectrum,
   if (r == cudaSuccess) r = cudaMallocHost(&e->h_lupd, tanb::kMaxLevels * e->max_channels * sizeof(EngLvlUpd));
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
-  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_audio, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_stage, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&e->ev_upd_done, cudaEventDisableTiming);
@@ -1213,7 +1225,7 @@ int32_t tanb_engine_session_snapshot(tanb_engine* e, int32_t session, void* buff
   ENG_CUDA(cudaSetDevice(e->ctx->device));
   ENG_CUDA(cudaStreamSynchronize(e->upd_stream));
   ENG_CUDA(cudaStreamSynchronize(e->stream));
-  ENG_CUDA(cudaStreamSynchronize(e->lstream));
+  for (cudaStream_t ls : e->lstreams) ENG_CUDA(cudaStreamSynchronize(ls));
   char* p = static_cast<char*>(buffer);
   SessSnapHeader h{};
   std::memcpy(h.magic, kSessSnapMagic, sizeof(h.magic));
