@@ -55,6 +55,7 @@ def measure(ctx, B: int, L: int, C: int, steps: int = 120, warmup: int = 8, seed
     y = torch.zeros_like(x)
     flush_w = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
     flush_r = torch.ones(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
+    flush_r2 = torch.ones(64 << 20, dtype=torch.float32, device=f"cuda:{dev}")
     results = []
     idx = 0
     while True:
@@ -72,9 +73,12 @@ def measure(ctx, B: int, L: int, C: int, steps: int = 120, warmup: int = 8, seed
         stream = torch.cuda.ExternalStream(conv.stream(), device=dev)
 
         def flush():
+            # a 256 MiB write, then two 256 MiB reads, so that no dirty line of
+            # the write is left in L2 to be written back inside a timed block
             with torch.cuda.stream(stream):
                 flush_w.zero_()
                 flush_r.sum()
+                flush_r2.sum()
 
         for _ in range(warmup):
             flush()
