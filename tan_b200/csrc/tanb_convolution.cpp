@@ -374,45 +374,43 @@ int32_t nu_process(tanb_convolution* v, Mem in_mem, const float* const* in, Mem 
 // unequal strides, misalignment, input and output spans that overlap -- takes
 // the staging path.
 // ---------------------------------------------------------------------------
-using PtrAttrFn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+using PtrAttrsFn = CUresult (*)(unsigned int, CUpointer_attribute*, void**, CUdeviceptr);
 
-PtrAttrFn ptr_attr_fn() {
-  static const PtrAttrFn fn = [] {
+PtrAttrsFn ptr_attrs_fn() {
+  static const PtrAttrsFn fn = [] {
     void* f = nullptr;
     cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) != cudaSuccess ||
+    if (cudaGetDriverEntryPoint("cuPointerGetAttributes", &f, cudaEnableDefault, &q) != cudaSuccess ||
         q != cudaDriverEntryPointSuccess) {
       (void)cudaGetLastError();
-      return static_cast<PtrAttrFn>(nullptr);
+      return static_cast<PtrAttrsFn>(nullptr);
     }
-    return reinterpret_cast<PtrAttrFn>(f);
+    return reinterpret_cast<PtrAttrsFn>(f);
   }();
   return fn;
 }
 
-bool host_mapped_same(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost && a.devicePointer == p;
-}
-
-// True when the bytes [lo, hi) lie in one pinned host allocation mapped at
-// the same addresses on the device.
+// True when the bytes [lo, hi) lie in one page-locked host allocation that the
+// device addresses at the same virtual addresses: one driver query of the
+// first byte (memory type, managed or not, its device address, the range of
+// its allocation). An address the driver does not know (pageable memory)
+// comes back with the default values, which fail the test. Within one
+// allocation the device mapping is one linear range, so identity at `lo`
+// holds for every byte up to `hi`.
 bool pinned_span(const void* lo, const void* hi) {
-  const PtrAttrFn fn = ptr_attr_fn();
+  const PtrAttrsFn fn = ptr_attrs_fn();
   if (!fn || hi <= lo) return false;
-  if (!host_mapped_same(lo)) return false;
-  CUdeviceptr start = 0;
+  unsigned int mem_type = 0, managed = 0;
+  CUdeviceptr dptr = 0, start = 0;
   size_t size = 0;
+  CUpointer_attribute attrs[5] = {CU_POINTER_ATTRIBUTE_MEMORY_TYPE, CU_POINTER_ATTRIBUTE_IS_MANAGED,
+                                  CU_POINTER_ATTRIBUTE_DEVICE_POINTER, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR,
+                                  CU_POINTER_ATTRIBUTE_RANGE_SIZE};
+  void* data[5] = {&mem_type, &managed, &dptr, &start, &size};
   const CUdeviceptr l = (CUdeviceptr) reinterpret_cast<uintptr_t>(lo);
-  if (fn(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, l) != CUDA_SUCCESS) return false;
-  if (fn(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, l) != CUDA_SUCCESS) return false;
   const CUdeviceptr h = (CUdeviceptr) reinterpret_cast<uintptr_t>(hi);
-  if (l < start || h > start + size) return false;
-  return host_mapped_same(static_cast<const char*>(hi) - 1);
+  if (fn(5, attrs, data, l) != CUDA_SUCCESS) return false;
+  return mem_type == CU_MEMORYTYPE_HOST && !managed && dptr == l && l >= start && h <= start + size;
 }
 
 struct PinnedRows {
