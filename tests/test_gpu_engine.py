@@ -325,3 +325,23 @@ def test_engine_many_heads_same_bits(tan_ctx):
     y_small = run_engine(small, [test], nb)[0]
     small.release()
     assert np.array_equal(y_big, y_small)
+
+
+@pytest.mark.parametrize("B", [128, 1024])
+@pytest.mark.parametrize("spectrum,limit_db", [(eng.SPECTRUM_FP16, -60.0), (eng.SPECTRUM_BF16, -40.0),
+                                               (eng.SPECTRUM_FP24, -90.0)])
+def test_engine_reduced_precision_at_other_block_sizes(tan_ctx, B, spectrum, limit_db):
+    """The 16- and 24-bit spectrum forms at the smallest and a large block
+    size, with a swap mid-stream and a session of one partition: every
+    channel within the form's bound of the FP64 statement."""
+    g = H.rng(20261204 + 80 + B + spectrum)
+    nb = 16
+    specs = [(2, 9 * B + 7, 0, [0, 6]), (1, B, 1, [0])]
+    sessions = make_sessions(g, B, specs, nb)
+    engine = eng.Engine(tan_ctx, B, spectrum, budget_bytes=1 << 28, max_channels=16, partitions_per_item=4)
+    outs = run_engine(engine, sessions, nb)
+    engine.release()
+    for s, y in zip(sessions, outs):
+        exp = fp64.stream_fp64(s["x"], B, [(k, {c: ir[c] for c in range(s["C"])}) for k, ir in s["events"].items()])
+        for c in range(s["C"]):
+            assert fp64.error_db(y[c], exp[c]) < limit_db, (B, spectrum, s["L"], c)
