@@ -309,12 +309,13 @@ def test_engine_block_sizes_match_alone_and_fp64(tan_ctx, B):
             assert fp64.error_db(y[c], exp[c]) < -120, (B, s["L"], c)
 
 
-def test_engine_many_heads_same_bits(tan_ctx):
+@pytest.mark.parametrize("B", [256, 1024])
+def test_engine_many_heads_same_bits(tan_ctx, B):
     """A launch with more heads than twice the SM count reads the twiddle table
     through L1 instead of copying it to shared memory: a session in it gives
     the samples it gives in a launch of few heads, bit for bit."""
-    g = H.rng(20261204 + 70)
-    B, nb = 256, 12
+    g = H.rng(20261204 + 70 + B)
+    nb = 12
     test = make_sessions(g, B, [(2, 5000, 0, [0, 6])], nb)[0]
     crowd = make_sessions(g, B, [(8, 1000, 0, [0])] * 40, nb)  # 320 more channel slots
     big = eng.Engine(tan_ctx, B, eng.SPECTRUM_FP32, budget_bytes=1 << 30, max_channels=400, partitions_per_item=8)
